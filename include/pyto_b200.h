@@ -1,0 +1,209 @@
+/*
+ * pyto_b200.h -- C ABI of the B200 voxel hex8 structural-FEA library.
+ *
+ * One shared library (libpyto_b200.so) built for sm_100a.  Every entry point
+ * takes plain pointers and sizes; device pointers are CUDA global-memory
+ * pointers of the calling process's current device, `stream` is a
+ * cudaStream_t (NULL = legacy default stream).  Calls are stream-ordered and
+ * return a status code; none aborts the process.  The library never allocates
+ * device memory: entry points that need scratch take a caller-provided
+ * workspace whose size is given by pyto_workspace_bytes().
+ *
+ * Connectivity is implicit.  A grid of nelx*nely*nelz box elements of size
+ * (hx,hy,hz) numbers nodes  n = ix + (nelx+1)*(iy + (nely+1)*iz),
+ * elements e = ex + nelx*(ey + nely*ez) and DOFs 3n+{0,1,2} (x,y,z), element
+ * corners in the order (0,0,0),(1,0,0),(1,1,0),(0,1,0),(0,0,1),(1,0,1),
+ * (1,1,1),(0,1,1) -- exactly PyTO's HexMesher.grid_mesh / createEdofMatStructural
+ * numbering (src/hex_mesher.py:72-169, :1080-1095).
+ *
+ * Each declaration names the PyTO (UW-ERSL/PyTO) interface it replaces.
+ */
+#ifndef PYTO_B200_H
+#define PYTO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define PYTO_OK 0
+#define PYTO_NOT_CONVERGED 1     /* iteration cap reached; result is the last iterate */
+#define PYTO_ERR_ARG (-1)        /* invalid argument (null pointer, bad size, bad Ke) */
+#define PYTO_ERR_CUDA (-2)       /* a CUDA runtime call failed */
+#define PYTO_ERR_WORKSPACE (-3)  /* workspace missing or too small */
+#define PYTO_ERR_BREAKDOWN (-4)  /* Krylov breakdown: p.Kp <= 0 or a non-finite scalar */
+#define PYTO_ERR_TOO_LARGE (-5)  /* size beyond a fixed limit of the entry point */
+
+/* ---- matvec / filter modes ---------------------------------------------- */
+#define PYTO_MASK_IN 1   /* treat fixed DOFs of the input vector as zero */
+#define PYTO_MASK_OUT 2  /* write zero to fixed DOFs of the output vector */
+
+#define PYTO_FILTER_RAW 0      /* y = H x                                  */
+#define PYTO_FILTER_DENSITY 1  /* y = (H x) / Hs                           */
+#define PYTO_FILTER_CHAIN 2    /* y = H^T (x / Hs)        (hs required)    */
+#define PYTO_FILTER_SENS 3     /* y = H (w .* x) / Hs ./ w  (w required)   */
+#define PYTO_FILTER_HS 4       /* y = Hs = H 1                             */
+
+/* ---- workspace kinds for pyto_workspace_bytes ---------------------------- */
+#define PYTO_WS_REDUCE 0  /* reductions of matvec/energy/stress (dot, compliance, p-norm) */
+#define PYTO_WS_PCG 1     /* pyto_pcg_solve                                               */
+#define PYTO_WS_DPCG 2    /* pyto_dpcg_setup / pyto_dpcg_solve (coarse inverse is separate) */
+#define PYTO_WS_OC 3      /* pyto_oc_update                                               */
+
+/* The operator: grid + the element stiffness matrix, plus the data derived
+ * from Ke that the kernels use (Ke rotated into the 8x8 Hadamard corner basis,
+ * where a box hex8 Ke splits into eight 3x3 blocks, and the corner diagonal). */
+typedef struct pyto_operator {
+  int32_t nelx, nely, nelz;
+  int32_t reserved;
+  double hx, hy, hz;
+  double E, nu;          /* material of Ke (stress recovery uses them) */
+  double ke[576];        /* 24x24 Ke, row-major, reference DOF order */
+  double khat[8][3][3];  /* parity-class blocks of Phi Ke Phi^T / 64 */
+  double kdiag[3];       /* Ke[3a+c][3a+c], equal for every corner a */
+} pyto_operator_t;
+
+typedef struct pyto_solve_cfg {
+  double rtol;          /* relative tolerance of the stopping rule */
+  int32_t max_iters;    /* iteration cap */
+  int32_t stop_rule;    /* 0: ||r||_2 < rtol ||b||_2 (scipy cg); 1: sqrt(r.z / r0.z0) <= rtol (PyTO DPCG) */
+  int32_t check_every;  /* host polls convergence every this many iterations (>=1) */
+  int32_t x0_given;     /* 1: u holds the initial guess on entry; 0: start from zero */
+} pyto_solve_cfg_t;
+
+typedef struct pyto_solve_status {
+  int32_t converged;    /* 1 if the stopping rule was met */
+  int32_t iters;        /* Krylov iterations performed */
+  int32_t breakdown;    /* 1 if p.Kp <= 0 or a scalar became non-finite */
+  int32_t reserved;
+  double rel_res;       /* stopping quantity at exit */
+  double true_rel_res;  /* ||b - K u||_2 / ||b||_2 recomputed in FP64 at exit */
+} pyto_solve_status_t;
+
+/* Deflation space: node groups with rigid-body modes about the group centre.
+ * modes = 6: columns [tx,ty,tz,rx,ry,rz] per group (src/deflation.py:386-457);
+ * modes = 3: translations only.  All pointers are device pointers. */
+typedef struct pyto_deflation {
+  int32_t ngroups;
+  int32_t modes;               /* 3 or 6 */
+  const int32_t* node_group;   /* [nnodes] group of each node */
+  const int32_t* group_ptr;    /* [ngroups+1] CSR offsets of group_nodes */
+  const int32_t* group_nodes;  /* [nnodes] node ids sorted by group */
+  const double* group_center;  /* [ngroups*3] centroid of each group */
+  double* coarse_inv;          /* [nc*nc], nc = ngroups*modes: written by pyto_dpcg_setup */
+  double shift;                /* diagonal shift added to W^T K W */
+  int32_t shift_relative;      /* 1: shift scales the mean diagonal; 0: absolute (PyTO: 1e-10) */
+  int32_t reserved;
+} pyto_deflation_t;
+
+/* ---- version / workspace ------------------------------------------------- */
+int pyto_version(void);
+/* Bytes of workspace for a call of the given kind on this operator (for
+ * PYTO_WS_DPCG: any coarse size up to 24576). */
+size_t pyto_workspace_bytes(const pyto_operator_t* op, int kind);
+
+/* ---- element matrices and operator set-up (host only, no GPU work) ------- */
+/* 24x24 Ke of a box hex8, 2x2x2 Gauss, isotropic (E, nu).
+ * Replaces hex_element_stiffness.hex8_stiffness_matrix_structural
+ * (src/hex_element_stiffness.py:232-286). */
+int pyto_ke_hex8(double E, double nu, double hx, double hy, double hz, double* ke_out);
+/* Fill *op.  ke may be NULL (then Ke = pyto_ke_hex8(E, nu, h)); a given Ke must have
+ * the reflection symmetry of a box hex8 or PYTO_ERR_ARG is returned.  Replaces the
+ * Ke / COO-index set-up of HexStructuralFEA.__init__ (src/hex_structural_fea.py:21-52). */
+int pyto_operator_init(pyto_operator_t* op, int32_t nelx, int32_t nely, int32_t nelz,
+                       double hx, double hy, double hz, double E, double nu, const double* ke);
+
+/* ---- material model -------------------------------------------------------- */
+/* s = emin + x^p (1-emin), ds = p x^(p-1) (1-emin) (ds may be NULL); active (may be
+ * NULL) zeroes s and ds of inactive elements.  Replaces
+ * get_structural_material_model_scaling / _sensitivity (src/topopt_material_model.py:76-139). */
+int pyto_simp(const double* x, const uint8_t* active, int64_t n, double penal, double emin,
+              double* s, double* ds, void* stream);
+
+/* ---- boundary conditions ------------------------------------------------------ */
+/* mask[n] bit c set <=> DOF 3n+c is fixed.  mask is cleared first; its pointer must be
+ * 4-byte aligned and the buffer must hold nnodes bytes rounded up to a multiple of 4
+ * (bits are set with 32-bit atomics).  Out-of-range DOF ids are ignored.
+ * Replaces BC.fixed_dofs / free_dofs (src/bound_cond.py:9-37). */
+int pyto_bc_mask(const pyto_operator_t* op, const int64_t* fixed_dofs, int64_t n_fixed,
+                 uint8_t* mask, void* stream);
+
+/* ---- operator application ------------------------------------------------------- */
+/* y = K(s) u, matrix-free, with Dirichlet masking per `mode` (PYTO_MASK_IN|PYTO_MASK_OUT
+ * gives the reduced operator K_ff of impose_dirichlet_bc, src/bound_cond.py:40-70, on
+ * full-length vectors).  If dot is non-NULL, *dot (device) = sum(u_masked . y); this
+ * needs a PYTO_WS_REDUCE workspace.  Replaces the COO assembly + CSR SpMV of
+ * HexStructuralFEA.solve / linear_solvers.solve (src/hex_structural_fea.py:87-102,
+ * src/linear_solvers.py:136-202). */
+int pyto_matvec(const pyto_operator_t* op, const double* s, const uint8_t* mask, const double* u,
+                double* y, int mode, double* dot, void* ws, size_t ws_bytes, void* stream);
+/* Jacobi data: diag(K)[3n+c] = kdiag[c] * sum_{e ni n} s_e.  Writes winv[n] = 1/sum s
+ * and flags[n] = mask bits | (clamp bits << 3), clamp bit c set when |diag| < 1e-12 (then
+ * the preconditioner is 1, src/linear_solvers.py:71-87).  diag_out (may be NULL) gets the
+ * full diagonal [3*nnodes]. */
+int pyto_jacobi(const pyto_operator_t* op, const double* s, const uint8_t* mask, double* winv,
+                uint8_t* flags, double* diag_out, void* stream);
+
+/* ---- solvers -------------------------------------------------------------------- */
+/* Jacobi PCG on the reduced system K_ff u_f = b_f (src/linear_solvers.py:164-168).
+ * b is full length; fixed entries are ignored.  u: solution, fixed entries set to 0. */
+int pyto_pcg_solve(const pyto_operator_t* op, const double* s, const uint8_t* mask, const double* b,
+                   double* u, const pyto_solve_cfg_t* cfg, pyto_solve_status_t* status, void* ws,
+                   size_t ws_bytes, void* stream);
+/* Build (W_f^T K_ff W_f + shift I)^-1 into defl->coarse_inv (dense FP64 sweep inversion on
+ * the GPU).  Replaces the WKW set-up of deflatedPCG_CPU (src/deflation.py:513-521). */
+int pyto_dpcg_setup(const pyto_operator_t* op, const double* s, const uint8_t* mask,
+                    pyto_deflation_t* defl, void* ws, size_t ws_bytes, void* stream);
+/* Deflated PCG (src/deflation.py:504-584): coarse start, p0 = z - W mu, per iteration
+ * one coarse correction; stopping rule per cfg.  Replaces DeflationSolver.deflatedPCG. */
+int pyto_dpcg_solve(const pyto_operator_t* op, const double* s, const uint8_t* mask,
+                    const pyto_deflation_t* defl, const double* b, double* u,
+                    const pyto_solve_cfg_t* cfg, pyto_solve_status_t* status, void* ws,
+                    size_t ws_bytes, void* stream);
+
+/* ---- objectives and sensitivities ------------------------------------------------ */
+/* ce[e] = u_e^T Ke v_e (u == v gives the element energy of compliance).  If s != NULL and
+ * total != NULL, *total (device) = sum_e s_e ce_e (needs PYTO_WS_REDUCE workspace).
+ * Replaces the gather + GEMM of compute_compliance_and_gradient
+ * (src/topopt_obj_cons_sensitivities.py:148-179, :279-282, :308-311). */
+int pyto_elem_energy(const pyto_operator_t* op, const double* u, const double* v, const double* s,
+                     double* ce, double* total, void* ws, size_t ws_bytes, void* stream);
+/* Centroid strain, stress = x^q D eps, von Mises, strain energy 0.5 eps.sigma
+ * (src/hex_structural_fea.py:152-234).  strain/stress [ne*6] and sed may be NULL. */
+int pyto_stress(const pyto_operator_t* op, const double* u, const double* x, double q,
+                double* strain, double* stress, double* vm, double* sed, void* stream);
+/* sum_e vm_e^P into *sum_out (device); needs PYTO_WS_REDUCE workspace. */
+int pyto_pnorm_sum(const pyto_operator_t* op, const double* vm, double P, double* sum_out,
+                   void* ws, size_t ws_bytes, void* stream);
+/* p-norm adjoint pieces (src/topopt_obj_cons_sensitivities.py:238-266): with
+ * dpn = (sum vm^P)^(1/P-1) read from *dpn_dev, T1[e] = dpn q x^(q-1) vm^(P-1) DvmDs.D.B.u_e
+ * and the adjoint load g = sum_e x^q dpn vm^(P-1) B^T D^T DvmDs (node-owned gather,
+ * no atomics).  x is clamped below at 1e-12 as in the reference.  tvec is scratch of
+ * [ne*6] doubles. */
+int pyto_pnorm_adjoint(const pyto_operator_t* op, const double* u, const double* x, double q,
+                       double P, const double* dpn_dev, double* T1, double* g, double* tvec,
+                       void* stream);
+
+/* ---- density filter and OC update ---------------------------------------------- */
+/* Linear hat filter H_ij = (r - d_ij)/r, d_ij <= r, r = rel_radius * hx, applied as a
+ * grid stencil (src/topopt_filters.py:8-38; density filter src/topopt_mma.py:255-258,
+ * chain rule :341-345; OC sensitivity filter src/topopt_ocm.py:239).  hs is needed by
+ * PYTO_FILTER_CHAIN, w by PYTO_FILTER_SENS; both may be NULL otherwise.  active (may be
+ * NULL) restricts H to active elements (inactive outputs are 0). */
+int pyto_filter(const pyto_operator_t* op, double rel_radius, int mode, const double* x,
+                const double* w, const double* hs, const uint8_t* active, double* y, void* stream);
+/* One OC update with bisection on the volume multiplier (src/topopt_ocm.py:244-283),
+ * the same bisection sequence as the reference.  x is updated in place; *change_out
+ * (device) = max |x_new - x_old|.  dc is the filtered objective gradient.  With an active
+ * mask (may be NULL) only its n_active elements are updated and counted in the volume. */
+int pyto_oc_update(const pyto_operator_t* op, double* x, const double* dc, const uint8_t* active,
+                   long long n_active, double volfrac, double move, double xmin, double xmax,
+                   double* change_out, void* ws, size_t ws_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PYTO_B200_H */

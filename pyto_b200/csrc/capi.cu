@@ -1,0 +1,28 @@
+// Workspace sizing of the C ABI.
+#include <algorithm>
+
+#include "krylov.cuh"
+
+namespace pyto {
+size_t pcg_workspace_bytes(const pyto_operator_t* op);
+size_t dpcg_workspace_bytes(const pyto_operator_t* op);
+int oc_grid_blocks();
+}  // namespace pyto
+
+using namespace pyto;
+
+extern "C" size_t pyto_workspace_bytes(const pyto_operator_t* op, int kind) {
+  if (!op) return 0;
+  switch (kind) {
+    case PYTO_WS_REDUCE:
+      return 1024 + 8 * 2 * reduce_slots(op);
+    case PYTO_WS_PCG:
+      return pcg_workspace_bytes(op);
+    case PYTO_WS_DPCG:
+      return dpcg_workspace_bytes(op);
+    case PYTO_WS_OC:
+      return 1024 + 8 * 3 * (size_t)std::max(oc_grid_blocks(), 4 * kNumSMs);
+    default:
+      return 0;
+  }
+}

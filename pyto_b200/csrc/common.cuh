@@ -1,0 +1,146 @@
+// Shared device/host helpers of libpyto_b200 (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/pyto_b200.h"
+
+#define PYTO_CUDA(call)                              \
+  do {                                               \
+    cudaError_t _e = (call);                         \
+    if (_e != cudaSuccess) return PYTO_ERR_CUDA;     \
+  } while (0)
+
+#define PYTO_LAUNCH_CHECK() PYTO_CUDA(cudaGetLastError())
+
+namespace pyto {
+
+constexpr int kNumSMs = 148;        // B200
+constexpr int kReduceBlocks = 1184; // max partial slots of a node-wise reduction (8 per SM)
+
+// Grid geometry passed by value to kernels.
+struct GridDims {
+  int nx, ny, nz;  // elements
+  int sx, sy, sz;  // nodes = elements + 1
+  long long nnodes, nelem;
+};
+
+inline GridDims make_dims(const pyto_operator_t* op) {
+  GridDims g;
+  g.nx = op->nelx; g.ny = op->nely; g.nz = op->nelz;
+  g.sx = g.nx + 1; g.sy = g.ny + 1; g.sz = g.nz + 1;
+  g.nnodes = (long long)g.sx * g.sy * g.sz;
+  g.nelem = (long long)g.nx * g.ny * g.nz;
+  return g;
+}
+
+// Element operator in the Hadamard corner basis, passed as a kernel argument
+// (lands in the constant bank: uniform, broadcast reads).
+struct KHat {
+  double b[8][9];   // class q block, row-major 3x3
+  double kd[3];     // corner diagonal per component
+};
+
+inline KHat make_khat(const pyto_operator_t* op) {
+  KHat k;
+  for (int q = 0; q < 8; ++q)
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) k.b[q][3 * i + j] = op->khat[q][i][j];
+  for (int c = 0; c < 3; ++c) k.kd[c] = op->kdiag[c];
+  return k;
+}
+
+// ---- deterministic block reductions ------------------------------------
+// Sum over a block in a fixed order: warp shuffle tree, then warp 0 over the
+// per-warp partials.  Result valid in thread 0.
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double* smem /*>= NT/32*/) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) smem[wid] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (wid == 0) {
+    r = (lane < NT / 32) ? smem[lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+  }
+  __syncthreads();
+  return r;
+}
+
+template <int NT>
+__device__ __forceinline__ double block_max(double v, double* smem) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) smem[wid] = v;
+  __syncthreads();
+  double r = -1.0e308;
+  if (wid == 0) {
+    r = (lane < NT / 32) ? smem[lane] : -1.0e308;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r = fmax(r, __shfl_down_sync(0xffffffffu, r, o));
+  }
+  __syncthreads();
+  return r;
+}
+
+// Sum of `n` partials in a fixed order by one warp; every lane gets the same
+// bitwise result (xor butterfly), so all blocks that call it agree.
+__device__ __forceinline__ double warp_sum_partials(const double* p, int n) {
+  const int lane = threadIdx.x & 31;
+  double v = 0.0;
+  for (int i = lane; i < n; i += 32) v += __ldcg(p + i);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Cross-block reduction: every block deposits its value(s) (thread 0 holds
+// them), the last block to arrive sums all partials in block order and calls
+// `fin(totals)` in its thread 0.  Deterministic: the summation order does not
+// depend on scheduling.  The counter is reset by the last block, so it can be
+// reused by the next launch on the same stream.
+template <int K, typename Fin>
+__device__ __forceinline__ void grid_reduce(const double (&v)[K], double* part /*[K][nblocks]*/,
+                                            unsigned* counter, int nblocks, Fin fin) {
+  __shared__ bool s_last;
+  const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) part[(size_t)k * nblocks + bid] = v[k];
+    __threadfence();
+    const unsigned t = atomicAdd(counter, 1u);
+    s_last = (t == (unsigned)nblocks - 1u);
+  }
+  __syncthreads();
+  if (s_last && threadIdx.x < 32) {
+    __threadfence();
+    double tot[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) tot[k] = warp_sum_partials(part + (size_t)k * nblocks, nblocks);
+    if (threadIdx.x == 0) {
+      fin(tot);
+      *counter = 0u;
+      __threadfence();
+    }
+  }
+}
+
+// Workspace carving helper (256-byte aligned sub-buffers).
+struct Carver {
+  char* base;
+  size_t off, cap;
+  template <typename T>
+  T* take(size_t count) {
+    off = (off + 255) & ~(size_t)255;
+    T* p = (T*)(base ? base + off : nullptr);
+    off += count * sizeof(T);
+    return p;
+  }
+  bool ok() const { return base != nullptr && off <= cap; }
+};
+
+}  // namespace pyto

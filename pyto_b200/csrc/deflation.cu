@@ -1,0 +1,739 @@
+// Aggregation-deflated PCG (src/deflation.py:386-584) on the GPU.
+//
+// Deflation space W: per node group g, rigid-body modes about the group
+// centre c_g (rel = x - c_g):
+//   mode 0,1,2: translations;  mode 3: (0,-rel_z,rel_y);  mode 4: (rel_z,0,-rel_x);
+//   mode 5: (-rel_y,rel_x,0)                         (src/deflation.py:415-450)
+// W is never stored: restriction W^T v reduces per group over its nodes, and
+// prolongation W mu is evaluated per node from its group's mu and centre.
+//
+// Coarse matrix E = W_f^T K_ff W_f (W rows of fixed DOFs dropped, as
+// W[free_dofs] in src/linear_solvers.py:184).  Rigid modes lie in the null
+// space of every element matrix, so only elements whose corners span two or
+// more groups (or touch a fixed DOF) contribute; each such element adds
+// s_e (Phi M_j)^T K^ (Phi M_i) to block (g_j, g_i) with FP64 atomics.
+//
+// E^-1 is formed explicitly (dense, FP64) by a blocked in-place sweep
+// (Gauss-Jordan on the SPD matrix, 64x64 pivot blocks); each DPCG iteration
+// then applies it with one dense GEMV, which is a single fully parallel pass
+// instead of two latency-bound triangular solves.
+#include <algorithm>
+
+#include "krylov.cuh"
+
+namespace pyto {
+
+constexpr int kSweepB = 64;
+
+__device__ __forceinline__ void node_xyz(const GridDims& g, long long n, double hx, double hy, double hz, double& x,
+                                         double& y, double& z) {
+  const int ix = (int)(n % g.sx);
+  const long long r = n / g.sx;
+  const int iy = (int)(r % g.sy);
+  const int iz = (int)(r / g.sy);
+  x = hx * ix;
+  y = hy * iy;
+  z = hz * iz;
+}
+
+// mode vector (3 components) of mode a at relative position rel
+__device__ __forceinline__ void rigid_mode(int a, double rx, double ry, double rz, double (&w)[3]) {
+  w[0] = w[1] = w[2] = 0.0;
+  switch (a) {
+    case 0: w[0] = 1.0; break;
+    case 1: w[1] = 1.0; break;
+    case 2: w[2] = 1.0; break;
+    case 3: w[1] = -rz; w[2] = ry; break;
+    case 4: w[0] = rz; w[2] = -rx; break;
+    default: w[0] = -ry; w[1] = rx; break;
+  }
+}
+
+struct DeflP {
+  double hx, hy, hz;
+  int modes, ngroups;
+  long long nc;
+};
+
+// Hadamard transform of the restriction of mode a of group G to the element's
+// corners (zero at corners of other groups and at fixed DOFs)
+__device__ __forceinline__ void mode_hat(const GridDims& g, const DeflP& dp, const long long (&nd)[8],
+                                         const int (&gr)[8], const int (&mk)[8], int G, const double* __restrict__ gc,
+                                         int a, double (&H)[3][8]) {
+  double A[3][8];
+  for (int k = 0; k < 8; ++k) {
+    double w[3] = {0.0, 0.0, 0.0};
+    if (gr[k] == G) {
+      double x, y, z;
+      node_xyz(g, nd[k], dp.hx, dp.hy, dp.hz, x, y, z);
+      const double* c = gc + 3 * (long long)G;
+      rigid_mode(a, x - c[0], y - c[1], z - c[2], w);
+    }
+    for (int c = 0; c < 3; ++c) A[c][k] = ((mk[k] >> c) & 1) ? 0.0 : w[c];
+  }
+  for (int c = 0; c < 3; ++c) {
+    double Fb[4], Ft[4];
+    face_fwd(A[c][0], A[c][1], A[c][2], A[c][3], Fb);
+    face_fwd(A[c][4], A[c][5], A[c][6], A[c][7], Ft);
+    for (int f = 0; f < 4; ++f) {
+      H[c][f] = Ft[f] + Fb[f];
+      H[c][f + 4] = Ft[f] - Fb[f];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// coarse matrix assembly
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_coarse_assemble(GridDims g, KHat kh, DeflP dp, const double* __restrict__ s,
+                                                         const uint8_t* __restrict__ mask,
+                                                         const int32_t* __restrict__ ngrp,
+                                                         const double* __restrict__ gc, double* __restrict__ E) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < g.nelem;
+       e += (long long)gridDim.x * blockDim.x) {
+    const double se = s[e];
+    if (se == 0.0) continue;
+    const int ex = (int)(e % g.nx);
+    const long long rr = e / g.nx;
+    const int ey = (int)(rr % g.ny);
+    const int ez = (int)(rr / g.ny);
+    long long nd[8];
+    int gr[8], mk[8];
+    bool need = false;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int bx = k & 1, by = (k >> 1) & 1, bz = k >> 2;
+      nd[k] = (ex + bx) + (long long)g.sx * ((ey + by) + (long long)g.sy * (ez + bz));
+      gr[k] = ngrp[nd[k]];
+      mk[k] = mask ? (mask[nd[k]] & 7) : 0;
+      if (mk[k] || gr[k] != gr[0]) need = true;
+    }
+    if (!need) continue;
+    int G[8], ng = 0;
+    for (int k = 0; k < 8; ++k) {
+      bool seen = false;
+      for (int t = 0; t < ng; ++t) seen |= (G[t] == gr[k]);
+      if (!seen) G[ng++] = gr[k];
+    }
+    for (int i = 0; i < ng; ++i) {
+      // Z_i[b] = s K^ Phi M_i[b]
+      double Zi[6][3][8];
+      for (int b = 0; b < dp.modes; ++b) {
+        double H[3][8];
+        mode_hat(g, dp, nd, gr, mk, G[i], gc, b, H);
+        for (int c = 0; c < 3; ++c)
+          for (int m = 0; m < 8; ++m) Zi[b][c][m] = 0.0;
+        for (int q = 0; q < 8; ++q)
+          for (int c = 0; c < 3; ++c) {
+            const int m = member_mode(q, c);
+            if (m == 0) continue;
+            double o = 0.0;
+            for (int d = 0; d < 3; ++d) {
+              const int n = member_mode(q, d);
+              if (n == 0) continue;
+              o = fma(kh.b[q][3 * c + d], H[d][n], o);
+            }
+            Zi[b][c][m] = se * o;
+          }
+      }
+      for (int j = 0; j < ng; ++j) {
+        for (int a = 0; a < dp.modes; ++a) {
+          double H[3][8];
+          mode_hat(g, dp, nd, gr, mk, G[j], gc, a, H);
+          const long long row = (long long)G[j] * dp.modes + a;
+          for (int b = 0; b < dp.modes; ++b) {
+            double v = 0.0;
+            for (int c = 0; c < 3; ++c)
+              for (int m = 1; m < 8; ++m) v = fma(H[c][m], Zi[b][c][m], v);
+            if (v != 0.0) atomicAdd(E + row * dp.nc + (long long)G[i] * dp.modes + b, v);
+          }
+        }
+      }
+    }
+  }
+}
+
+// mean |diag(E)| (one block) -> *out
+__global__ void k_diag_mean(long long nc, const double* __restrict__ E, double* out) {
+  __shared__ double sred[8];
+  double acc = 0.0;
+  for (long long i = threadIdx.x; i < nc; i += blockDim.x) acc += fabs(E[i * nc + i]);
+  const double t = block_sum<256>(acc, sred);
+  if (threadIdx.x == 0) *out = t / (double)nc;
+}
+
+// (E + E^T)/2, zero rows -> identity, diagonal shift (relative: times mean |diag|)
+__global__ void k_coarse_finish(long long nc, double* E, double shift, const double* mean_diag) {
+  const double sh = mean_diag ? shift * (*mean_diag) : shift;
+  for (long long i = blockIdx.x; i < nc; i += gridDim.x) {
+    for (long long j = threadIdx.x; j < i; j += blockDim.x) {
+      const double a = 0.5 * (E[i * nc + j] + E[j * nc + i]);
+      E[i * nc + j] = a;
+      E[j * nc + i] = a;
+    }
+    if (threadIdx.x == 0) {
+      double d = E[i * nc + i];
+      if (d == 0.0) d = 1.0;  // column of W that vanishes on the free DOFs
+      E[i * nc + i] = d + sh;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// blocked sweep inversion: after all pivot blocks A = -E^-1
+//   P = A_KK^-1, U = P A_K:, A_ij -= A_iK U_Kj, A_Kj = U_Kj, A_iK = U_Ki^T, A_KK = -P
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_sweep_pivot(long long n, int k0, int bk, const double* __restrict__ A,
+                                                     double* __restrict__ P) {
+  __shared__ double M[kSweepB][kSweepB + 1];
+  for (int t = threadIdx.x; t < kSweepB * kSweepB; t += blockDim.x) {
+    const int i = t / kSweepB, j = t % kSweepB;
+    M[i][j] = (i < bk && j < bk) ? A[(k0 + i) * n + (k0 + j)] : (i == j ? 1.0 : 0.0);
+  }
+  __syncthreads();
+  // in-place sweep of the small block: result -M^-1
+  for (int p = 0; p < bk; ++p) {
+    const double piv = M[p][p];
+    __syncthreads();
+    for (int t = threadIdx.x; t < kSweepB * kSweepB; t += blockDim.x) {
+      const int i = t / kSweepB, j = t % kSweepB;
+      if (i == p || j == p) continue;
+      M[i][j] -= M[i][p] * M[p][j] / piv;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < kSweepB; t += blockDim.x) {
+      if (t != p) {
+        M[t][p] = M[t][p] / piv;
+        M[p][t] = M[p][t] / piv;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) M[p][p] = -1.0 / piv;
+    __syncthreads();
+  }
+  for (int t = threadIdx.x; t < kSweepB * kSweepB; t += blockDim.x) {
+    const int i = t / kSweepB, j = t % kSweepB;
+    P[t] = -M[i][j];  // P = A_KK^-1
+  }
+}
+
+// Rp = A_K: (copy), U = P Rp   (16 columns per block)
+__global__ void __launch_bounds__(256) k_sweep_panel(long long n, int k0, int bk, const double* __restrict__ A,
+                                                     const double* __restrict__ P, double* __restrict__ Rp,
+                                                     double* __restrict__ U) {
+  __shared__ double sP[kSweepB][kSweepB];
+  __shared__ double sR[kSweepB][17];
+  for (int t = threadIdx.x; t < kSweepB * kSweepB; t += blockDim.x) sP[t / kSweepB][t % kSweepB] = P[t];
+  const long long j0 = (long long)blockIdx.x * 16;
+  for (int t = threadIdx.x; t < kSweepB * 16; t += blockDim.x) {
+    const int i = t / 16, jj = t % 16;
+    const long long j = j0 + jj;
+    double v = 0.0;
+    if (i < bk && j < n) v = A[(k0 + i) * n + j];
+    sR[i][jj] = v;
+    if (i < bk && j < n) Rp[i * n + j] = v;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < kSweepB * 16; t += blockDim.x) {
+    const int i = t / 16, jj = t % 16;
+    const long long j = j0 + jj;
+    if (i >= bk || j >= n) continue;
+    double acc = 0.0;
+    for (int k = 0; k < bk; ++k) acc = fma(sP[i][k], sR[k][jj], acc);
+    U[i * n + j] = acc;
+  }
+}
+
+// tile update, 64x64 tiles, 256 threads x (4x4) outputs, k in chunks of 32
+__global__ void __launch_bounds__(256) k_sweep_update(long long n, int k0, int bk, double* __restrict__ A,
+                                                      const double* __restrict__ P, const double* __restrict__ Rp,
+                                                      const double* __restrict__ U) {
+  __shared__ double sL[32][65];  // A_iK for the tile rows: Rp[k][i]
+  __shared__ double sU[32][65];  // U_Kj for the tile cols
+  const long long i0 = (long long)blockIdx.y * 64, j0 = (long long)blockIdx.x * 64;
+  const bool rowK = (i0 == k0), colK = (j0 == k0);
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  if (rowK || colK) {
+    for (int t = threadIdx.x; t < 64 * 64; t += blockDim.x) {
+      const int ii = t / 64, jj = t % 64;
+      const long long i = i0 + ii, j = j0 + jj;
+      if (i >= n || j >= n) continue;
+      double v;
+      if (rowK && colK) v = (ii < bk && jj < bk) ? -P[ii * kSweepB + jj] : A[i * n + j];
+      else if (rowK) v = (ii < bk) ? U[ii * n + j] : A[i * n + j];
+      else v = (jj < bk) ? U[jj * n + i] : A[i * n + j];
+      A[i * n + j] = v;
+    }
+    return;
+  }
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  for (int kc = 0; kc < bk; kc += 32) {
+    __syncthreads();
+    for (int t = threadIdx.x; t < 32 * 64; t += blockDim.x) {
+      const int k = t / 64, c = t % 64;
+      const bool kin = kc + k < bk;
+      sL[k][c] = (kin && i0 + c < n) ? Rp[(kc + k) * n + i0 + c] : 0.0;
+      sU[k][c] = (kin && j0 + c < n) ? U[(kc + k) * n + j0 + c] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int k = 0; k < 32; ++k) {
+      double l[4], u[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) l[a] = sL[k][ty + 16 * a];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) u[b] = sU[k][tx + 16 * b];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = fma(l[a], u[b], acc[a][b]);
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const long long i = i0 + ty + 16 * a, j = j0 + tx + 16 * b;
+      if (i < n && j < n) A[i * n + j] -= acc[a][b];
+    }
+}
+
+__global__ void k_negate(long long n, double* A) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    A[i] = -A[i];
+}
+
+// ---------------------------------------------------------------------------
+// DPCG pieces
+// ---------------------------------------------------------------------------
+// v = W_f^T y (one warp per group, nodes in CSR order -> deterministic)
+__global__ void __launch_bounds__(256) k_restrict(GridDims g, DeflP dp, const int32_t* __restrict__ gptr,
+                                                  const int32_t* __restrict__ gnodes, const double* __restrict__ gc,
+                                                  const uint8_t* __restrict__ fl, const double* __restrict__ y,
+                                                  double* __restrict__ v) {
+  const int lane = threadIdx.x & 31;
+  const long long grp = (long long)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  if (grp >= dp.ngroups) return;
+  const double cx = gc[3 * grp], cy = gc[3 * grp + 1], cz = gc[3 * grp + 2];
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (int t = gptr[grp] + lane; t < gptr[grp + 1]; t += 32) {
+    const long long n = gnodes[t];
+    double x, yy, z;
+    node_xyz(g, n, dp.hx, dp.hy, dp.hz, x, yy, z);
+    const double rx = x - cx, ry = yy - cy, rz = z - cz;
+    const int f = fl[n];
+    const double vx = (f & 1) ? 0.0 : y[3 * n], vy = (f & 2) ? 0.0 : y[3 * n + 1], vz = (f & 4) ? 0.0 : y[3 * n + 2];
+    acc[0] += vx;
+    acc[1] += vy;
+    acc[2] += vz;
+    acc[3] += -rz * vy + ry * vz;
+    acc[4] += rz * vx - rx * vz;
+    acc[5] += -ry * vx + rx * vy;
+  }
+#pragma unroll
+  for (int a = 0; a < 6; ++a)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc[a] += __shfl_xor_sync(0xffffffffu, acc[a], o);
+  if (lane == 0)
+    for (int a = 0; a < dp.modes; ++a) v[grp * dp.modes + a] = acc[a];
+}
+
+// mu = Einv v (one warp per row, v staged in shared memory)
+__global__ void __launch_bounds__(256) k_coarse_gemv(long long nc, const double* __restrict__ Einv,
+                                                     const double* __restrict__ v, double* __restrict__ mu,
+                                                     const KrylovState* S) {
+  extern __shared__ double sv[];
+  if (S && S->done) return;
+  for (long long i = threadIdx.x; i < nc; i += blockDim.x) sv[i] = v[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  for (long long row = (long long)blockIdx.x * 8 + (threadIdx.x >> 5); row < nc; row += (long long)gridDim.x * 8) {
+    const double* a = Einv + row * nc;
+    double acc = 0.0;
+    for (long long j = lane; j < nc; j += 32) acc = fma(__ldg(a + j), sv[j], acc);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) mu[row] = acc;
+  }
+}
+
+// prolongation term of node n: (W mu) at its 3 DOFs
+__device__ __forceinline__ void prolong_node(const GridDims& g, const DeflP& dp, long long n,
+                                             const int32_t* __restrict__ ngrp, const double* __restrict__ gc,
+                                             const double* __restrict__ mu, double (&w)[3]) {
+  const int grp = ngrp[n];
+  double x, y, z;
+  node_xyz(g, n, dp.hx, dp.hy, dp.hz, x, y, z);
+  const double* c = gc + 3 * (long long)grp;
+  const double rx = x - c[0], ry = y - c[1], rz = z - c[2];
+  const double* m = mu + (long long)grp * dp.modes;
+  w[0] = m[0];
+  w[1] = m[1];
+  w[2] = m[2];
+  if (dp.modes == 6) {
+    w[0] += rz * m[4] - ry * m[5];
+    w[1] += -rz * m[3] + rx * m[5];
+    w[2] += ry * m[3] - rx * m[4];
+  }
+}
+
+// x = W mu (masked)
+__global__ void __launch_bounds__(256) k_prolong(GridDims g, DeflP dp, const int32_t* __restrict__ ngrp,
+                                                 const double* __restrict__ gc, const double* __restrict__ mu,
+                                                 const uint8_t* __restrict__ fl, double* __restrict__ x) {
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < g.nnodes;
+       n += (long long)gridDim.x * blockDim.x) {
+    double w[3];
+    prolong_node(g, dp, n, ngrp, gc, mu, w);
+    const int f = fl[n];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) x[3 * n + c] = ((f >> c) & 1) ? 0.0 : w[c];
+  }
+}
+
+// r = b - t (masked), z = M^-1 r; reductions r.z, r.r, b.b
+__global__ void __launch_bounds__(kNodeThreads) k_dpcg_init(GridDims g, Prec pc, const double* __restrict__ b,
+                                                            const double* __restrict__ t, const double* __restrict__ w,
+                                                            const uint8_t* __restrict__ fl, double* __restrict__ r,
+                                                            double* __restrict__ z, KrylovState* S, double* part,
+                                                            unsigned* counter) {
+  __shared__ double sred[kNodeThreads / 32];
+  double rz = 0.0, rr = 0.0, bb = 0.0;
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < g.nnodes;
+       n += (long long)gridDim.x * blockDim.x) {
+    const int f = fl[n];
+    const double wn = w[n];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const long long i = 3 * n + c;
+      const bool fixed = (f >> c) & 1;
+      const double bi = fixed ? 0.0 : b[i];
+      const double ri = fixed ? 0.0 : bi - t[i];
+      const double zi = jacobi_apply(ri, f, c, wn, pc);
+      r[i] = ri;
+      z[i] = zi;
+      rz = fma(ri, zi, rz);
+      rr = fma(ri, ri, rr);
+      bb = fma(bi, bi, bb);
+    }
+  }
+  double v[3];
+  v[0] = block_sum<kNodeThreads>(rz, sred);
+  v[1] = block_sum<kNodeThreads>(rr, sred);
+  v[2] = block_sum<kNodeThreads>(bb, sred);
+  grid_reduce<3>(v, part, counter, gridDim.x, [&](const double* tot) {
+    S->rz = tot[0];
+    S->rz0 = tot[0];
+    S->rr = tot[1];
+    S->bb = tot[2];
+    if (tot[2] == 0.0 || (S->stop_rule == 0 && sqrt(tot[1]) < S->rtol * sqrt(tot[2]))) {
+      S->done = 1;
+      S->converged = 1;
+    }
+  });
+}
+
+// x += a p, r -= a q, z = M^-1 r (stored), reductions -> beta, convergence
+__global__ void __launch_bounds__(kNodeThreads) k_dpcg_update1(GridDims g, Prec pc, const double* __restrict__ w,
+                                                               const uint8_t* __restrict__ fl,
+                                                               double* __restrict__ x, double* __restrict__ r,
+                                                               double* __restrict__ z, const double* __restrict__ p,
+                                                               const double* __restrict__ q, KrylovState* S,
+                                                               double* part, unsigned* counter) {
+  __shared__ double sred[kNodeThreads / 32];
+  if (S->done) return;
+  const double pq = S->pq, rz = S->rz;
+  const double alpha = rz / pq;
+  if (!(pq > 0.0) || !isfinite(alpha)) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      S->breakdown = 1;
+      S->done = 1;
+    }
+    return;
+  }
+  double rr = 0.0, rzn = 0.0;
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < g.nnodes;
+       n += (long long)gridDim.x * blockDim.x) {
+    const int f = fl[n];
+    const double wn = w[n];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const long long i = 3 * n + c;
+      x[i] = fma(alpha, p[i], x[i]);
+      const double ri = fma(-alpha, q[i], r[i]);
+      r[i] = ri;
+      const double zi = jacobi_apply(ri, f, c, wn, pc);
+      z[i] = zi;
+      rr = fma(ri, ri, rr);
+      rzn = fma(ri, zi, rzn);
+    }
+  }
+  double v[2];
+  v[0] = block_sum<kNodeThreads>(rr, sred);
+  v[1] = block_sum<kNodeThreads>(rzn, sred);
+  grid_reduce<2>(v, part, counter, gridDim.x, [&](const double* tot) {
+    S->alpha = alpha;
+    S->iters += 1;
+    S->rr = tot[0];
+    const double rz_new = tot[1];
+    if (!isfinite(tot[0]) || !isfinite(rz_new)) {
+      S->breakdown = 1;
+      S->done = 1;
+    } else if (krylov_converged(*S, tot[0], rz_new)) {
+      S->converged = 1;
+      S->done = 1;
+    } else if (S->iters >= S->max_iters) {
+      S->done = 1;
+    }
+    S->beta = rz_new / S->rz;
+    S->rz = rz_new;
+  });
+}
+
+// p = z + beta p - W mu  (beta = 0 for the start vector)
+__global__ void __launch_bounds__(kNodeThreads) k_dpcg_update2(GridDims g, DeflP dp, const int32_t* __restrict__ ngrp,
+                                                               const double* __restrict__ gc,
+                                                               const double* __restrict__ mu,
+                                                               const uint8_t* __restrict__ fl,
+                                                               const double* __restrict__ z, double* __restrict__ p,
+                                                               const KrylovState* S, int first) {
+  if (!first && S->done) return;
+  const double beta = first ? 0.0 : S->beta;
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < g.nnodes;
+       n += (long long)gridDim.x * blockDim.x) {
+    double w[3];
+    prolong_node(g, dp, n, ngrp, gc, mu, w);
+    const int f = fl[n];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const long long i = 3 * n + c;
+      const double pi = first ? 0.0 : p[i];
+      p[i] = ((f >> c) & 1) ? 0.0 : fma(beta, pi, z[i]) - w[c];
+    }
+  }
+}
+
+__global__ void k_state_init2(KrylovState* S, double rtol, int max_iters, int stop_rule) {
+  KrylovState z{};
+  z.rtol = rtol;
+  z.max_iters = max_iters;
+  z.stop_rule = stop_rule;
+  *S = z;
+}
+
+__global__ void __launch_bounds__(kNodeThreads) k_true_residual2(GridDims g, const double* __restrict__ b,
+                                                                 const double* __restrict__ t,
+                                                                 const uint8_t* __restrict__ fl, KrylovState* S,
+                                                                 double* part, unsigned* counter) {
+  __shared__ double sred[kNodeThreads / 32];
+  double rr = 0.0, bb = 0.0;
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < g.nnodes;
+       n += (long long)gridDim.x * blockDim.x) {
+    const int f = fl[n];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      if ((f >> c) & 1) continue;
+      const double bi = b[3 * n + c];
+      const double d = bi - t[3 * n + c];
+      rr = fma(d, d, rr);
+      bb = fma(bi, bi, bb);
+    }
+  }
+  double v[2] = {block_sum<kNodeThreads>(rr, sred), block_sum<kNodeThreads>(bb, sred)};
+  grid_reduce<2>(v, part, counter, gridDim.x, [&](const double* tot) {
+    S->true_rr = tot[0];
+    S->bb = tot[1];
+  });
+}
+
+struct DpcgWs {
+  KrylovState* S;
+  unsigned* counter;
+  double* part;
+  double *r, *p, *q, *z, *w;
+  uint8_t* fl;
+  double *cv, *mu;     // coarse vectors
+  double *P, *Rp, *U;  // sweep scratch
+};
+
+constexpr long long kMaxCoarse = 24576;  // coarse vector staged in shared memory (192 KB)
+
+static DpcgWs carve_dpcg(const pyto_operator_t* op, long long nc, void* ws, size_t bytes, size_t* need) {
+  const GridDims g = make_dims(op);
+  Carver cv{(char*)ws, 0, bytes};
+  DpcgWs W;
+  W.S = cv.take<KrylovState>(1);
+  W.counter = cv.take<unsigned>(64);
+  W.part = cv.take<double>(4 * reduce_slots(op));
+  W.r = cv.take<double>(3 * g.nnodes);
+  W.p = cv.take<double>(3 * g.nnodes);
+  W.q = cv.take<double>(3 * g.nnodes);
+  W.z = cv.take<double>(3 * g.nnodes);
+  W.w = cv.take<double>(g.nnodes);
+  W.fl = cv.take<uint8_t>(g.nnodes);
+  W.cv = cv.take<double>(nc > 0 ? nc : 1);
+  W.mu = cv.take<double>(nc > 0 ? nc : 1);
+  W.P = cv.take<double>(kSweepB * kSweepB);
+  W.Rp = cv.take<double>(kSweepB * (nc > 0 ? nc : 1));
+  W.U = cv.take<double>(kSweepB * (nc > 0 ? nc : 1));
+  *need = cv.off + 256;
+  return W;
+}
+
+size_t dpcg_workspace_bytes(const pyto_operator_t* op) {
+  size_t need = 0;
+  carve_dpcg(op, kMaxCoarse, nullptr, 0, &need);
+  return need;
+}
+
+static DeflP make_deflp(const pyto_operator_t* op, const pyto_deflation_t* d) {
+  DeflP dp;
+  dp.hx = op->hx;
+  dp.hy = op->hy;
+  dp.hz = op->hz;
+  dp.modes = d->modes;
+  dp.ngroups = d->ngroups;
+  dp.nc = (long long)d->ngroups * d->modes;
+  return dp;
+}
+
+static bool defl_ok(const pyto_deflation_t* d) {
+  return d && d->ngroups > 0 && (d->modes == 3 || d->modes == 6) && d->node_group && d->group_ptr &&
+         d->group_nodes && d->group_center && d->coarse_inv;
+}
+
+// mu = Einv W_f^T y
+static int coarse_solve(const GridDims& g, const DeflP& dp, const pyto_deflation_t* d, const double* y,
+                        const DpcgWs& W, const KrylovState* S, cudaStream_t st) {
+  k_restrict<<<(dp.ngroups + 7) / 8, 256, 0, st>>>(g, dp, d->group_ptr, d->group_nodes, d->group_center, W.fl, y,
+                                                   W.cv);
+  const size_t shm = (size_t)dp.nc * sizeof(double);
+  const int nb = (int)std::min<long long>((dp.nc + 7) / 8, 4 * kNumSMs);
+  k_coarse_gemv<<<nb, 256, shm, st>>>(dp.nc, d->coarse_inv, W.cv, W.mu, S);
+  PYTO_LAUNCH_CHECK();
+  return PYTO_OK;
+}
+
+static int gemv_smem_ok(long long nc) {
+  static bool done = false;
+  if (!done) {
+    if (cudaFuncSetAttribute(k_coarse_gemv, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(kMaxCoarse * sizeof(double))) != cudaSuccess)
+      return PYTO_ERR_CUDA;
+    done = true;
+  }
+  return nc <= kMaxCoarse ? PYTO_OK : PYTO_ERR_TOO_LARGE;
+}
+
+}  // namespace pyto
+
+using namespace pyto;
+
+extern "C" int pyto_dpcg_setup(const pyto_operator_t* op, const double* s, const uint8_t* mask,
+                               pyto_deflation_t* defl, void* ws, size_t ws_bytes, void* stream) {
+  if (!op || !s || !defl_ok(defl)) return PYTO_ERR_ARG;
+  const DeflP dp = make_deflp(op, defl);
+  if (dp.nc > kMaxCoarse) return PYTO_ERR_TOO_LARGE;
+  size_t need = 0;
+  DpcgWs W = carve_dpcg(op, dp.nc, ws, ws_bytes, &need);
+  if (!ws || ws_bytes < need) return PYTO_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  const GridDims g = make_dims(op);
+  double* E = defl->coarse_inv;
+  const long long n = dp.nc;
+  PYTO_CUDA(cudaMemsetAsync(E, 0, (size_t)n * n * sizeof(double), st));
+  k_coarse_assemble<<<(int)std::min<long long>((g.nelem + 127) / 128, 16 * kNumSMs), 128, 0, st>>>(
+      g, make_khat(op), dp, s, mask, defl->node_group, defl->group_center, E);
+  if (defl->shift_relative) k_diag_mean<<<1, 256, 0, st>>>(n, E, W.part);
+  k_coarse_finish<<<(int)std::min<long long>(n, 4 * kNumSMs), 256, 0, st>>>(
+      n, E, defl->shift, defl->shift_relative ? W.part : nullptr);
+  PYTO_LAUNCH_CHECK();
+  const int tiles = (int)((n + 63) / 64);
+  for (long long k0 = 0; k0 < n; k0 += kSweepB) {
+    const int bk = (int)std::min<long long>(kSweepB, n - k0);
+    k_sweep_pivot<<<1, 256, 0, st>>>(n, (int)k0, bk, E, W.P);
+    k_sweep_panel<<<(int)((n + 15) / 16), 256, 0, st>>>(n, (int)k0, bk, E, W.P, W.Rp, W.U);
+    k_sweep_update<<<dim3(tiles, tiles), 256, 0, st>>>(n, (int)k0, bk, E, W.P, W.Rp, W.U);
+  }
+  k_negate<<<(int)std::min<long long>((n * n + 255) / 256, 8 * kNumSMs), 256, 0, st>>>(n * n, E);
+  PYTO_LAUNCH_CHECK();
+  return PYTO_OK;
+}
+
+extern "C" int pyto_dpcg_solve(const pyto_operator_t* op, const double* s, const uint8_t* mask,
+                               const pyto_deflation_t* defl, const double* b, double* u, const pyto_solve_cfg_t* cfg,
+                               pyto_solve_status_t* status, void* ws, size_t ws_bytes, void* stream) {
+  if (!op || !s || !b || !u || !cfg || !status || !defl_ok(defl)) return PYTO_ERR_ARG;
+  if (!(cfg->rtol >= 0.0) || cfg->max_iters < 0 || cfg->stop_rule < 0 || cfg->stop_rule > 1) return PYTO_ERR_ARG;
+  const DeflP dp = make_deflp(op, defl);
+  int rc = gemv_smem_ok(dp.nc);
+  if (rc) return rc;
+  size_t need = 0;
+  DpcgWs W = carve_dpcg(op, dp.nc, ws, ws_bytes, &need);
+  if (!ws || ws_bytes < need) return PYTO_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  const GridDims g = make_dims(op);
+  const Prec pc = make_prec(op);
+  const int mm = PYTO_MASK_IN | PYTO_MASK_OUT;
+  PYTO_CUDA(cudaMemsetAsync(W.counter, 0, 64 * sizeof(unsigned), st));
+  k_state_init2<<<1, 1, 0, st>>>(W.S, cfg->rtol, cfg->max_iters, cfg->stop_rule);
+  rc = pyto_jacobi(op, s, mask, W.w, W.fl, nullptr, stream);
+  if (rc) return rc;
+  // coarse start: x = W Einv W_f^T b   (src/deflation.py:532-537)
+  rc = coarse_solve(g, dp, defl, b, W, nullptr, st);
+  if (rc) return rc;
+  k_prolong<<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center, W.mu, W.fl, u);
+  // r = b - K x, z = M r
+  rc = launch_matvec64(op, s, mask, u, W.q, mm, nullptr, nullptr, nullptr, st);
+  if (rc) return rc;
+  k_dpcg_init<<<kNodeBlocks, kNodeThreads, 0, st>>>(g, pc, b, W.q, W.w, W.fl, W.r, W.z, W.S, W.part, W.counter);
+  // p0 = z - W Einv W^T K z
+  rc = launch_matvec64(op, s, mask, W.z, W.q, mm, nullptr, nullptr, nullptr, st);
+  if (rc) return rc;
+  rc = coarse_solve(g, dp, defl, W.q, W, nullptr, st);
+  if (rc) return rc;
+  k_dpcg_update2<<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center, W.mu, W.fl, W.z,
+                                                       W.p, W.S, 1);
+  PYTO_LAUNCH_CHECK();
+  const int every = std::max(1, cfg->check_every);
+  KrylovState hs{};
+  PYTO_CUDA(cudaMemcpyAsync(&hs, W.S, sizeof(hs), cudaMemcpyDeviceToHost, st));
+  PYTO_CUDA(cudaStreamSynchronize(st));
+  while (!hs.done && hs.iters < cfg->max_iters) {
+    for (int k = 0; k < every; ++k) {
+      rc = launch_matvec64(op, s, mask, W.p, W.q, mm, W.part, W.counter, &W.S->pq, st);
+      if (rc) return rc;
+      k_dpcg_update1<<<kNodeBlocks, kNodeThreads, 0, st>>>(g, pc, W.w, W.fl, u, W.r, W.z, W.p, W.q, W.S, W.part,
+                                                           W.counter);
+      // K z -> q (q is free again), mu = Einv W^T K z, p = z + beta p - W mu
+      rc = launch_matvec64(op, s, mask, W.z, W.q, mm, nullptr, nullptr, nullptr, st);
+      if (rc) return rc;
+      rc = coarse_solve(g, dp, defl, W.q, W, W.S, st);
+      if (rc) return rc;
+      k_dpcg_update2<<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center, W.mu, W.fl,
+                                                           W.z, W.p, W.S, 0);
+    }
+    PYTO_LAUNCH_CHECK();
+    PYTO_CUDA(cudaMemcpyAsync(&hs, W.S, sizeof(hs), cudaMemcpyDeviceToHost, st));
+    PYTO_CUDA(cudaStreamSynchronize(st));
+  }
+  const KrylovState before = hs;
+  rc = launch_matvec64(op, s, mask, u, W.q, mm, nullptr, nullptr, nullptr, st);
+  if (rc) return rc;
+  k_true_residual2<<<kNodeBlocks, kNodeThreads, 0, st>>>(g, b, W.q, W.fl, W.S, W.part, W.counter);
+  PYTO_LAUNCH_CHECK();
+  PYTO_CUDA(cudaMemcpyAsync(&hs, W.S, sizeof(hs), cudaMemcpyDeviceToHost, st));
+  PYTO_CUDA(cudaStreamSynchronize(st));
+  status->converged = hs.converged;
+  status->iters = hs.iters;
+  status->breakdown = hs.breakdown;
+  status->rel_res = hs.stop_rule == 0 ? (before.bb > 0 ? sqrt(before.rr / before.bb) : 0.0)
+                                      : (before.rz0 > 0 ? sqrt(before.rz / before.rz0) : 0.0);
+  status->true_rel_res = hs.bb > 0 ? sqrt(hs.true_rr / hs.bb) : 0.0;
+  if (hs.breakdown) return PYTO_ERR_BREAKDOWN;
+  return hs.converged ? PYTO_OK : PYTO_NOT_CONVERGED;
+}

@@ -1,0 +1,133 @@
+// FP64 matrix-free hex8 operator: shared between the plain matvec entry point
+// and the fused Krylov kernels.
+//
+// Work decomposition.  A CTA owns a box of (TX-1) x (TY-1) node columns and a
+// slab of node planes [Z0, Z1).  Its TX x TY threads each own one *element
+// column* (ex, ey) = (X0-1+tx, Y0-1+ty) and march up the element layers
+// ez = Z0-1 .. Z1-1.  Elements of the one-element halo are recomputed by the
+// neighbouring CTAs, so every node's sum is formed by exactly one thread and
+// no atomics are needed (results are bitwise reproducible).
+//
+// Per element, in the Hadamard corner basis (see element.cu):
+//   face transform of the new top face (8 add/comp), z-combination with the
+//   bottom face kept in registers from the previous layer, 57 FMAs of the
+//   block operator scaled by s_e, inverse z-split into bottom/top face
+//   contributions; a face is inverse-transformed once after both elements
+//   that share it were accumulated.  Node contributions of the 4 columns
+//   around a vertical node line are combined with one shuffle (x) and one
+//   shared-memory exchange (y).
+//
+// Node planes are staged in shared memory (SoA, double-buffered) with flat,
+// fully coalesced loads; the next plane and the next s_e are prefetched into
+// registers one layer ahead.
+#pragma once
+#include "common.cuh"
+
+namespace pyto {
+
+template <int TX, int TY>
+struct MvTile {
+  static_assert(TX == 32, "x-combine uses warp shuffles: one warp per row");
+  static constexpr int NT = TX * TY;
+  static constexpr int PX = TX + 1, PY = TY + 1;
+  static constexpr int PLANE = PX * PY;
+  static constexpr int PLANE_D = 3 * PLANE;
+  static constexpr int LOADS = (PLANE_D + NT - 1) / NT;
+};
+
+// Mode of component c in parity class q (the pair (c, q ^ (1<<c))).
+__host__ __device__ constexpr int member_mode(int q, int c) { return q ^ (1 << c); }
+
+// Element core in the Hadamard basis.  Fb/Ft: face transforms of bottom/top
+// faces, [comp][face mode].  Adds the bottom-face part of s*K^u to Gb and the
+// top-face part to Gt.
+template <typename T>
+__device__ __forceinline__ void hex8_core(const KHat& kh, T s, const T (&Fb)[3][4], const T (&Ft)[3][4],
+                                          T (&Gb)[3][4], T (&Gt)[3][4]) {
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    T v[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const int m = member_mode(q, d);
+      const int f = m & 3;
+      if (m == 0) {
+        v[d] = T(0);
+      } else if (m & 4) {
+        v[d] = s * (Ft[d][f] - Fb[d][f]);
+      } else {
+        v[d] = s * (Ft[d][f] + Fb[d][f]);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int m = member_mode(q, c);
+      if (m == 0) continue;
+      const int f = m & 3;
+      T o = T(0);
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        if (member_mode(q, d) == 0) continue;
+        o = fma((T)kh.b[q][3 * c + d], v[d], o);
+      }
+      if (m & 4) {
+        Gb[c][f] -= o;
+        Gt[c][f] += o;
+      } else {
+        Gb[c][f] += o;
+        Gt[c][f] += o;
+      }
+    }
+  }
+}
+
+// 2-D Hadamard transform of a face's 4 corner values (a_xy).
+template <typename T>
+__device__ __forceinline__ void face_fwd(T a00, T a10, T a01, T a11, T (&F)[4]) {
+  const T s0 = a00 + a10, d0 = a10 - a00, s1 = a01 + a11, d1 = a11 - a01;
+  F[0] = s0 + s1;
+  F[1] = d0 + d1;
+  F[2] = s1 - s0;
+  F[3] = d1 - d0;
+}
+
+// Inverse (= transpose) face transform: corner values from face-mode values.
+template <typename T>
+__device__ __forceinline__ void face_inv(const T (&G)[4], T& c00, T& c10, T& c01, T& c11) {
+  const T A = G[0] - G[2], B = G[1] - G[3], C = G[0] + G[2], D = G[1] + G[3];
+  c00 = A - B;
+  c10 = A + B;
+  c01 = C - D;
+  c11 = C + D;
+}
+
+// Number of node planes per CTA: aim at ~2 waves of 2 resident CTAs per SM
+// while keeping the one-layer halo overhead small.
+inline int matvec_zc(int bx, int by, int sz) {
+  const long long nxy = (long long)bx * by;
+  long long want = (2LL * kNumSMs * 2 + nxy - 1) / nxy;
+  if (want < 1) want = 1;
+  if (want > sz) want = sz;
+  int zc = (int)((sz + want - 1) / want);
+  if (zc < 4) zc = (sz < 4) ? sz : 4;
+  return zc;
+}
+
+struct MvLaunch {
+  dim3 grid;
+  int zc;
+  long long nblocks;
+};
+
+template <int TX, int TY>
+inline MvLaunch matvec_launch(const GridDims& g) {
+  MvLaunch L;
+  const int bx = (g.sx + TX - 2) / (TX - 1), by = (g.sy + TY - 2) / (TY - 1);
+  L.zc = matvec_zc(bx, by, g.sz);
+  const int bz = (g.sz + L.zc - 1) / L.zc;
+  L.grid = dim3(bx, by, bz);
+  L.nblocks = (long long)bx * by * bz;
+  return L;
+}
+
+}  // namespace pyto
