@@ -101,6 +101,9 @@ typedef struct pyto_deflation {
 
 /* ---- version / workspace ------------------------------------------------- */
 int pyto_version(void);
+/* Number of kernel launches this library has issued in the process so far (no
+ * reference counterpart: instrumentation of the launch count). */
+long long pyto_launch_count(void);
 /* Bytes of workspace for a call of the given kind on this operator (for
  * PYTO_WS_DPCG: any coarse size up to 24576). */
 size_t pyto_workspace_bytes(const pyto_operator_t* op, int kind);

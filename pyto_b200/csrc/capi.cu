@@ -1,5 +1,6 @@
 // Workspace sizing of the C ABI.
 #include <algorithm>
+#include <atomic>
 
 #include "krylov.cuh"
 
@@ -9,7 +10,14 @@ size_t dpcg_workspace_bytes(const pyto_operator_t* op);
 int oc_grid_blocks();
 }  // namespace pyto
 
+namespace pyto {
+static std::atomic<long long> g_launches{0};
+void count_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+}  // namespace pyto
+
 using namespace pyto;
+
+extern "C" long long pyto_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 
 extern "C" size_t pyto_workspace_bytes(const pyto_operator_t* op, int kind) {
   if (!op) return 0;

@@ -14,6 +14,13 @@
 #define PYTO_LAUNCH_CHECK() PYTO_CUDA(cudaGetLastError())
 
 namespace pyto {
+// process-wide count of kernel launches issued by the library (reported by
+// pyto_launch_count; used to state how many of the library's kernels ran)
+void count_launches(long long n);
+}  // namespace pyto
+#define PYTO_COUNT(n) ::pyto::count_launches(n)
+
+namespace pyto {
 
 constexpr int kNumSMs = 148;        // B200
 constexpr int kReduceBlocks = 1184; // max partial slots of a node-wise reduction (8 per SM)

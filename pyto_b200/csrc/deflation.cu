@@ -611,9 +611,11 @@ static int coarse_solve(const GridDims& g, const DeflP& dp, const pyto_deflation
                         const DpcgWs& W, const KrylovState* S, cudaStream_t st) {
   k_restrict<<<(dp.ngroups + 7) / 8, 256, 0, st>>>(g, dp, d->group_ptr, d->group_nodes, d->group_center, W.fl, y,
                                                    W.cv);
+  PYTO_COUNT(1);
   const size_t shm = (size_t)dp.nc * sizeof(double);
   const int nb = (int)std::min<long long>((dp.nc + 7) / 8, 4 * kNumSMs);
   k_coarse_gemv<<<nb, 256, shm, st>>>(dp.nc, d->coarse_inv, W.cv, W.mu, S);
+  PYTO_COUNT(1);
   PYTO_LAUNCH_CHECK();
   return PYTO_OK;
 }
@@ -648,18 +650,27 @@ extern "C" int pyto_dpcg_setup(const pyto_operator_t* op, const double* s, const
   PYTO_CUDA(cudaMemsetAsync(E, 0, (size_t)n * n * sizeof(double), st));
   k_coarse_assemble<<<(int)std::min<long long>((g.nelem + 127) / 128, 16 * kNumSMs), 128, 0, st>>>(
       g, make_khat(op), dp, s, mask, defl->node_group, defl->group_center, E);
-  if (defl->shift_relative) k_diag_mean<<<1, 256, 0, st>>>(n, E, W.part);
+  PYTO_COUNT(1);
+  if (defl->shift_relative) {
+    k_diag_mean<<<1, 256, 0, st>>>(n, E, W.part);
+    PYTO_COUNT(1);
+  }
   k_coarse_finish<<<(int)std::min<long long>(n, 4 * kNumSMs), 256, 0, st>>>(
       n, E, defl->shift, defl->shift_relative ? W.part : nullptr);
+  PYTO_COUNT(1);
   PYTO_LAUNCH_CHECK();
   const int tiles = (int)((n + 63) / 64);
   for (long long k0 = 0; k0 < n; k0 += kSweepB) {
     const int bk = (int)std::min<long long>(kSweepB, n - k0);
     k_sweep_pivot<<<1, 256, 0, st>>>(n, (int)k0, bk, E, W.P);
+    PYTO_COUNT(1);
     k_sweep_panel<<<(int)((n + 15) / 16), 256, 0, st>>>(n, (int)k0, bk, E, W.P, W.Rp, W.U);
+    PYTO_COUNT(1);
     k_sweep_update<<<dim3(tiles, tiles), 256, 0, st>>>(n, (int)k0, bk, E, W.P, W.Rp, W.U);
+    PYTO_COUNT(1);
   }
   k_negate<<<(int)std::min<long long>((n * n + 255) / 256, 8 * kNumSMs), 256, 0, st>>>(n * n, E);
+  PYTO_COUNT(1);
   PYTO_LAUNCH_CHECK();
   return PYTO_OK;
 }
@@ -681,16 +692,19 @@ extern "C" int pyto_dpcg_solve(const pyto_operator_t* op, const double* s, const
   const int mm = PYTO_MASK_IN | PYTO_MASK_OUT;
   PYTO_CUDA(cudaMemsetAsync(W.counter, 0, 64 * sizeof(unsigned), st));
   k_state_init2<<<1, 1, 0, st>>>(W.S, cfg->rtol, cfg->max_iters, cfg->stop_rule);
+  PYTO_COUNT(1);
   rc = pyto_jacobi(op, s, mask, W.w, W.fl, nullptr, stream);
   if (rc) return rc;
   // coarse start: x = W Einv W_f^T b   (src/deflation.py:532-537)
   rc = coarse_solve(g, dp, defl, b, W, nullptr, st);
   if (rc) return rc;
   k_prolong<<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center, W.mu, W.fl, u);
+  PYTO_COUNT(1);
   // r = b - K x, z = M r
   rc = launch_matvec64(op, s, mask, u, W.q, mm, nullptr, nullptr, nullptr, st);
   if (rc) return rc;
   k_dpcg_init<<<kNodeBlocks, kNodeThreads, 0, st>>>(g, pc, b, W.q, W.w, W.fl, W.r, W.z, W.S, W.part, W.counter);
+  PYTO_COUNT(1);
   // p0 = z - W Einv W^T K z
   rc = launch_matvec64(op, s, mask, W.z, W.q, mm, nullptr, nullptr, nullptr, st);
   if (rc) return rc;
@@ -698,6 +712,7 @@ extern "C" int pyto_dpcg_solve(const pyto_operator_t* op, const double* s, const
   if (rc) return rc;
   k_dpcg_update2<<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center, W.mu, W.fl, W.z,
                                                        W.p, W.S, 1);
+  PYTO_COUNT(1);
   PYTO_LAUNCH_CHECK();
   const int every = std::max(1, cfg->check_every);
   KrylovState hs{};
@@ -709,6 +724,7 @@ extern "C" int pyto_dpcg_solve(const pyto_operator_t* op, const double* s, const
       if (rc) return rc;
       k_dpcg_update1<<<kNodeBlocks, kNodeThreads, 0, st>>>(g, pc, W.w, W.fl, u, W.r, W.z, W.p, W.q, W.S, W.part,
                                                            W.counter);
+      PYTO_COUNT(1);
       // K z -> q (q is free again), mu = Einv W^T K z, p = z + beta p - W mu
       rc = launch_matvec64(op, s, mask, W.z, W.q, mm, nullptr, nullptr, nullptr, st);
       if (rc) return rc;
@@ -716,6 +732,7 @@ extern "C" int pyto_dpcg_solve(const pyto_operator_t* op, const double* s, const
       if (rc) return rc;
       k_dpcg_update2<<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center, W.mu, W.fl,
                                                            W.z, W.p, W.S, 0);
+      PYTO_COUNT(1);
     }
     PYTO_LAUNCH_CHECK();
     PYTO_CUDA(cudaMemcpyAsync(&hs, W.S, sizeof(hs), cudaMemcpyDeviceToHost, st));
@@ -725,6 +742,7 @@ extern "C" int pyto_dpcg_solve(const pyto_operator_t* op, const double* s, const
   rc = launch_matvec64(op, s, mask, u, W.q, mm, nullptr, nullptr, nullptr, st);
   if (rc) return rc;
   k_true_residual2<<<kNodeBlocks, kNodeThreads, 0, st>>>(g, b, W.q, W.fl, W.S, W.part, W.counter);
+  PYTO_COUNT(1);
   PYTO_LAUNCH_CHECK();
   PYTO_CUDA(cudaMemcpyAsync(&hs, W.S, sizeof(hs), cudaMemcpyDeviceToHost, st));
   PYTO_CUDA(cudaStreamSynchronize(st));

@@ -295,6 +295,7 @@ extern "C" int pyto_elem_energy(const pyto_operator_t* op, const double* u, cons
     PYTO_CUDA(cudaMemsetAsync(counter, 0, 64 * sizeof(unsigned), st));
   }
   k_elem_energy<<<nb, kElemThreads, 0, st>>>(g, make_khat(op), u, v, s, ce, part, counter, total);
+  PYTO_COUNT(1);
   PYTO_LAUNCH_CHECK();
   return PYTO_OK;
 }
@@ -305,6 +306,7 @@ extern "C" int pyto_stress(const pyto_operator_t* op, const double* u, const dou
   const GridDims g = make_dims(op);
   k_stress<<<elem_blocks(g.nelem), kElemThreads, 0, (cudaStream_t)stream>>>(g, make_stress(op), u, x, q, strain,
                                                                              stress, vm, sed);
+  PYTO_COUNT(1);
   PYTO_LAUNCH_CHECK();
   return PYTO_OK;
 }
@@ -321,6 +323,7 @@ extern "C" int pyto_pnorm_sum(const pyto_operator_t* op, const double* vm, doubl
   if (!cv.ok()) return PYTO_ERR_WORKSPACE;
   PYTO_CUDA(cudaMemsetAsync(counter, 0, 64 * sizeof(unsigned), st));
   k_pow_sum<<<nb, kElemThreads, 0, st>>>(g.nelem, vm, P, part, counter, sum_out);
+  PYTO_COUNT(1);
   PYTO_LAUNCH_CHECK();
   return PYTO_OK;
 }
@@ -332,7 +335,9 @@ extern "C" int pyto_pnorm_adjoint(const pyto_operator_t* op, const double* u, co
   cudaStream_t st = (cudaStream_t)stream;
   const StressP Pp = make_stress(op);
   k_pnorm_elem<<<elem_blocks(g.nelem), kElemThreads, 0, st>>>(g, Pp, u, x, q, P, dpn_dev, T1, tvec);
+  PYTO_COUNT(1);
   k_pnorm_gather<<<elem_blocks(g.nnodes), kElemThreads, 0, st>>>(g, Pp, tvec, gvec);
+  PYTO_COUNT(1);
   PYTO_LAUNCH_CHECK();
   return PYTO_OK;
 }

@@ -104,6 +104,7 @@ extern "C" int pyto_filter(const pyto_operator_t* op, double rel_radius, int mod
     case PYTO_FILTER_HS: k_filter<PYTO_FILTER_HS><<<nb, 256, 0, st>>>(g, t, x, w, hs, active, y); break;
     default: return PYTO_ERR_ARG;
   }
+  PYTO_COUNT(1);
   PYTO_LAUNCH_CHECK();
   return PYTO_OK;
 }

@@ -166,6 +166,7 @@ int launch_matvec64(const pyto_operator_t* op, const double* s, const uint8_t* m
   else
     k_matvec64<TX, TY, false><<<L.grid, TX * TY, 0, st>>>(g, kh, s, mask, u, y, L.zc, mode, nullptr, nullptr,
                                                           nullptr);
+  PYTO_COUNT(1);
   PYTO_LAUNCH_CHECK();
   return PYTO_OK;
 }
@@ -241,6 +242,7 @@ extern "C" int pyto_bc_mask(const pyto_operator_t* op, const int64_t* fixed_dofs
   if (n_fixed > 0) {
     const int nb = (int)std::min<int64_t>((n_fixed + 255) / 256, 4 * kNumSMs);
     k_bc_mask<<<nb, 256, 0, st>>>(fixed_dofs, n_fixed, 3 * g.nnodes, (unsigned*)mask);
+    PYTO_COUNT(1);
     PYTO_LAUNCH_CHECK();
   }
   return PYTO_OK;
@@ -252,6 +254,7 @@ extern "C" int pyto_simp(const double* x, const uint8_t* active, int64_t n, doub
   if (n == 0) return PYTO_OK;
   const int nb = (int)std::min<int64_t>((n + 255) / 256, 8 * kNumSMs);
   k_simp<<<nb, 256, 0, (cudaStream_t)stream>>>(x, active, n, penal, emin, s, ds);
+  PYTO_COUNT(1);
   PYTO_LAUNCH_CHECK();
   return PYTO_OK;
 }
@@ -262,6 +265,7 @@ extern "C" int pyto_jacobi(const pyto_operator_t* op, const double* s, const uin
   const GridDims g = make_dims(op);
   const int nb = (int)std::min<long long>((g.nnodes + 255) / 256, 8 * kNumSMs);
   k_jacobi<<<nb, 256, 0, (cudaStream_t)stream>>>(g, make_khat(op), s, mask, winv, flags, diag_out);
+  PYTO_COUNT(1);
   PYTO_LAUNCH_CHECK();
   return PYTO_OK;
 }

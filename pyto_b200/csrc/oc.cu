@@ -111,5 +111,6 @@ extern "C" int pyto_oc_update(const pyto_operator_t* op, double* x, const double
   void* args[] = {&n, &x, (void*)&dc, (void*)&active, &n_act, &volfrac, &move, &xmin, &xmax, &part, &change_out};
   PYTO_CUDA(cudaLaunchCooperativeKernel((const void*)k_oc_update, dim3(nb), dim3(kOcThreads), args, 0,
                                         (cudaStream_t)stream));
+  PYTO_COUNT(1);
   return PYTO_OK;
 }

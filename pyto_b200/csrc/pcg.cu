@@ -214,6 +214,7 @@ extern "C" int pyto_pcg_solve(const pyto_operator_t* op, const double* s, const 
   const Prec pc = make_prec(op);
   PYTO_CUDA(cudaMemsetAsync(W.counter, 0, 64 * sizeof(unsigned), st));
   k_state_init<<<1, 1, 0, st>>>(W.S, cfg->rtol, cfg->max_iters, cfg->stop_rule);
+  PYTO_COUNT(1);
   PYTO_LAUNCH_CHECK();
   int rc = pyto_jacobi(op, s, mask, W.w, W.fl, nullptr, stream);
   if (rc) return rc;
@@ -224,6 +225,7 @@ extern "C" int pyto_pcg_solve(const pyto_operator_t* op, const double* s, const 
   }
   k_pcg_init<<<kNodeBlocks, kNodeThreads, 0, st>>>(g, pc, b, cfg->x0_given ? W.q : nullptr, W.w, W.fl, u, W.r, W.p,
                                                    W.S, W.part, W.counter);
+  PYTO_COUNT(1);
   PYTO_LAUNCH_CHECK();
   const int every = std::max(1, cfg->check_every);
   KrylovState hs{};
@@ -235,7 +237,9 @@ extern "C" int pyto_pcg_solve(const pyto_operator_t* op, const double* s, const 
       if (rc) return rc;
       k_pcg_update1<<<kNodeBlocks, kNodeThreads, 0, st>>>(g, pc, W.w, W.fl, u, W.r, W.p, W.q, W.S, W.part,
                                                           W.counter);
+      PYTO_COUNT(1);
       k_pcg_update2<<<kNodeBlocks, kNodeThreads, 0, st>>>(g, pc, W.w, W.fl, W.r, W.p, W.S);
+      PYTO_COUNT(1);
     }
     PYTO_LAUNCH_CHECK();
     PYTO_CUDA(cudaMemcpyAsync(&hs, W.S, sizeof(hs), cudaMemcpyDeviceToHost, st));
@@ -246,6 +250,7 @@ extern "C" int pyto_pcg_solve(const pyto_operator_t* op, const double* s, const 
   rc = launch_matvec64(op, s, mask, u, W.q, mm, nullptr, nullptr, nullptr, st);
   if (rc) return rc;
   k_true_residual<<<kNodeBlocks, kNodeThreads, 0, st>>>(g, b, W.q, W.fl, W.S, W.part, W.counter);
+  PYTO_COUNT(1);
   PYTO_LAUNCH_CHECK();
   PYTO_CUDA(cudaMemcpyAsync(&hs, W.S, sizeof(hs), cudaMemcpyDeviceToHost, st));
   PYTO_CUDA(cudaStreamSynchronize(st));

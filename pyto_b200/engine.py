@@ -1,0 +1,228 @@
+"""Device-side engine of one voxel grid: every call goes through the C ABI.
+
+``HexGrid`` holds the operator struct (grid + Ke), the per-node Dirichlet mask
+and the optional active-element mask on the device, and exposes the library's
+entry points on torch CUDA float64 tensors.  Torch provides device memory and
+the current stream only; all arithmetic runs in libpyto_b200.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _capi as A
+
+F64 = torch.float64
+
+
+def _round4(n: int) -> int:
+    return (n + 3) // 4 * 4
+
+
+@dataclass
+class SolveInfo:
+    """Outcome of one Krylov solve (mirrors pyto_solve_status_t)."""
+    converged: bool
+    iters: int
+    breakdown: bool
+    rel_res: float
+    true_rel_res: float
+    code: int
+
+
+class HexGrid:
+    """A box grid of nelx*nely*nelz hex8 elements on one CUDA device."""
+
+    def __init__(self, nel, elem_size=(1.0, 1.0, 1.0), E=1.0, nu=0.3, ke=None, device=None):
+        if not torch.cuda.is_available():
+            raise RuntimeError("pyto_b200 needs a CUDA device (sm_100a); no CPU path exists")
+        self.device = torch.device(device if device is not None else "cuda")
+        self.nel = tuple(int(n) for n in nel)
+        self.h = tuple(float(v) for v in elem_size)
+        self.op = A.make_operator(*self.nel, self.h, E, nu, ke)
+        nx, ny, nz = self.nel
+        self.nnodes = (nx + 1) * (ny + 1) * (nz + 1)
+        self.nelem = nx * ny * nz
+        self.ndof = 3 * self.nnodes
+        self.mask = torch.zeros(_round4(self.nnodes), dtype=torch.uint8, device=self.device)
+        self.active = None
+        self.n_active = self.nelem
+        self._scalars = torch.zeros(8, dtype=F64, device=self.device)
+
+    # ---- helpers -------------------------------------------------------------
+    @property
+    def opp(self):
+        return C.byref(self.op)
+
+    def _st(self):
+        return A.stream_ptr(self.device)
+
+    def _ws(self, kind: int, tag: str):
+        n = A.ws_bytes(self.op, kind)
+        buf = A.workspace(n, self.device, tag)
+        return A.ptr(buf), buf.numel()
+
+    def tensor(self, a, dtype=F64):
+        """Contiguous device tensor of `a` (numpy or torch)."""
+        if isinstance(a, torch.Tensor):
+            return a.to(device=self.device, dtype=dtype).contiguous()
+        return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype, device=self.device)
+
+    # ---- set-up -----------------------------------------------------------------
+    def set_fixed_dofs(self, fixed_dofs):
+        fd = self.tensor(np.asarray(fixed_dofs, dtype=np.int64).ravel() if not isinstance(fixed_dofs, torch.Tensor)
+                         else fixed_dofs, dtype=torch.int64)
+        A.call("pyto_bc_mask", self.opp, A.ptr(fd) if fd.numel() else None, int(fd.numel()), A.ptr(self.mask),
+               self._st())
+        return self
+
+    def set_active(self, active):
+        if active is None:
+            self.active, self.n_active = None, self.nelem
+            return self
+        a = np.asarray(active.cpu().numpy() if isinstance(active, torch.Tensor) else active).astype(bool).ravel()
+        if a.size != self.nelem:
+            raise ValueError("active mask must have one entry per element")
+        self.active = torch.as_tensor(a.astype(np.uint8), device=self.device)
+        self.n_active = int(a.sum())
+        return self
+
+    # ---- material ------------------------------------------------------------------
+    def simp(self, x, penal=3.0, emin=1e-9, want_ds=True):
+        x = self.tensor(x)
+        s = torch.empty_like(x)
+        ds = torch.empty_like(x) if want_ds else None
+        A.call("pyto_simp", A.ptr(x), A.ptr(self.active), int(x.numel()), float(penal), float(emin), A.ptr(s),
+               A.ptr(ds), self._st())
+        return s, ds
+
+    # ---- operator -------------------------------------------------------------------
+    def matvec(self, s, u, mode=A.MASK_IN | A.MASK_OUT, out=None, dot=False):
+        """y = K(s) u on full-length vectors (Dirichlet masking per mode)."""
+        y = out if out is not None else torch.empty(self.ndof, dtype=F64, device=self.device)
+        d = self._scalars[0:1] if dot else None
+        wsp, wsn = self._ws(A.WS_REDUCE, "reduce") if dot else (None, 0)
+        A.call("pyto_matvec", self.opp, A.ptr(s), A.ptr(self.mask), A.ptr(u), A.ptr(y), int(mode), A.ptr(d), wsp, wsn,
+               self._st())
+        return (y, d) if dot else y
+
+    def jacobi(self, s):
+        winv = torch.empty(self.nnodes, dtype=F64, device=self.device)
+        flags = torch.empty(self.nnodes, dtype=torch.uint8, device=self.device)
+        diag = torch.empty(self.ndof, dtype=F64, device=self.device)
+        A.call("pyto_jacobi", self.opp, A.ptr(s), A.ptr(self.mask), A.ptr(winv), A.ptr(flags), A.ptr(diag),
+               self._st())
+        return diag, flags
+
+    # ---- solvers ---------------------------------------------------------------------
+    @staticmethod
+    def _cfg(rtol, max_iters, stop_rule, check_every, x0):
+        return A.SolveCfg(float(rtol), int(max_iters), int(stop_rule), int(check_every), 1 if x0 else 0)
+
+    def pcg(self, s, b, rtol=1e-8, max_iters=100000, stop_rule=0, x0=None, check_every=25, out=None):
+        """Jacobi PCG on K_ff (fixed DOFs of the result are 0)."""
+        u = out if out is not None else torch.empty(self.ndof, dtype=F64, device=self.device)
+        if x0 is not None:
+            u.copy_(x0)
+        cfg = self._cfg(rtol, max_iters, stop_rule, check_every, x0 is not None)
+        stt = A.SolveStatus()
+        wsp, wsn = self._ws(A.WS_PCG, "krylov")
+        rc = A.call("pyto_pcg_solve", self.opp, A.ptr(s), A.ptr(self.mask), A.ptr(b), A.ptr(u), C.byref(cfg),
+                    C.byref(stt), wsp, wsn, self._st(), allow=(A.OK, A.NOT_CONVERGED, A.ERR_BREAKDOWN))
+        return u, SolveInfo(bool(stt.converged), int(stt.iters), bool(stt.breakdown), float(stt.rel_res),
+                            float(stt.true_rel_res), rc)
+
+    def dpcg_setup(self, s, defl):
+        wsp, wsn = self._ws(A.WS_DPCG, "krylov")
+        A.call("pyto_dpcg_setup", self.opp, A.ptr(s), A.ptr(self.mask), C.byref(defl.struct), wsp, wsn, self._st())
+
+    def dpcg(self, s, b, defl, rtol=1e-8, max_iters=2000, stop_rule=1, check_every=25, out=None, setup=True):
+        """Deflated PCG (coarse inverse rebuilt for s when setup=True)."""
+        if setup:
+            self.dpcg_setup(s, defl)
+        u = out if out is not None else torch.empty(self.ndof, dtype=F64, device=self.device)
+        cfg = self._cfg(rtol, max_iters, stop_rule, check_every, False)
+        stt = A.SolveStatus()
+        wsp, wsn = self._ws(A.WS_DPCG, "krylov")
+        rc = A.call("pyto_dpcg_solve", self.opp, A.ptr(s), A.ptr(self.mask), C.byref(defl.struct), A.ptr(b),
+                    A.ptr(u), C.byref(cfg), C.byref(stt), wsp, wsn, self._st(),
+                    allow=(A.OK, A.NOT_CONVERGED, A.ERR_BREAKDOWN))
+        return u, SolveInfo(bool(stt.converged), int(stt.iters), bool(stt.breakdown), float(stt.rel_res),
+                            float(stt.true_rel_res), rc)
+
+    # ---- element quantities ---------------------------------------------------------------
+    def energy(self, u, v=None, s=None):
+        """ce_e = u_e^T Ke v_e; with s also returns sum_e s_e ce_e (device scalar)."""
+        v = u if v is None else v
+        ce = torch.empty(self.nelem, dtype=F64, device=self.device)
+        tot = self._scalars[1:2] if s is not None else None
+        wsp, wsn = self._ws(A.WS_REDUCE, "reduce") if s is not None else (None, 0)
+        A.call("pyto_elem_energy", self.opp, A.ptr(u), A.ptr(v), A.ptr(s), A.ptr(ce), A.ptr(tot), wsp, wsn,
+               self._st())
+        return (ce, tot) if s is not None else ce
+
+    def stress(self, u, x, q=0.5, want=("strain", "stress", "vm", "sed")):
+        out = {}
+        for k, n in (("strain", 6), ("stress", 6), ("vm", 1), ("sed", 1)):
+            out[k] = torch.empty(self.nelem * n, dtype=F64, device=self.device) if k in want else None
+        A.call("pyto_stress", self.opp, A.ptr(u), A.ptr(self.tensor(x)), float(q), A.ptr(out["strain"]),
+               A.ptr(out["stress"]), A.ptr(out["vm"]), A.ptr(out["sed"]), self._st())
+        for k in ("strain", "stress"):
+            if out[k] is not None:
+                out[k] = out[k].view(self.nelem, 6)
+        return out
+
+    def pow_sum(self, vm, P):
+        out = self._scalars[2:3]
+        wsp, wsn = self._ws(A.WS_REDUCE, "reduce")
+        A.call("pyto_pnorm_sum", self.opp, A.ptr(vm), float(P), A.ptr(out), wsp, wsn, self._st())
+        return out
+
+    def pnorm_adjoint(self, u, x, q, P, dpn_dev):
+        T1 = torch.empty(self.nelem, dtype=F64, device=self.device)
+        g = torch.empty(self.ndof, dtype=F64, device=self.device)
+        tvec = torch.empty(6 * self.nelem, dtype=F64, device=self.device)
+        A.call("pyto_pnorm_adjoint", self.opp, A.ptr(u), A.ptr(self.tensor(x)), float(q), float(P), A.ptr(dpn_dev),
+               A.ptr(T1), A.ptr(g), A.ptr(tvec), self._st())
+        return T1, g
+
+    # ---- filter / OC ------------------------------------------------------------------------
+    def filter(self, rel_radius, mode, x=None, w=None, hs=None, out=None):
+        y = out if out is not None else torch.empty(self.nelem, dtype=F64, device=self.device)
+        A.call("pyto_filter", self.opp, float(rel_radius), int(mode), A.ptr(x), A.ptr(w), A.ptr(hs),
+               A.ptr(self.active), A.ptr(y), self._st())
+        return y
+
+    def oc_update(self, x, dc, volfrac, move=0.2, xmin=0.001, xmax=1.0):
+        """In-place OC update of x; returns max |dx| as a device scalar."""
+        ch = self._scalars[3:4]
+        wsp, wsn = self._ws(A.WS_OC, "oc")
+        A.call("pyto_oc_update", self.opp, A.ptr(x), A.ptr(dc), A.ptr(self.active), int(self.n_active),
+               float(volfrac), float(move), float(xmin), float(xmax), A.ptr(ch), wsp, wsn, self._st())
+        return ch
+
+
+class DeviceDeflation:
+    """Device data of a deflation space (node groups + rigid modes)."""
+
+    def __init__(self, grid: HexGrid, node_group, centers, modes=6, shift=1e-10, shift_relative=False):
+        node_group = np.asarray(node_group, dtype=np.int32).ravel()
+        centers = np.asarray(centers, dtype=np.float64).reshape(-1, 3)
+        ng = centers.shape[0]
+        order = np.argsort(node_group, kind="stable").astype(np.int32)
+        counts = np.bincount(node_group, minlength=ng)
+        gptr = np.concatenate([[0], np.cumsum(counts)]).astype(np.int32)
+        dev = grid.device
+        self.node_group = torch.as_tensor(node_group, device=dev)
+        self.group_ptr = torch.as_tensor(gptr, device=dev)
+        self.group_nodes = torch.as_tensor(order, device=dev)
+        self.group_center = torch.as_tensor(np.ascontiguousarray(centers), device=dev)
+        self.ngroups, self.modes = ng, int(modes)
+        self.nc = ng * self.modes
+        self.coarse_inv = torch.empty(self.nc * self.nc, dtype=F64, device=dev)
+        self.struct = A.Deflation(ng, self.modes, A.ptr(self.node_group), A.ptr(self.group_ptr),
+                                  A.ptr(self.group_nodes), A.ptr(self.group_center), A.ptr(self.coarse_inv),
+                                  float(shift), 1 if shift_relative else 0, 0)
