@@ -1,0 +1,69 @@
+"""Micro-benchmark of single library kernels (also the command profiled with ncu).
+
+    python -m pyto_b200.kernel_bench --kernel matvec --nel 192,96,96 --reps 20
+
+Prints one JSON line per kernel: average launch time (CUDA events on the
+launching stream, after warm-up) and the achieved algorithmic bandwidth.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+
+import numpy as np
+import torch
+
+from . import _capi as A
+from .engine import HexGrid
+from .hex_mesher import HexMesher
+from .problems import cantilever
+
+
+def _timeit(fn, reps, warm=3):
+    for _ in range(warm):
+        fn()
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    for _ in range(reps):
+        fn()
+    e1.record(st)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / reps / 1e3
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--kernel", default="matvec", choices=["matvec", "energy", "filter", "jacobi", "stress"])
+    ap.add_argument("--nel", default="192,96,96")
+    ap.add_argument("--reps", type=int, default=20)
+    ap.add_argument("--warm", type=int, default=3)
+    a = ap.parse_args(argv)
+    nel = tuple(int(v) for v in a.nel.split(","))
+    mesh = HexMesher()
+    mesh.grid_mesh(nel, (1.0, 1.0, 1.0))
+    f, fixed = cantilever(mesh)
+    g = HexGrid(nel).set_fixed_dofs(fixed)
+    rng = np.random.default_rng(0)
+    s = g.tensor(rng.uniform(0.01, 1.0, g.nelem))
+    u = g.tensor(rng.normal(size=g.ndof))
+    y = torch.empty_like(u)
+    if a.kernel == "matvec":
+        fn, nbytes = (lambda: g.matvec(s, u, out=y)), 48 * g.nnodes + 8 * g.nelem + g.nnodes
+    elif a.kernel == "energy":
+        fn, nbytes = (lambda: g.energy(u, s=s)), 24 * g.nnodes + 16 * g.nelem
+    elif a.kernel == "filter":
+        out = torch.empty_like(s)
+        fn, nbytes = (lambda: g.filter(2.0, A.FILTER_DENSITY, s, out=out)), 16 * g.nelem
+    elif a.kernel == "jacobi":
+        fn, nbytes = (lambda: g.jacobi(s)), 8 * g.nelem + 33 * g.nnodes
+    else:
+        fn, nbytes = (lambda: g.stress(u, s, 0.5, want=("vm",))), 24 * g.nnodes + 16 * g.nelem
+    t = _timeit(fn, a.reps, a.warm)
+    print(json.dumps({"kernel": a.kernel, "nel": nel, "ms": t * 1e3, "algorithmic_bytes": int(nbytes),
+                      "GB_s": nbytes / t / 1e9}))
+
+
+if __name__ == "__main__":
+    main()
