@@ -104,6 +104,11 @@ int pyto_version(void);
 /* Number of kernel launches this library has issued in the process so far (no
  * reference counterpart: instrumentation of the launch count). */
 long long pyto_launch_count(void);
+/* Select the tile variant of a kernel (no reference counterpart: the tile
+ * choice of the project's autotuner).  PYTO_KERNEL_MATVEC variants 0..3.
+ * Process-wide; not thread-safe against concurrent launches. */
+#define PYTO_KERNEL_MATVEC 0
+int pyto_tune(int kernel, int variant);
 /* Bytes of workspace for a call of the given kind on this operator (for
  * PYTO_WS_DPCG: any coarse size up to 24576). */
 size_t pyto_workspace_bytes(const pyto_operator_t* op, int kind);

@@ -63,6 +63,7 @@ _OP = C.POINTER(Operator)
 SIGNATURES = {
     "pyto_version": (C.c_int, []),
     "pyto_launch_count": (C.c_longlong, []),
+    "pyto_tune": (C.c_int, [C.c_int, C.c_int]),
     "pyto_workspace_bytes": (C.c_size_t, [_OP, C.c_int]),
     "pyto_ke_hex8": (C.c_int, [C.c_double] * 5 + [_P]),
     "pyto_operator_init": (C.c_int, [_OP, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,

@@ -8,6 +8,7 @@ namespace pyto {
 size_t pcg_workspace_bytes(const pyto_operator_t* op);
 size_t dpcg_workspace_bytes(const pyto_operator_t* op);
 int oc_grid_blocks();
+int set_matvec_variant(int v);
 }  // namespace pyto
 
 namespace pyto {
@@ -16,6 +17,13 @@ void count_launches(long long n) { g_launches.fetch_add(n, std::memory_order_rel
 }  // namespace pyto
 
 using namespace pyto;
+
+extern "C" int pyto_tune(int kernel, int variant) {
+  switch (kernel) {
+    case PYTO_KERNEL_MATVEC: return set_matvec_variant(variant);
+    default: return PYTO_ERR_ARG;
+  }
+}
 
 extern "C" long long pyto_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 

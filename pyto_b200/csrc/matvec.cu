@@ -8,170 +8,305 @@ namespace pyto {
 
 // ---------------------------------------------------------------------------
 // matrix-free y = K(s) u
+//
+// Per element layer ez (one barrier):
+//   1. barrier; write the owned nodes of plane ez-1 (their 4 column
+//      contributions were combined in the previous layer: x by shuffle, y
+//      through `sc`);
+//   2. stage plane ez+2 (prefetched in registers) into smem ring slot
+//      (ez+2)&3 and issue the global loads of plane ez+3;
+//   3. element core for layer ez from the face transforms of planes ez (kept
+//      from the previous layer) and ez+1;  the bottom-face part plus the
+//      pending top-face part of layer ez-1 completes plane ez, which is
+//      inverse-transformed and combined across columns for output in the
+//      next layer.  The pending top-face accumulators of a thread live in its
+//      own shared-memory slots (`sG`) rather than in registers.
+// Four plane slots are in flight: ez-1 (output: BC mask and u for the fused
+// dot), ez and ez+1 (compute), ez+2 (being staged).
 // ---------------------------------------------------------------------------
-template <int TX, int TY, bool DOT>
-__global__ void __launch_bounds__(TX* TY, 2)
+template <int TY>
+struct MvSmem {
+  static constexpr int TX = 32, NT = TX * TY, PX = TX + 1, PY = TY + 1, PLANE = PX * PY, RING = 5;
+  static constexpr size_t su = RING * 3 * PLANE;  // doubles
+  static constexpr size_t sG = 12 * NT;           // doubles
+  static constexpr size_t sc = 2 * 3 * TY * TX;   // doubles
+  static constexpr size_t bytes = 8 * (su + sG + sc) + RING * PLANE + 16;
+};
+
+__device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc, bool valid) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+  const int n = valid ? 8 : 0;  // 0: zero-fill, the source is not read
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gsrc), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+__device__ __forceinline__ int ring5(int k) { return (k + 5) % 5; }
+
+template <int TY, bool DOT, bool MASKIN, int MINB>
+__global__ void __launch_bounds__(32 * TY, MINB)
     k_matvec64(GridDims g, KHat kh, const double* __restrict__ s, const uint8_t* __restrict__ mask,
                const double* __restrict__ u, double* __restrict__ y, int zc, int mode, double* part,
                unsigned* counter, double* dot_out) {
-  using T = MvTile<TX, TY>;
-  __shared__ double su[2][3][T::PLANE];
-  __shared__ double sc[3][TY][TX];
-  __shared__ double sred[T::NT / 32];
+  using M = MvSmem<TY>;
+  constexpr int TX = M::TX, NT = M::NT, PX = M::PX, PLANE = M::PLANE;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* su = reinterpret_cast<double*>(smem_raw);  // [RING][3][PLANE]
+  double* sG = su + M::su;                           // [12][NT] pending top-face accumulators
+  double* sc = sG + M::sG;                           // [2][3][TY][TX] y-combine partials
+  uint8_t* smk = reinterpret_cast<uint8_t*>(sc + M::sc);  // [RING][PLANE] BC mask
+  __shared__ double sred[NT / 32];
 
   const int tid = threadIdx.x;
-  const int tx = tid & (TX - 1), ty = tid / TX;
+  const int tx = tid & 31, ty = tid >> 5;
   const int X0 = blockIdx.x * (TX - 1), Y0 = blockIdx.y * (TY - 1);
   const int Z0 = blockIdx.z * zc;
   const int Z1 = min(Z0 + zc, g.sz);
   const int ex = X0 - 1 + tx, ey = Y0 - 1 + ty;
   const bool col_in = ex >= 0 && ex < g.nx && ey >= 0 && ey < g.ny;
-  const bool mask_in = (mode & PYTO_MASK_IN) && mask != nullptr;
   const bool mask_out = (mode & PYTO_MASK_OUT) && mask != nullptr;
   const long long plane_nodes = (long long)g.sx * g.sy;
 
-  // flat, coalesced plane loader: tile rows of PX nodes x 3 components
-  double pre[T::LOADS];
-  auto load_plane = [&](int k) {
+  // staging slots: node (tx, ty) of the (TX+1) x (TY+1) tile, plus the last
+  // tile row / column for the first TX+1+TY threads
+  auto plane_off = [&](int lx, int ly) -> int {
+    const int gx = X0 - 1 + lx, gy = Y0 - 1 + ly;
+    return (gx >= 0 && gx < g.sx && gy >= 0 && gy < g.sy) ? gx + g.sx * gy : -1;
+  };
+  int lxe = -1, lye = -1;
+  if (tid < PX) {
+    lxe = tid;
+    lye = TY;
+  } else if (tid < PX + TY) {
+    lxe = TX;
+    lye = tid - PX;
+  }
+  const int offm = plane_off(tx, ty);
+  const int offe = lxe >= 0 ? plane_off(lxe, lye) : -1;
+  const int sim = ty * PX + tx, sie = lye * PX + lxe;
+  // asynchronous copy of plane k into ring slot ring5(k) (zero outside the domain)
+  auto issue_plane = [&](int k) {
+    const bool kin = k >= 0 && k < g.sz;
+    const long long base = plane_nodes * (kin ? k : 0);
+    double* d = su + (size_t)ring5(k) * 3 * PLANE;
+    {
+      const bool v = kin && offm >= 0;
+      const double* src = u + (v ? 3 * (base + offm) : 0);
 #pragma unroll
-    for (int i = 0; i < T::LOADS; ++i) {
-      const int idx = tid + i * T::NT;
-      double v = 0.0;
-      if (idx < T::PLANE_D && k >= 0 && k < g.sz) {
-        const int row = idx / (3 * T::PX);
-        const int rem = idx - row * 3 * T::PX;
-        const int nxl = rem / 3;
-        const int c = rem - 3 * nxl;
-        const int gx = X0 - 1 + nxl, gy = Y0 - 1 + row;
-        if (gx >= 0 && gx < g.sx && gy >= 0 && gy < g.sy) {
-          const long long node = gx + (long long)g.sx * gy + plane_nodes * k;
-          v = __ldg(u + 3 * node + c);
-          if (mask_in && ((__ldg(mask + node) >> c) & 1)) v = 0.0;
-        }
-      }
-      pre[i] = v;
+      for (int c = 0; c < 3; ++c) cp_async8(d + c * PLANE + sim, src + c, v);
+    }
+    if (lxe >= 0) {
+      const bool v = kin && offe >= 0;
+      const double* src = u + (v ? 3 * (base + offe) : 0);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) cp_async8(d + c * PLANE + sie, src + c, v);
+    }
+    cp_async_commit();
+  };
+  int mm = 0, me = 0;
+  auto load_mask = [&](int k) {
+    mm = me = 0;
+    if (mask && k >= 0 && k < g.sz) {
+      const long long base = plane_nodes * k;
+      if (offm >= 0) mm = __ldg(mask + base + offm);
+      if (offe >= 0) me = __ldg(mask + base + offe);
     }
   };
-  auto store_plane = [&](int b) {
-#pragma unroll
-    for (int i = 0; i < T::LOADS; ++i) {
-      const int idx = tid + i * T::NT;
-      if (idx < T::PLANE_D) {
-        const int row = idx / (3 * T::PX);
-        const int rem = idx - row * 3 * T::PX;
-        const int nxl = rem / 3;
-        const int c = rem - 3 * nxl;
-        su[b][c][row * T::PX + nxl] = pre[i];
-      }
-    }
+  auto store_mask = [&](int k) {
+    uint8_t* d = smk + ring5(k) * PLANE;
+    d[sim] = (uint8_t)mm;
+    if (lxe >= 0) d[sie] = (uint8_t)me;
   };
   auto load_s = [&](int ez) -> double {
     if (!col_in || ez < 0 || ez >= g.nz) return 0.0;
     return __ldg(s + ex + (long long)g.nx * (ey + (long long)g.ny * ez));
   };
-  auto face = [&](int b, double (&F)[3][4]) {
-    const int i00 = ty * T::PX + tx;
+  auto face = [&](int k, double (&F)[3][4]) {
+    const double* b = su + (size_t)ring5(k) * 3 * PLANE + ty * PX + tx;
+    int m00 = 0, m10 = 0, m01 = 0, m11 = 0;
+    if (MASKIN) {
+      const uint8_t* mb = smk + ring5(k) * PLANE + ty * PX + tx;
+      m00 = mb[0];
+      m10 = mb[1];
+      m01 = mb[PX];
+      m11 = mb[PX + 1];
+    }
 #pragma unroll
-    for (int c = 0; c < 3; ++c)
-      face_fwd(su[b][c][i00], su[b][c][i00 + 1], su[b][c][i00 + T::PX], su[b][c][i00 + T::PX + 1], F[c]);
+    for (int c = 0; c < 3; ++c) {
+      const double* bc = b + c * PLANE;
+      double a00 = bc[0], a10 = bc[1], a01 = bc[PX], a11 = bc[PX + 1];
+      if (MASKIN) {
+        if ((m00 >> c) & 1) a00 = 0.0;
+        if ((m10 >> c) & 1) a10 = 0.0;
+        if ((m01 >> c) & 1) a01 = 0.0;
+        if ((m11 >> c) & 1) a11 = 0.0;
+      }
+      face_fwd(a00, a10, a01, a11, F[c]);
+    }
+  };
+  const bool owner = tx < TX - 1 && ty < TY - 1 && (X0 + tx) < g.sx && (Y0 + ty) < g.sy;
+  double dot = 0.0;
+  double cT[3] = {0.0, 0.0, 0.0};
+  auto output = [&](int k) {  // owned node of plane k
+    if (!owner) return;
+    const int li = (ty + 1) * PX + tx + 1;
+    const int mk = mask_out ? (int)smk[ring5(k) * PLANE + li] : 0;
+    const long long node = (X0 + tx) + (long long)g.sx * (Y0 + ty) + plane_nodes * k;
+    const double* scb = sc + (size_t)(k & 1) * 3 * TY * TX;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      double v = cT[c] + scb[(c * TY + ty + 1) * TX + tx];
+      if ((mk >> c) & 1) v = 0.0;
+      y[3 * node + c] = v;
+      if (DOT) {
+        double uv = su[(size_t)(ring5(k) * 3 + c) * PLANE + li];
+        if (MASKIN && ((smk[ring5(k) * PLANE + li] >> c) & 1)) uv = 0.0;
+        dot = fma(uv, v, dot);
+      }
+    }
   };
 
-  // prologue: bottom plane of the first element layer
-  load_plane(Z0 - 1);
-  store_plane(0);
-  load_plane(Z0);
+  // prologue: planes Z0-1, Z0 in flight, masks of Z0-1, Z0 staged, mask of Z0+1 in registers
+  issue_plane(Z0 - 1);
+  issue_plane(Z0);
+  load_mask(Z0 - 1);
+  store_mask(Z0 - 1);
+  load_mask(Z0);
+  store_mask(Z0);
+  load_mask(Z0 + 1);
   double s_next = load_s(Z0 - 1);
-  __syncthreads();
-  double Fb[3][4], Gp[3][4];
-  face(0, Fb);
 #pragma unroll
-  for (int c = 0; c < 3; ++c)
-#pragma unroll
-    for (int f = 0; f < 4; ++f) Gp[c][f] = 0.0;
+  for (int i = 0; i < 12; ++i) sG[i * NT + tid] = 0.0;
+  if (Z0 + 1 <= Z1) issue_plane(Z0 + 1);
+  else cp_async_commit();
 
-  double dot = 0.0;
-  const bool owner = tx < TX - 1 && ty < TY - 1 && (X0 + tx) < g.sx && (Y0 + ty) < g.sy;
-
+  // layer ez: planes ez, ez+1 landed (wait_group 1 leaves plane ez+2 in flight)
   for (int ez = Z0 - 1; ez < Z1; ++ez) {
-    const int bt = (ez - Z0 + 2) & 1;  // buffer of plane ez+1
-    store_plane(bt);
-    if (ez + 2 <= Z1) load_plane(ez + 2);
+    cp_async_wait1();
+    __syncthreads();
+    if (ez - 1 >= Z0) output(ez - 1);
+    store_mask(ez + 2);  // harmless for planes beyond Z1 (never read)
+    load_mask(ez + 3);
+    if (ez + 3 <= Z1) issue_plane(ez + 3);
+    else cp_async_commit();
     const double se = s_next;
     if (ez + 1 < Z1) s_next = load_s(ez + 1);
-    __syncthreads();
-
-    double Ft[3][4], Gn[3][4];
-    face(bt, Ft);
+    double Fb[3][4], Ft[3][4], Gs[3][4];
+    face(ez, Fb);
+    face(ez + 1, Ft);
 #pragma unroll
     for (int c = 0; c < 3; ++c)
 #pragma unroll
-      for (int f = 0; f < 4; ++f) Gn[c][f] = 0.0;
-    hex8_core<double>(kh, se, Fb, Ft, Gp, Gn);  // Gp: plane ez complete, Gn: pending for ez+1
-
+      for (int f = 0; f < 4; ++f) Gs[c][f] = sG[(c * 4 + f) * NT + tid];
+    // classes in pairs (qp, qp^4): after a pair, its three top-face entries are final
+#pragma unroll
+    for (int qp = 0; qp < 4; ++qp) {
+      double gt[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int q = qp + 4 * h;
+        double v[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const int m = member_mode(q, d);
+          const int f = m & 3;
+          v[d] = (m == 0) ? 0.0 : ((m & 4) ? se * (Ft[d][f] - Fb[d][f]) : se * (Ft[d][f] + Fb[d][f]));
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const int m = member_mode(q, c);
+          if (m == 0) continue;
+          const int f = m & 3;
+          double o = 0.0;
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            if (member_mode(q, d) == 0) continue;
+            o = fma(kh.b[q][3 * c + d], v[d], o);
+          }
+          Gs[c][f] += (m & 4) ? -o : o;
+          gt[c] += o;
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) sG[(c * 4 + ((qp ^ (1 << c)) & 3)) * NT + tid] = gt[c];
+    }
     if (ez >= Z0) {
-      double cT[3];
+      double* scb = sc + (size_t)(ez & 1) * 3 * TY * TX;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         double c00, c10, c01, c11;
-        face_inv(Gp[c], c00, c10, c01, c11);
+        face_inv(Gs[c], c00, c10, c01, c11);
         cT[c] = c11 + __shfl_down_sync(0xffffffffu, c01, 1);
-        sc[c][ty][tx] = c10 + __shfl_down_sync(0xffffffffu, c00, 1);
-      }
-      // u of the owned node (for the fused dot) before the exchange barrier
-      double un[3] = {0.0, 0.0, 0.0};
-      if (DOT && owner) {
-        const int bb = (ez - Z0 + 1) & 1;  // buffer of plane ez
-        const int li = (ty + 1) * T::PX + tx + 1;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) un[c] = su[bb][c][li];
-      }
-      __syncthreads();
-      if (owner) {
-        const long long node = (X0 + tx) + (long long)g.sx * (Y0 + ty) + plane_nodes * ez;
-        const int mk = mask_out ? (int)__ldg(mask + node) : 0;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          double v = cT[c] + sc[c][ty + 1][tx];
-          if ((mk >> c) & 1) v = 0.0;
-          y[3 * node + c] = v;
-          if (DOT) dot = fma(un[c], v, dot);
-        }
+        scb[(c * TY + ty) * TX + tx] = c10 + __shfl_down_sync(0xffffffffu, c00, 1);
       }
     }
-#pragma unroll
-    for (int c = 0; c < 3; ++c)
-#pragma unroll
-      for (int f = 0; f < 4; ++f) {
-        Fb[c][f] = Ft[c][f];
-        Gp[c][f] = Gn[c][f];
-      }
   }
+  cp_async_wait0();
+  __syncthreads();
+  if (Z1 - 1 >= Z0) output(Z1 - 1);
   if (DOT) {
-    const double bsum = block_sum<T::NT>(dot, sred);
+    const double bsum = block_sum<NT>(dot, sred);
     double v[1] = {bsum};
     grid_reduce<1>(v, part, counter, (int)(gridDim.x * gridDim.y * gridDim.z),
                    [&](const double* t) { *dot_out = t[0]; });
   }
 }
 
-// launcher used by the entry point and by the solvers
-int launch_matvec64(const pyto_operator_t* op, const double* s, const uint8_t* mask, const double* u, double* y,
-                    int mode, double* part, unsigned* counter, double* dot, cudaStream_t st) {
-  constexpr int TX = 32, TY = 8;
-  const GridDims g = make_dims(op);
-  const KHat kh = make_khat(op);
-  const MvLaunch L = matvec_launch<TX, TY>(g);
-  if (dot)
-    k_matvec64<TX, TY, true><<<L.grid, TX * TY, 0, st>>>(g, kh, s, mask, u, y, L.zc, mode, part, counter, dot);
-  else
-    k_matvec64<TX, TY, false><<<L.grid, TX * TY, 0, st>>>(g, kh, s, mask, u, y, L.zc, mode, nullptr, nullptr,
-                                                          nullptr);
+template <int TY, bool DOT, bool MI, int MINB>
+static int launch_mv_t(const MvLaunch& L, size_t smem, const GridDims& g, const KHat& kh, const double* s,
+                       const uint8_t* mask, const double* u, double* y, int mode, double* part, unsigned* counter,
+                       double* dot, cudaStream_t st) {
+  static bool attr = false;
+  if (!attr) {
+    PYTO_CUDA(cudaFuncSetAttribute(k_matvec64<TY, DOT, MI, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem));
+    attr = true;
+  }
+  k_matvec64<TY, DOT, MI, MINB><<<L.grid, 32 * TY, smem, st>>>(g, kh, s, mask, u, y, L.zc, mode, part, counter, dot);
   PYTO_COUNT(1);
   PYTO_LAUNCH_CHECK();
   return PYTO_OK;
 }
 
-long long matvec_blocks(const pyto_operator_t* op) { return matvec_launch<32, 8>(make_dims(op)).nblocks; }
+template <int TY, int MINB>
+static int launch_mv(const GridDims& g, const KHat& kh, const double* s, const uint8_t* mask, const double* u,
+                     double* y, int mode, double* part, unsigned* counter, double* dot, cudaStream_t st) {
+  const size_t smem = MvSmem<TY>::bytes;
+  const MvLaunch L = matvec_launch<32, TY>(g);
+  const bool mi = (mode & PYTO_MASK_IN) && mask != nullptr;
+  if (dot)
+    return mi ? launch_mv_t<TY, true, true, MINB>(L, smem, g, kh, s, mask, u, y, mode, part, counter, dot, st)
+              : launch_mv_t<TY, true, false, MINB>(L, smem, g, kh, s, mask, u, y, mode, part, counter, dot, st);
+  return mi ? launch_mv_t<TY, false, true, MINB>(L, smem, g, kh, s, mask, u, y, mode, nullptr, nullptr, nullptr, st)
+            : launch_mv_t<TY, false, false, MINB>(L, smem, g, kh, s, mask, u, y, mode, nullptr, nullptr, nullptr, st);
+}
+
+// Tile variant of the FP64 matvec (0 = default):
+//   0: 32x8 threads, 2 CTAs/SM (128 registers)   1: 32x8, 1 CTA/SM (no register cap)
+//   2: 32x4, 3 CTAs/SM                            3: 32x16, 1 CTA/SM
+static int g_mv_variant = 0;
+
+int launch_matvec64(const pyto_operator_t* op, const double* s, const uint8_t* mask, const double* u, double* y,
+                    int mode, double* part, unsigned* counter, double* dot, cudaStream_t st) {
+  const GridDims g = make_dims(op);
+  const KHat kh = make_khat(op);
+  switch (g_mv_variant) {
+    case 1: return launch_mv<8, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
+    case 2: return launch_mv<4, 3>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
+    case 3: return launch_mv<16, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
+    default: return launch_mv<8, 2>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
+  }
+}
+
+// upper bound of the block count over the tile variants (the smallest tile has the most)
+long long matvec_blocks(const pyto_operator_t* op) { return matvec_launch<32, 4>(make_dims(op)).nblocks; }
+
+int set_matvec_variant(int v) {
+  if (v < 0 || v > 3) return PYTO_ERR_ARG;
+  g_mv_variant = v;
+  return PYTO_OK;
+}
 
 // ---------------------------------------------------------------------------
 // BC mask, SIMP, Jacobi

@@ -39,8 +39,10 @@ def main(argv=None):
     ap.add_argument("--nel", default="192,96,96")
     ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--warm", type=int, default=3)
+    ap.add_argument("--variant", type=int, default=0, help="matvec tile variant (pyto_tune)")
     a = ap.parse_args(argv)
     nel = tuple(int(v) for v in a.nel.split(","))
+    A.call("pyto_tune", 0, a.variant)
     mesh = HexMesher()
     mesh.grid_mesh(nel, (1.0, 1.0, 1.0))
     f, fixed = cantilever(mesh)
@@ -61,7 +63,7 @@ def main(argv=None):
     else:
         fn, nbytes = (lambda: g.stress(u, s, 0.5, want=("vm",))), 24 * g.nnodes + 16 * g.nelem
     t = _timeit(fn, a.reps, a.warm)
-    print(json.dumps({"kernel": a.kernel, "nel": nel, "ms": t * 1e3, "algorithmic_bytes": int(nbytes),
+    print(json.dumps({"kernel": a.kernel, "variant": a.variant, "nel": nel, "ms": t * 1e3, "algorithmic_bytes": int(nbytes),
                       "GB_s": nbytes / t / 1e9}))
 
 

@@ -52,6 +52,30 @@ def test_matvec_matches_assembled_K(nel, h, masked):
     assert abs(dot.item() - uu @ yref) <= 1e-12 * abs(uu @ yref)
 
 
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("nel", [(33, 9, 17), (7, 20, 5), (70, 11, 30)])
+def test_matvec_tile_variants(variant, nel):
+    from pyto_b200 import _capi as A
+    rng = np.random.default_rng(7)
+    m = O.grid_mesh(*nel)
+    s = rng.uniform(0.01, 1.0, m["num_elems"])
+    u = rng.normal(size=3 * m["num_nodes"])
+    f, fixed = O.cantilever_bc(m)
+    yref = O.matvec_free(m, s, O.ke_hex8(1.0, 0.3), u, fixed)
+    uu = u.copy()
+    uu[fixed] = 0
+    g = _grid(nel, fixed=fixed)
+    try:
+        A.call("pyto_tune", 0, variant)
+        for mode in (3, 2):  # masked input / unmasked input with zeroed fixed entries
+            uin = u if mode == 3 else uu
+            y, dot = g.matvec(_dev(s), _dev(uin), mode=mode, dot=True)
+            assert np.abs(y.cpu().numpy() - yref).max() <= 1e-13 * np.abs(yref).max()
+            assert abs(dot.item() - uu @ yref) <= 1e-12 * abs(uu @ yref)
+    finally:
+        A.call("pyto_tune", 0, 0)
+
+
 def test_matvec_bitwise_deterministic():
     nel = (40, 20, 20)
     rng = np.random.default_rng(2)
