@@ -35,7 +35,8 @@ def _timeit(fn, reps, warm=3):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--kernel", default="matvec", choices=["matvec", "energy", "filter", "jacobi", "stress"])
+    ap.add_argument("--kernel", default="matvec", choices=["matvec", "energy", "filter", "jacobi", "stress", "dpcg", "pcg"])
+    ap.add_argument("--groups", type=int, default=432, help="deflation groups for --kernel dpcg")
     ap.add_argument("--nel", default="192,96,96")
     ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--warm", type=int, default=3)
@@ -60,9 +61,25 @@ def main(argv=None):
         fn, nbytes = (lambda: g.filter(2.0, A.FILTER_DENSITY, s, out=out)), 16 * g.nelem
     elif a.kernel == "jacobi":
         fn, nbytes = (lambda: g.jacobi(s)), 8 * g.nelem + 33 * g.nnodes
+    elif a.kernel in ("dpcg", "pcg"):
+        from .deflation import DeflationSolver
+        F = g.tensor(f)
+        if a.kernel == "dpcg":
+            ds = DeflationSolver(shift=1e-14, shift_relative=True)
+            ds.create_deflation_groups(mesh, a.groups)
+            defl = ds.device_deflation(g)
+            fn = lambda: g.dpcg(s, F, defl, rtol=1e-8, max_iters=5000, stop_rule=0, check_every=20)
+        else:
+            fn = lambda: g.pcg(s, F, rtol=1e-8, check_every=20)
+        nbytes = 0
     else:
         fn, nbytes = (lambda: g.stress(u, s, 0.5, want=("vm",))), 24 * g.nnodes + 16 * g.nelem
     t = _timeit(fn, a.reps, a.warm)
+    if a.kernel in ("dpcg", "pcg"):
+        _, info = fn()
+        print(json.dumps({"kernel": a.kernel, "nel": nel, "ms": t * 1e3, "iters": info.iters,
+                          "true_rel_res": info.true_rel_res}))
+        return
     print(json.dumps({"kernel": a.kernel, "variant": a.variant, "nel": nel, "ms": t * 1e3, "algorithmic_bytes": int(nbytes),
                       "GB_s": nbytes / t / 1e9}))
 
