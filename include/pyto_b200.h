@@ -148,6 +148,15 @@ int pyto_bc_mask(const pyto_operator_t* op, const int64_t* fixed_dofs, int64_t n
  * src/linear_solvers.py:136-202). */
 int pyto_matvec(const pyto_operator_t* op, const double* s, const uint8_t* mask, const double* u,
                 double* y, int mode, double* dot, void* ws, size_t ws_bytes, void* stream);
+/* pyto_matvec with a non-NULL dot, for callers that cannot allocate device memory
+ * (plugins whose host owns every allocation, loops where allocation is forbidden after
+ * start-up).  No counterpart in the reference.  The cross-block scratch is a fixed
+ * array inside the library (~64 KB held on every GPU that loads it until process
+ * exit); launches needing more than 8192 matvec blocks return PYTO_ERR_TOO_LARGE.  The
+ * first call on a device looks up the array's device address and should precede any
+ * stream capture; calls that overlap on the GPU race on the shared array. */
+int pyto_matvec_dot_noalloc(const pyto_operator_t* op, const double* s, const uint8_t* mask,
+                            const double* u, double* y, int mode, double* dot, void* stream);
 /* Jacobi data: diag(K)[3n+c] = kdiag[c] * sum_{e ni n} s_e.  Writes winv[n] = 1/sum s
  * and flags[n] = mask bits | (clamp bits << 3), clamp bit c set when |diag| < 1e-12 (then
  * the preconditioner is 1, src/linear_solvers.py:71-87).  diag_out (may be NULL) gets the

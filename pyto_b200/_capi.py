@@ -72,6 +72,7 @@ SIGNATURES = {
     "pyto_bc_mask": (C.c_int, [_OP, _P, C.c_int64, _P, _P]),
     "pyto_matvec": (C.c_int, [_OP, _P, _P, _P, _P, C.c_int, _P, _P, C.c_size_t, _P]),
     "pyto_jacobi": (C.c_int, [_OP, _P, _P, _P, _P, _P, _P]),
+    "pyto_matvec_dot_noalloc": (C.c_int, [_OP, _P, _P, _P, _P, C.c_int, _P, _P]),
     "pyto_pcg_solve": (C.c_int, [_OP, _P, _P, _P, _P, C.POINTER(SolveCfg), C.POINTER(SolveStatus), _P, C.c_size_t,
                                  _P]),
     "pyto_dpcg_setup": (C.c_int, [_OP, _P, _P, C.POINTER(Deflation), _P, C.c_size_t, _P]),
