@@ -96,6 +96,12 @@ typedef struct pyto_deflation {
   double* coarse_inv;          /* [nc*nc], nc = ngroups*modes: written by pyto_dpcg_setup */
   double shift;                /* diagonal shift added to W^T K W */
   int32_t shift_relative;      /* 1: shift scales the mean diagonal; 0: absolute (PyTO: 1e-10) */
+  int32_t max_group_nodes;     /* largest group (nodes) */
+  const int32_t* group_box;    /* [ngroups*6] element index box touching the group:
+                                  ex0,ex1,ey0,ey1,ez0,ez1 (inclusive) */
+  const int32_t* nbr_ptr;      /* [ngroups+1] CSR offsets of nbr_list */
+  const int32_t* nbr_list;     /* groups sharing an element with each group (incl. itself), ascending */
+  int32_t max_nbr;             /* largest neighbour list (<= 128) */
   int32_t reserved;
 } pyto_deflation_t;
 

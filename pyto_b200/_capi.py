@@ -55,7 +55,9 @@ class SolveStatus(C.Structure):
 class Deflation(C.Structure):
     _fields_ = [("ngroups", C.c_int32), ("modes", C.c_int32), ("node_group", C.c_void_p), ("group_ptr", C.c_void_p),
                 ("group_nodes", C.c_void_p), ("group_center", C.c_void_p), ("coarse_inv", C.c_void_p),
-                ("shift", C.c_double), ("shift_relative", C.c_int32), ("reserved", C.c_int32)]
+                ("shift", C.c_double), ("shift_relative", C.c_int32), ("max_group_nodes", C.c_int32),
+                ("group_box", C.c_void_p), ("nbr_ptr", C.c_void_p), ("nbr_list", C.c_void_p), ("max_nbr", C.c_int32),
+                ("reserved", C.c_int32)]
 
 
 _P = C.c_void_p

@@ -11,7 +11,8 @@
 // W[free_dofs] in src/linear_solvers.py:184).  Rigid modes lie in the null
 // space of every element matrix, so only elements whose corners span two or
 // more groups (or touch a fixed DOF) contribute; each such element adds
-// s_e (Phi M_j)^T K^ (Phi M_i) to block (g_j, g_i) with FP64 atomics.
+// s_e (Phi M_g)^T K^ (Phi M_h) to block (g, h).  Row blocks are accumulated
+// per group in shared memory and written once (no global atomics).
 //
 // E^-1 is formed explicitly (dense, FP64) by a blocked in-place sweep
 // (Gauss-Jordan on the SPD matrix, 64x64 pivot blocks); each DPCG iteration
@@ -85,44 +86,68 @@ __device__ __forceinline__ void mode_hat(const GridDims& g, const DeflP& dp, con
 // ---------------------------------------------------------------------------
 // coarse matrix assembly
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_coarse_assemble(GridDims g, KHat kh, DeflP dp, const double* __restrict__ s,
-                                                         const uint8_t* __restrict__ mask,
-                                                         const int32_t* __restrict__ ngrp,
-                                                         const double* __restrict__ gc, double* __restrict__ E) {
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < g.nelem;
-       e += (long long)gridDim.x * blockDim.x) {
+// Row block E[g, :] of one group per CTA (no global atomics): the CTA visits
+// the elements touching group g; for each element with corners outside g (or
+// on fixed DOFs) it adds s_e (Phi M_g)^T K^ (Phi M_h) for every corner group h
+// into a shared-memory accumulator (one 6x6 slot per neighbour group), then
+// writes its row blocks.  Every block of E is written by exactly one CTA.
+constexpr int kAsmThreads = 128;
+__global__ void __launch_bounds__(kAsmThreads) k_coarse_rows(GridDims g, KHat kh, DeflP dp,
+                                                            const double* __restrict__ s,
+                                                            const uint8_t* __restrict__ mask,
+                                                            const int32_t* __restrict__ ngrp,
+                                                            const double* __restrict__ gc,
+                                                            const int32_t* __restrict__ gbox,
+                                                            const int32_t* __restrict__ nptr,
+                                                            const int32_t* __restrict__ nlist,
+                                                            double* __restrict__ E) {
+  extern __shared__ double acc[];  // [nnbr][36]
+  __shared__ int snb[128];
+  const int G = blockIdx.x;
+  const int nb0 = nptr[G], nnb = nptr[G + 1] - nb0;
+  for (int t = threadIdx.x; t < nnb; t += blockDim.x) snb[t] = nlist[nb0 + t];
+  for (int t = threadIdx.x; t < nnb * 36; t += blockDim.x) acc[t] = 0.0;
+  __syncthreads();
+  const int* bx = gbox + 6 * G;
+  const int ex0 = bx[0], ey0 = bx[2], ez0 = bx[4];
+  const int lx = bx[1] - ex0 + 1, ly = bx[3] - ey0 + 1, lz = bx[5] - ez0 + 1;
+  const long long nvis = (long long)lx * ly * lz;
+  for (long long t = threadIdx.x; t < nvis; t += blockDim.x) {
+    const int ex = ex0 + (int)(t % lx);
+    const int ey = ey0 + (int)((t / lx) % ly);
+    const int ez = ez0 + (int)(t / ((long long)lx * ly));
+    const long long e = ex + (long long)g.nx * (ey + (long long)g.ny * ez);
     const double se = s[e];
     if (se == 0.0) continue;
-    const int ex = (int)(e % g.nx);
-    const long long rr = e / g.nx;
-    const int ey = (int)(rr % g.ny);
-    const int ez = (int)(rr / g.ny);
     long long nd[8];
     int gr[8], mk[8];
-    bool need = false;
+    bool mine = false, other = false;
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-      const int bx = k & 1, by = (k >> 1) & 1, bz = k >> 2;
-      nd[k] = (ex + bx) + (long long)g.sx * ((ey + by) + (long long)g.sy * (ez + bz));
+      const int bxk = k & 1, byk = (k >> 1) & 1, bzk = k >> 2;
+      nd[k] = (ex + bxk) + (long long)g.sx * ((ey + byk) + (long long)g.sy * (ez + bzk));
       gr[k] = ngrp[nd[k]];
       mk[k] = mask ? (mask[nd[k]] & 7) : 0;
-      if (mk[k] || gr[k] != gr[0]) need = true;
+      mine |= (gr[k] == G);
+      other |= (gr[k] != G) || (mk[k] != 0);
     }
-    if (!need) continue;
-    int G[8], ng = 0;
+    if (!mine || !other) continue;
+    double Hg[6][3][8];
+    for (int a = 0; a < dp.modes; ++a) mode_hat(g, dp, nd, gr, mk, G, gc, a, Hg[a]);
+    int H[8], nh = 0;
     for (int k = 0; k < 8; ++k) {
       bool seen = false;
-      for (int t = 0; t < ng; ++t) seen |= (G[t] == gr[k]);
-      if (!seen) G[ng++] = gr[k];
+      for (int t2 = 0; t2 < nh; ++t2) seen |= (H[t2] == gr[k]);
+      if (!seen) H[nh++] = gr[k];
     }
-    for (int i = 0; i < ng; ++i) {
-      // Z_i[b] = s K^ Phi M_i[b]
-      double Zi[6][3][8];
+    for (int hi = 0; hi < nh; ++hi) {
+      const int h = H[hi];
+      int slot = 0;
+      while (slot < nnb && snb[slot] != h) ++slot;
+      if (slot == nnb) continue;  // not possible for a consistent neighbour list
       for (int b = 0; b < dp.modes; ++b) {
-        double H[3][8];
-        mode_hat(g, dp, nd, gr, mk, G[i], gc, b, H);
-        for (int c = 0; c < 3; ++c)
-          for (int m = 0; m < 8; ++m) Zi[b][c][m] = 0.0;
+        double Hh[3][8], Z[3][8];
+        mode_hat(g, dp, nd, gr, mk, h, gc, b, Hh);
         for (int q = 0; q < 8; ++q)
           for (int c = 0; c < 3; ++c) {
             const int m = member_mode(q, c);
@@ -131,25 +156,24 @@ __global__ void __launch_bounds__(128) k_coarse_assemble(GridDims g, KHat kh, De
             for (int d = 0; d < 3; ++d) {
               const int n = member_mode(q, d);
               if (n == 0) continue;
-              o = fma(kh.b[q][3 * c + d], H[d][n], o);
+              o = fma(kh.b[q][3 * c + d], Hh[d][n], o);
             }
-            Zi[b][c][m] = se * o;
+            Z[c][m] = se * o;
           }
-      }
-      for (int j = 0; j < ng; ++j) {
         for (int a = 0; a < dp.modes; ++a) {
-          double H[3][8];
-          mode_hat(g, dp, nd, gr, mk, G[j], gc, a, H);
-          const long long row = (long long)G[j] * dp.modes + a;
-          for (int b = 0; b < dp.modes; ++b) {
-            double v = 0.0;
-            for (int c = 0; c < 3; ++c)
-              for (int m = 1; m < 8; ++m) v = fma(H[c][m], Zi[b][c][m], v);
-            if (v != 0.0) atomicAdd(E + row * dp.nc + (long long)G[i] * dp.modes + b, v);
-          }
+          double v = 0.0;
+          for (int c = 0; c < 3; ++c)
+            for (int m = 1; m < 8; ++m) v = fma(Hg[a][c][m], Z[c][m], v);
+          if (v != 0.0) atomicAdd(&acc[slot * 36 + a * 6 + b], v);
         }
       }
     }
+  }
+  __syncthreads();
+  const int M = dp.modes;
+  for (int t = threadIdx.x; t < nnb * M * M; t += blockDim.x) {
+    const int slot = t / (M * M), a = (t / M) % M, b = t % M;
+    E[((long long)G * M + a) * dp.nc + (long long)snb[slot] * M + b] = acc[slot * 36 + a * 6 + b];
   }
 }
 
@@ -183,32 +207,33 @@ __global__ void k_coarse_finish(long long nc, double* E, double shift, const dou
 // blocked sweep inversion: after all pivot blocks A = -E^-1
 //   P = A_KK^-1, U = P A_K:, A_ij -= A_iK U_Kj, A_Kj = U_Kj, A_iK = U_Ki^T, A_KK = -P
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_sweep_pivot(long long n, int k0, int bk, const double* __restrict__ A,
-                                                     double* __restrict__ P) {
+__global__ void __launch_bounds__(1024) k_sweep_pivot(long long n, int k0, int bk, const double* __restrict__ A,
+                                                      double* __restrict__ P) {
   __shared__ double M[kSweepB][kSweepB + 1];
   for (int t = threadIdx.x; t < kSweepB * kSweepB; t += blockDim.x) {
     const int i = t / kSweepB, j = t % kSweepB;
     M[i][j] = (i < bk && j < bk) ? A[(k0 + i) * n + (k0 + j)] : (i == j ? 1.0 : 0.0);
   }
   __syncthreads();
-  // in-place sweep of the small block: result -M^-1
+  // in-place sweep of the small block (result -M^-1): each thread owns 4 entries
   for (int p = 0; p < bk; ++p) {
+    double nv[4];
     const double piv = M[p][p];
-    __syncthreads();
-    for (int t = threadIdx.x; t < kSweepB * kSweepB; t += blockDim.x) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int t = threadIdx.x + r * 1024;
       const int i = t / kSweepB, j = t % kSweepB;
-      if (i == p || j == p) continue;
-      M[i][j] -= M[i][p] * M[p][j] / piv;
+      if (i == p && j == p) nv[r] = -1.0 / piv;
+      else if (i == p) nv[r] = M[p][j] / piv;
+      else if (j == p) nv[r] = M[i][p] / piv;
+      else nv[r] = M[i][j] - M[i][p] * M[p][j] / piv;
     }
     __syncthreads();
-    for (int t = threadIdx.x; t < kSweepB; t += blockDim.x) {
-      if (t != p) {
-        M[t][p] = M[t][p] / piv;
-        M[p][t] = M[p][t] / piv;
-      }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int t = threadIdx.x + r * 1024;
+      M[t / kSweepB][t % kSweepB] = nv[r];
     }
-    __syncthreads();
-    if (threadIdx.x == 0) M[p][p] = -1.0 / piv;
     __syncthreads();
   }
   for (int t = threadIdx.x; t < kSweepB * kSweepB; t += blockDim.x) {
@@ -310,17 +335,24 @@ __global__ void k_negate(long long n, double* A) {
 // ---------------------------------------------------------------------------
 // DPCG pieces
 // ---------------------------------------------------------------------------
-// v = W_f^T y (one warp per group, nodes in CSR order -> deterministic)
+// v = W_f^T y.  Block (group, chunk) reduces up to kRestrictChunk nodes of one
+// group (CSR order) to 6 partials; the last block to finish sums each group's
+// chunk partials in chunk order, so the result does not depend on scheduling.
+constexpr int kRestrictChunk = 2048;
+constexpr int kRestrictMaxBlocks = 65536;
 __global__ void __launch_bounds__(256) k_restrict(GridDims g, DeflP dp, const int32_t* __restrict__ gptr,
                                                   const int32_t* __restrict__ gnodes, const double* __restrict__ gc,
                                                   const uint8_t* __restrict__ fl, const double* __restrict__ y,
+                                                  int nch, double* __restrict__ part, unsigned* counter,
                                                   double* __restrict__ v) {
-  const int lane = threadIdx.x & 31;
-  const long long grp = (long long)blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
-  if (grp >= dp.ngroups) return;
+  __shared__ double sred[8];
+  __shared__ bool s_last;
+  const int grp = blockIdx.x / nch, ch = blockIdx.x % nch;
+  const int beg = gptr[grp] + ch * kRestrictChunk;
+  const int end = min(gptr[grp + 1], beg + kRestrictChunk);
   const double cx = gc[3 * grp], cy = gc[3 * grp + 1], cz = gc[3 * grp + 2];
   double acc[6] = {0, 0, 0, 0, 0, 0};
-  for (int t = gptr[grp] + lane; t < gptr[grp + 1]; t += 32) {
+  for (int t = beg + threadIdx.x; t < end; t += blockDim.x) {
     const long long n = gnodes[t];
     double x, yy, z;
     node_xyz(g, n, dp.hx, dp.hy, dp.hz, x, yy, z);
@@ -334,12 +366,24 @@ __global__ void __launch_bounds__(256) k_restrict(GridDims g, DeflP dp, const in
     acc[4] += rz * vx - rx * vz;
     acc[5] += -ry * vx + rx * vy;
   }
-#pragma unroll
-  for (int a = 0; a < 6; ++a)
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc[a] += __shfl_xor_sync(0xffffffffu, acc[a], o);
-  if (lane == 0)
-    for (int a = 0; a < dp.modes; ++a) v[grp * dp.modes + a] = acc[a];
+  for (int a = 0; a < dp.modes; ++a) {
+    const double t = block_sum<256>(acc[a], sred);
+    if (threadIdx.x == 0) part[(size_t)blockIdx.x * 6 + a] = t;
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = (atomicAdd(counter, 1u) == gridDim.x - 1u);
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  for (int i = threadIdx.x; i < dp.ngroups * dp.modes; i += blockDim.x) {
+    const int gg = i / dp.modes, a = i % dp.modes;
+    double t = 0.0;
+    for (int c = 0; c < nch; ++c) t += __ldcg(part + ((size_t)gg * nch + c) * 6 + a);
+    v[i] = t;
+  }
+  if (threadIdx.x == 0) *counter = 0u;
 }
 
 // mu = Einv v (one warp per row, v staged in shared memory)
@@ -557,6 +601,8 @@ struct DpcgWs {
   double *r, *p, *q, *z, *w;
   uint8_t* fl;
   double *cv, *mu;     // coarse vectors
+  double* rpart;       // restriction partials
+  unsigned* rcounter;
   double *P, *Rp, *U;  // sweep scratch
 };
 
@@ -575,6 +621,8 @@ static DpcgWs carve_dpcg(const pyto_operator_t* op, long long nc, void* ws, size
   W.z = cv.take<double>(3 * g.nnodes);
   W.w = cv.take<double>(g.nnodes);
   W.fl = cv.take<uint8_t>(g.nnodes);
+  W.rcounter = cv.take<unsigned>(64);
+  W.rpart = cv.take<double>((size_t)6 * kRestrictMaxBlocks);
   W.cv = cv.take<double>(nc > 0 ? nc : 1);
   W.mu = cv.take<double>(nc > 0 ? nc : 1);
   W.P = cv.take<double>(kSweepB * kSweepB);
@@ -602,15 +650,20 @@ static DeflP make_deflp(const pyto_operator_t* op, const pyto_deflation_t* d) {
 }
 
 static bool defl_ok(const pyto_deflation_t* d) {
-  return d && d->ngroups > 0 && (d->modes == 3 || d->modes == 6) && d->node_group && d->group_ptr &&
-         d->group_nodes && d->group_center && d->coarse_inv;
+  if (!(d && d->ngroups > 0 && (d->modes == 3 || d->modes == 6) && d->node_group && d->group_ptr &&
+        d->group_nodes && d->group_center && d->coarse_inv && d->group_box && d->nbr_ptr && d->nbr_list &&
+        d->max_group_nodes > 0 && d->max_nbr > 0 && d->max_nbr <= 128))
+    return false;
+  const long long nch = (d->max_group_nodes + kRestrictChunk - 1) / kRestrictChunk;
+  return (long long)d->ngroups * nch <= kRestrictMaxBlocks;
 }
 
 // mu = Einv W_f^T y
 static int coarse_solve(const GridDims& g, const DeflP& dp, const pyto_deflation_t* d, const double* y,
                         const DpcgWs& W, const KrylovState* S, cudaStream_t st) {
-  k_restrict<<<(dp.ngroups + 7) / 8, 256, 0, st>>>(g, dp, d->group_ptr, d->group_nodes, d->group_center, W.fl, y,
-                                                   W.cv);
+  const int nch = (d->max_group_nodes + kRestrictChunk - 1) / kRestrictChunk;
+  k_restrict<<<dp.ngroups * nch, 256, 0, st>>>(g, dp, d->group_ptr, d->group_nodes, d->group_center, W.fl, y, nch,
+                                               W.rpart, W.rcounter, W.cv);
   PYTO_COUNT(1);
   const size_t shm = (size_t)dp.nc * sizeof(double);
   const int nb = (int)std::min<long long>((dp.nc + 7) / 8, 4 * kNumSMs);
@@ -648,9 +701,13 @@ extern "C" int pyto_dpcg_setup(const pyto_operator_t* op, const double* s, const
   double* E = defl->coarse_inv;
   const long long n = dp.nc;
   PYTO_CUDA(cudaMemsetAsync(E, 0, (size_t)n * n * sizeof(double), st));
-  k_coarse_assemble<<<(int)std::min<long long>((g.nelem + 127) / 128, 16 * kNumSMs), 128, 0, st>>>(
-      g, make_khat(op), dp, s, mask, defl->node_group, defl->group_center, E);
-  PYTO_COUNT(1);
+  {
+    const size_t shm = (size_t)defl->max_nbr * 36 * sizeof(double);
+    k_coarse_rows<<<dp.ngroups, kAsmThreads, shm, st>>>(g, make_khat(op), dp, s, mask, defl->node_group,
+                                                         defl->group_center, defl->group_box, defl->nbr_ptr,
+                                                         defl->nbr_list, E);
+    PYTO_COUNT(1);
+  }
   if (defl->shift_relative) {
     k_diag_mean<<<1, 256, 0, st>>>(n, E, W.part);
     PYTO_COUNT(1);
@@ -662,7 +719,7 @@ extern "C" int pyto_dpcg_setup(const pyto_operator_t* op, const double* s, const
   const int tiles = (int)((n + 63) / 64);
   for (long long k0 = 0; k0 < n; k0 += kSweepB) {
     const int bk = (int)std::min<long long>(kSweepB, n - k0);
-    k_sweep_pivot<<<1, 256, 0, st>>>(n, (int)k0, bk, E, W.P);
+    k_sweep_pivot<<<1, 1024, 0, st>>>(n, (int)k0, bk, E, W.P);
     PYTO_COUNT(1);
     k_sweep_panel<<<(int)((n + 15) / 16), 256, 0, st>>>(n, (int)k0, bk, E, W.P, W.Rp, W.U);
     PYTO_COUNT(1);
@@ -691,6 +748,7 @@ extern "C" int pyto_dpcg_solve(const pyto_operator_t* op, const double* s, const
   const Prec pc = make_prec(op);
   const int mm = PYTO_MASK_IN | PYTO_MASK_OUT;
   PYTO_CUDA(cudaMemsetAsync(W.counter, 0, 64 * sizeof(unsigned), st));
+  PYTO_CUDA(cudaMemsetAsync(W.rcounter, 0, 64 * sizeof(unsigned), st));
   k_state_init2<<<1, 1, 0, st>>>(W.S, cfg->rtol, cfg->max_iters, cfg->stop_rule);
   PYTO_COUNT(1);
   rc = pyto_jacobi(op, s, mask, W.w, W.fl, nullptr, stream);

@@ -206,7 +206,13 @@ class HexGrid:
 
 
 class DeviceDeflation:
-    """Device data of a deflation space (node groups + rigid modes)."""
+    """Device data of a deflation space (node groups + rigid modes).
+
+    Besides the node->group map, the CSR of nodes per group and the group
+    centres, set-up derives once per mesh: the box of elements touching each
+    group and, per group, the sorted list of groups sharing an element with it
+    (the non-zero block pattern of W^T K W).
+    """
 
     def __init__(self, grid: HexGrid, node_group, centers, modes=6, shift=1e-10, shift_relative=False):
         node_group = np.asarray(node_group, dtype=np.int32).ravel()
@@ -215,14 +221,45 @@ class DeviceDeflation:
         order = np.argsort(node_group, kind="stable").astype(np.int32)
         counts = np.bincount(node_group, minlength=ng)
         gptr = np.concatenate([[0], np.cumsum(counts)]).astype(np.int32)
+        nx, ny, nz = grid.nel
+        sx, sy = nx + 1, ny + 1
+        n = np.arange(node_group.size)
+        ix, iy, iz = n % sx, (n // sx) % sy, n // (sx * sy)
+        box = np.zeros((ng, 6), dtype=np.int32)
+        for d, (coord, ne) in enumerate(((ix, nx), (iy, ny), (iz, nz))):
+            lo = np.full(ng, np.iinfo(np.int64).max)
+            hi = np.full(ng, -1)
+            np.minimum.at(lo, node_group, coord)
+            np.maximum.at(hi, node_group, coord)
+            box[:, 2 * d] = np.clip(lo - 1, 0, ne - 1)
+            box[:, 2 * d + 1] = np.clip(hi, 0, ne - 1)
+        # group pairs sharing an element: corners of every element
+        ez, ey, ex = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+        n0 = (ex + sx * (ey + sy * ez)).ravel()
+        pairs = []
+        corner = [0, 1, sx, sx + 1, sx * sy, sx * sy + 1, sx * sy + sx, sx * sy + sx + 1]
+        cg = np.stack([node_group[n0 + c] for c in corner], 1)
+        for a in range(8):
+            for b in range(8):
+                pairs.append(cg[:, a].astype(np.int64) * ng + cg[:, b])
+        key = np.unique(np.concatenate(pairs))
+        ga, gb = (key // ng).astype(np.int32), (key % ng).astype(np.int32)
+        nptr = np.concatenate([[0], np.cumsum(np.bincount(ga, minlength=ng))]).astype(np.int32)
+        self.max_nbr = int(np.diff(nptr).max())
+        if self.max_nbr > 128:
+            raise ValueError(f"a deflation group touches {self.max_nbr} groups (limit 128)")
         dev = grid.device
         self.node_group = torch.as_tensor(node_group, device=dev)
         self.group_ptr = torch.as_tensor(gptr, device=dev)
         self.group_nodes = torch.as_tensor(order, device=dev)
         self.group_center = torch.as_tensor(np.ascontiguousarray(centers), device=dev)
+        self.group_box = torch.as_tensor(np.ascontiguousarray(box), device=dev)
+        self.nbr_ptr = torch.as_tensor(nptr, device=dev)
+        self.nbr_list = torch.as_tensor(gb, device=dev)
         self.ngroups, self.modes = ng, int(modes)
         self.nc = ng * self.modes
         self.coarse_inv = torch.empty(self.nc * self.nc, dtype=F64, device=dev)
         self.struct = A.Deflation(ng, self.modes, A.ptr(self.node_group), A.ptr(self.group_ptr),
                                   A.ptr(self.group_nodes), A.ptr(self.group_center), A.ptr(self.coarse_inv),
-                                  float(shift), 1 if shift_relative else 0, 0)
+                                  float(shift), 1 if shift_relative else 0, int(counts.max()), A.ptr(self.group_box),
+                                  A.ptr(self.nbr_ptr), A.ptr(self.nbr_list), self.max_nbr, 0)
