@@ -26,12 +26,14 @@ namespace pyto {
 
 constexpr int kSweepB = 64;
 
+// node ids fit in int32 (checked by pyto_operator_init), so 32-bit division suffices
 __device__ __forceinline__ void node_xyz(const GridDims& g, long long n, double hx, double hy, double hz, double& x,
                                          double& y, double& z) {
-  const int ix = (int)(n % g.sx);
-  const long long r = n / g.sx;
-  const int iy = (int)(r % g.sy);
-  const int iz = (int)(r / g.sy);
+  const int ni = (int)n;
+  const int r = ni / g.sx;
+  const int ix = ni - r * g.sx;
+  const int iz = r / g.sy;
+  const int iy = r - iz * g.sy;
   x = hx * ix;
   y = hy * iy;
   z = hz * iz;
@@ -57,25 +59,25 @@ struct DeflP {
 };
 
 // Hadamard transform of the restriction of mode a of group G to the element's
-// corners (zero at corners of other groups and at fixed DOFs)
-__device__ __forceinline__ void mode_hat(const GridDims& g, const DeflP& dp, const long long (&nd)[8],
-                                         const int (&gr)[8], const int (&mk)[8], int G, const double* __restrict__ gc,
-                                         int a, double (&H)[3][8]) {
+// corners (zero at corners of other groups and at fixed DOFs); xyz: corner
+// coordinates in bit order
+__device__ __forceinline__ void mode_hat(const double (&xyz)[8][3], const int (&gr)[8], const int (&mk)[8], int G,
+                                         const double* __restrict__ gc, int a, double (&H)[3][8]) {
+  const double c0 = gc[3 * (long long)G], c1 = gc[3 * (long long)G + 1], c2 = gc[3 * (long long)G + 2];
   double A[3][8];
+#pragma unroll
   for (int k = 0; k < 8; ++k) {
     double w[3] = {0.0, 0.0, 0.0};
-    if (gr[k] == G) {
-      double x, y, z;
-      node_xyz(g, nd[k], dp.hx, dp.hy, dp.hz, x, y, z);
-      const double* c = gc + 3 * (long long)G;
-      rigid_mode(a, x - c[0], y - c[1], z - c[2], w);
-    }
+    if (gr[k] == G) rigid_mode(a, xyz[k][0] - c0, xyz[k][1] - c1, xyz[k][2] - c2, w);
+#pragma unroll
     for (int c = 0; c < 3; ++c) A[c][k] = ((mk[k] >> c) & 1) ? 0.0 : w[c];
   }
+#pragma unroll
   for (int c = 0; c < 3; ++c) {
     double Fb[4], Ft[4];
     face_fwd(A[c][0], A[c][1], A[c][2], A[c][3], Fb);
     face_fwd(A[c][4], A[c][5], A[c][6], A[c][7], Ft);
+#pragma unroll
     for (int f = 0; f < 4; ++f) {
       H[c][f] = Ft[f] + Fb[f];
       H[c][f + 4] = Ft[f] - Fb[f];
@@ -91,7 +93,7 @@ __device__ __forceinline__ void mode_hat(const GridDims& g, const DeflP& dp, con
 // on fixed DOFs) it adds s_e (Phi M_g)^T K^ (Phi M_h) for every corner group h
 // into a shared-memory accumulator (one 6x6 slot per neighbour group), then
 // writes its row blocks.  Every block of E is written by exactly one CTA.
-constexpr int kAsmThreads = 128;
+constexpr int kAsmThreads = 256;
 __global__ void __launch_bounds__(kAsmThreads) k_coarse_rows(GridDims g, KHat kh, DeflP dp,
                                                             const double* __restrict__ s,
                                                             const uint8_t* __restrict__ mask,
@@ -119,21 +121,24 @@ __global__ void __launch_bounds__(kAsmThreads) k_coarse_rows(GridDims g, KHat kh
     const long long e = ex + (long long)g.nx * (ey + (long long)g.ny * ez);
     const double se = s[e];
     if (se == 0.0) continue;
-    long long nd[8];
     int gr[8], mk[8];
+    double xyz[8][3];
     bool mine = false, other = false;
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
       const int bxk = k & 1, byk = (k >> 1) & 1, bzk = k >> 2;
-      nd[k] = (ex + bxk) + (long long)g.sx * ((ey + byk) + (long long)g.sy * (ez + bzk));
-      gr[k] = ngrp[nd[k]];
-      mk[k] = mask ? (mask[nd[k]] & 7) : 0;
+      const long long nd = (ex + bxk) + (long long)g.sx * ((ey + byk) + (long long)g.sy * (ez + bzk));
+      gr[k] = ngrp[nd];
+      mk[k] = mask ? (mask[nd] & 7) : 0;
+      xyz[k][0] = dp.hx * (ex + bxk);
+      xyz[k][1] = dp.hy * (ey + byk);
+      xyz[k][2] = dp.hz * (ez + bzk);
       mine |= (gr[k] == G);
       other |= (gr[k] != G) || (mk[k] != 0);
     }
     if (!mine || !other) continue;
     double Hg[6][3][8];
-    for (int a = 0; a < dp.modes; ++a) mode_hat(g, dp, nd, gr, mk, G, gc, a, Hg[a]);
+    for (int a = 0; a < dp.modes; ++a) mode_hat(xyz, gr, mk, G, gc, a, Hg[a]);
     int H[8], nh = 0;
     for (int k = 0; k < 8; ++k) {
       bool seen = false;
@@ -147,7 +152,7 @@ __global__ void __launch_bounds__(kAsmThreads) k_coarse_rows(GridDims g, KHat kh
       if (slot == nnb) continue;  // not possible for a consistent neighbour list
       for (int b = 0; b < dp.modes; ++b) {
         double Hh[3][8], Z[3][8];
-        mode_hat(g, dp, nd, gr, mk, h, gc, b, Hh);
+        mode_hat(xyz, gr, mk, h, gc, b, Hh);
         for (int q = 0; q < 8; ++q)
           for (int c = 0; c < 3; ++c) {
             const int m = member_mode(q, c);
@@ -218,15 +223,15 @@ __global__ void __launch_bounds__(1024) k_sweep_pivot(long long n, int k0, int b
   // in-place sweep of the small block (result -M^-1): each thread owns 4 entries
   for (int p = 0; p < bk; ++p) {
     double nv[4];
-    const double piv = M[p][p];
+    const double ipiv = 1.0 / M[p][p];
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
       const int t = threadIdx.x + r * 1024;
       const int i = t / kSweepB, j = t % kSweepB;
-      if (i == p && j == p) nv[r] = -1.0 / piv;
-      else if (i == p) nv[r] = M[p][j] / piv;
-      else if (j == p) nv[r] = M[i][p] / piv;
-      else nv[r] = M[i][j] - M[i][p] * M[p][j] / piv;
+      if (i == p && j == p) nv[r] = -ipiv;
+      else if (i == p) nv[r] = M[p][j] * ipiv;
+      else if (j == p) nv[r] = M[i][p] * ipiv;
+      else nv[r] = fma(-M[i][p], M[p][j] * ipiv, M[i][j]);
     }
     __syncthreads();
 #pragma unroll

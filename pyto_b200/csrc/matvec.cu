@@ -42,8 +42,6 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-__device__ __forceinline__ int ring5(int k) { return (k + 5) % 5; }
-
 template <int TY, bool DOT, bool MASKIN, int MINB>
 __global__ void __launch_bounds__(32 * TY, MINB)
     k_matvec64(GridDims g, KHat kh, const double* __restrict__ s, const uint8_t* __restrict__ mask,
@@ -66,7 +64,9 @@ __global__ void __launch_bounds__(32 * TY, MINB)
   const int ex = X0 - 1 + tx, ey = Y0 - 1 + ty;
   const bool col_in = ex >= 0 && ex < g.nx && ey >= 0 && ey < g.ny;
   const bool mask_out = (mode & PYTO_MASK_OUT) && mask != nullptr;
-  const long long plane_nodes = (long long)g.sx * g.sy;
+  // node ids and DOF ids fit in int32 (checked by pyto_operator_init)
+  const int pn = g.sx * g.sy;  // nodes per plane
+  const int pe = g.nx * g.ny;  // elements per layer
 
   // staging slots: node (tx, ty) of the (TX+1) x (TY+1) tile, plus the last
   // tile row / column for the first TX+1+TY threads
@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(32 * TY, MINB)
     const int gx = X0 - 1 + lx, gy = Y0 - 1 + ly;
     return (gx >= 0 && gx < g.sx && gy >= 0 && gy < g.sy) ? gx + g.sx * gy : -1;
   };
-  int lxe = -1, lye = -1;
+  int lxe = -1, lye = 0;
   if (tid < PX) {
     lxe = tid;
     lye = TY;
@@ -82,23 +82,29 @@ __global__ void __launch_bounds__(32 * TY, MINB)
     lxe = TX;
     lye = tid - PX;
   }
+  const bool has_e = lxe >= 0;
   const int offm = plane_off(tx, ty);
-  const int offe = lxe >= 0 ? plane_off(lxe, lye) : -1;
-  const int sim = ty * PX + tx, sie = lye * PX + lxe;
-  // asynchronous copy of plane k into ring slot ring5(k) (zero outside the domain)
-  auto issue_plane = [&](int k) {
+  const int offe = has_e ? plane_off(lxe, lye) : -1;
+  const int sim = ty * PX + tx, sie = lye * PX + (has_e ? lxe : 0);
+
+  // ring slots (double offsets into su, byte offsets into smk) of planes
+  // ez-1 .. ez+3, rotated once per layer
+  int r0 = 0, r1 = 1, r2 = 2, r3 = 3, r4 = 4;  // slot of plane ez-1+i
+
+  // plane k is issued into the slot held by `slot`; n_off: its first node of the plane
+  auto issue_plane = [&](int k, int slot) {
     const bool kin = k >= 0 && k < g.sz;
-    const long long base = plane_nodes * (kin ? k : 0);
-    double* d = su + (size_t)ring5(k) * 3 * PLANE;
+    double* d = su + slot * (3 * PLANE);
+    const int nb = kin ? pn * k : 0;
     {
       const bool v = kin && offm >= 0;
-      const double* src = u + (v ? 3 * (base + offm) : 0);
+      const double* src = u + 3 * (v ? nb + offm : 0);
 #pragma unroll
       for (int c = 0; c < 3; ++c) cp_async8(d + c * PLANE + sim, src + c, v);
     }
-    if (lxe >= 0) {
+    if (has_e) {
       const bool v = kin && offe >= 0;
-      const double* src = u + (v ? 3 * (base + offe) : 0);
+      const double* src = u + 3 * (v ? nb + offe : 0);
 #pragma unroll
       for (int c = 0; c < 3; ++c) cp_async8(d + c * PLANE + sie, src + c, v);
     }
@@ -108,25 +114,21 @@ __global__ void __launch_bounds__(32 * TY, MINB)
   auto load_mask = [&](int k) {
     mm = me = 0;
     if (mask && k >= 0 && k < g.sz) {
-      const long long base = plane_nodes * k;
-      if (offm >= 0) mm = __ldg(mask + base + offm);
-      if (offe >= 0) me = __ldg(mask + base + offe);
+      const int nb = pn * k;
+      if (offm >= 0) mm = __ldg(mask + nb + offm);
+      if (offe >= 0) me = __ldg(mask + nb + offe);
     }
   };
-  auto store_mask = [&](int k) {
-    uint8_t* d = smk + ring5(k) * PLANE;
+  auto store_mask = [&](int slot) {
+    uint8_t* d = smk + slot * PLANE;
     d[sim] = (uint8_t)mm;
-    if (lxe >= 0) d[sie] = (uint8_t)me;
+    if (has_e) d[sie] = (uint8_t)me;
   };
-  auto load_s = [&](int ez) -> double {
-    if (!col_in || ez < 0 || ez >= g.nz) return 0.0;
-    return __ldg(s + ex + (long long)g.nx * (ey + (long long)g.ny * ez));
-  };
-  auto face = [&](int k, double (&F)[3][4]) {
-    const double* b = su + (size_t)ring5(k) * 3 * PLANE + ty * PX + tx;
+  auto face = [&](int slot, double (&F)[3][4]) {
+    const double* b = su + slot * (3 * PLANE) + sim;
     int m00 = 0, m10 = 0, m01 = 0, m11 = 0;
     if (MASKIN) {
-      const uint8_t* mb = smk + ring5(k) * PLANE + ty * PX + tx;
+      const uint8_t* mb = smk + slot * PLANE + sim;
       m00 = mb[0];
       m10 = mb[1];
       m01 = mb[PX];
@@ -146,55 +148,59 @@ __global__ void __launch_bounds__(32 * TY, MINB)
     }
   };
   const bool owner = tx < TX - 1 && ty < TY - 1 && (X0 + tx) < g.sx && (Y0 + ty) < g.sy;
+  const int li = (ty + 1) * PX + tx + 1;  // owned node in the tile
   double dot = 0.0;
   double cT[3] = {0.0, 0.0, 0.0};
-  auto output = [&](int k) {  // owned node of plane k
+  auto output = [&](int k, int slot) {  // owned node of plane k
     if (!owner) return;
-    const int li = (ty + 1) * PX + tx + 1;
-    const int mk = mask_out ? (int)smk[ring5(k) * PLANE + li] : 0;
-    const long long node = (X0 + tx) + (long long)g.sx * (Y0 + ty) + plane_nodes * k;
-    const double* scb = sc + (size_t)(k & 1) * 3 * TY * TX;
+    const int mk = mask_out ? (int)smk[slot * PLANE + li] : 0;
+    const int dof = 3 * ((X0 + tx) + g.sx * (Y0 + ty) + pn * k);
+    const double* scb = sc + (k & 1) * (3 * TY * TX) + (ty + 1) * TX + tx;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      double v = cT[c] + scb[(c * TY + ty + 1) * TX + tx];
+      double v = cT[c] + scb[c * TY * TX];
       if ((mk >> c) & 1) v = 0.0;
-      y[3 * node + c] = v;
+      y[dof + c] = v;
       if (DOT) {
-        double uv = su[(size_t)(ring5(k) * 3 + c) * PLANE + li];
-        if (MASKIN && ((smk[ring5(k) * PLANE + li] >> c) & 1)) uv = 0.0;
+        double uv = su[slot * (3 * PLANE) + c * PLANE + li];
+        if (MASKIN && ((smk[slot * PLANE + li] >> c) & 1)) uv = 0.0;
         dot = fma(uv, v, dot);
       }
     }
   };
+  // element index of this column at layer ez, advanced by pe per layer
+  int eidx = ex + g.nx * ey + pe * (Z0 - 1);
 
-  // prologue: planes Z0-1, Z0 in flight, masks of Z0-1, Z0 staged, mask of Z0+1 in registers
-  issue_plane(Z0 - 1);
-  issue_plane(Z0);
+  // prologue: planes Z0-1, Z0 in flight; masks of Z0-1, Z0 staged; mask of Z0+1 in registers
+  issue_plane(Z0 - 1, r0);
+  issue_plane(Z0, r1);
   load_mask(Z0 - 1);
-  store_mask(Z0 - 1);
+  store_mask(r0);
   load_mask(Z0);
-  store_mask(Z0);
+  store_mask(r1);
   load_mask(Z0 + 1);
-  double s_next = load_s(Z0 - 1);
+  double s_next = (col_in && Z0 - 1 >= 0) ? __ldg(s + eidx) : 0.0;
 #pragma unroll
   for (int i = 0; i < 12; ++i) sG[i * NT + tid] = 0.0;
-  if (Z0 + 1 <= Z1) issue_plane(Z0 + 1);
+  if (Z0 + 1 <= Z1) issue_plane(Z0 + 1, r2);
   else cp_async_commit();
 
-  // layer ez: planes ez, ez+1 landed (wait_group 1 leaves plane ez+2 in flight)
+  // layer ez: planes ez (slot r1), ez+1 (r2) landed; ez+2 (r3) may be in flight
   for (int ez = Z0 - 1; ez < Z1; ++ez) {
     cp_async_wait1();
     __syncthreads();
-    if (ez - 1 >= Z0) output(ez - 1);
-    store_mask(ez + 2);  // harmless for planes beyond Z1 (never read)
+    if (ez - 1 >= Z0) output(ez - 1, r0);
+    store_mask(r3);  // mask of plane ez+2 (unused for planes beyond Z1)
     load_mask(ez + 3);
-    if (ez + 3 <= Z1) issue_plane(ez + 3);
+    if (ez + 3 <= Z1) issue_plane(ez + 3, r4);
     else cp_async_commit();
     const double se = s_next;
-    if (ez + 1 < Z1) s_next = load_s(ez + 1);
+    eidx += pe;
+    s_next = (col_in && ez + 1 < Z1 && ez + 1 < g.nz) ? __ldg(s + eidx) : 0.0;
+    const double sv = (ez >= 0 && ez < g.nz) ? se : 0.0;
     double Fb[3][4], Ft[3][4], Gs[3][4];
-    face(ez, Fb);
-    face(ez + 1, Ft);
+    face(r1, Fb);
+    face(r2, Ft);
 #pragma unroll
     for (int c = 0; c < 3; ++c)
 #pragma unroll
@@ -202,7 +208,8 @@ __global__ void __launch_bounds__(32 * TY, MINB)
     // classes in pairs (qp, qp^4): after a pair, its three top-face entries are final
 #pragma unroll
     for (int qp = 0; qp < 4; ++qp) {
-      double gt[3] = {0.0, 0.0, 0.0};
+      double gt[3];
+      bool gt_set[3] = {false, false, false};
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int q = qp + 4 * h;
@@ -211,7 +218,7 @@ __global__ void __launch_bounds__(32 * TY, MINB)
         for (int d = 0; d < 3; ++d) {
           const int m = member_mode(q, d);
           const int f = m & 3;
-          v[d] = (m == 0) ? 0.0 : ((m & 4) ? se * (Ft[d][f] - Fb[d][f]) : se * (Ft[d][f] + Fb[d][f]));
+          v[d] = (m == 0) ? 0.0 : ((m & 4) ? sv * (Ft[d][f] - Fb[d][f]) : sv * (Ft[d][f] + Fb[d][f]));
         }
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
@@ -219,32 +226,41 @@ __global__ void __launch_bounds__(32 * TY, MINB)
           if (m == 0) continue;
           const int f = m & 3;
           double o = 0.0;
+          bool first = true;
 #pragma unroll
           for (int d = 0; d < 3; ++d) {
             if (member_mode(q, d) == 0) continue;
-            o = fma(kh.b[q][3 * c + d], v[d], o);
+            o = first ? kh.b[q][3 * c + d] * v[d] : fma(kh.b[q][3 * c + d], v[d], o);
+            first = false;
           }
           Gs[c][f] += (m & 4) ? -o : o;
-          gt[c] += o;
+          gt[c] = gt_set[c] ? gt[c] + o : o;
+          gt_set[c] = true;
         }
       }
 #pragma unroll
-      for (int c = 0; c < 3; ++c) sG[(c * 4 + ((qp ^ (1 << c)) & 3)) * NT + tid] = gt[c];
+      for (int c = 0; c < 3; ++c) sG[(c * 4 + ((qp ^ (1 << c)) & 3)) * NT + tid] = gt_set[c] ? gt[c] : 0.0;
     }
     if (ez >= Z0) {
-      double* scb = sc + (size_t)(ez & 1) * 3 * TY * TX;
+      double* scb = sc + (ez & 1) * (3 * TY * TX) + ty * TX + tx;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         double c00, c10, c01, c11;
         face_inv(Gs[c], c00, c10, c01, c11);
         cT[c] = c11 + __shfl_down_sync(0xffffffffu, c01, 1);
-        scb[(c * TY + ty) * TX + tx] = c10 + __shfl_down_sync(0xffffffffu, c00, 1);
+        scb[c * TY * TX] = c10 + __shfl_down_sync(0xffffffffu, c00, 1);
       }
     }
+    const int rt = r0;
+    r0 = r1;
+    r1 = r2;
+    r2 = r3;
+    r3 = r4;
+    r4 = rt;
   }
   cp_async_wait0();
   __syncthreads();
-  if (Z1 - 1 >= Z0) output(Z1 - 1);
+  if (Z1 - 1 >= Z0) output(Z1 - 1, r0);
   if (DOT) {
     const double bsum = block_sum<NT>(dot, sred);
     double v[1] = {bsum};
