@@ -87,9 +87,8 @@ __global__ void __launch_bounds__(32 * TY, MINB)
   const int offe = has_e ? plane_off(lxe, lye) : -1;
   const int sim = ty * PX + tx, sie = lye * PX + (has_e ? lxe : 0);
 
-  // ring slots (double offsets into su, byte offsets into smk) of planes
-  // ez-1 .. ez+3, rotated once per layer
-  int r0 = 0, r1 = 1, r2 = 2, r3 = 3, r4 = 4;  // slot of plane ez-1+i
+  // ring slots of planes ez-1 .. ez+3 (r_i holds plane ez-1+i), rotated once per layer
+  int r0 = 0, r1 = 1, r2 = 2, r3 = 3, r4 = 4;
 
   // plane k is issued into the slot held by `slot`; n_off: its first node of the plane
   auto issue_plane = [&](int k, int slot) {
@@ -171,18 +170,19 @@ __global__ void __launch_bounds__(32 * TY, MINB)
   // element index of this column at layer ez, advanced by pe per layer
   int eidx = ex + g.nx * ey + pe * (Z0 - 1);
 
-  // prologue: planes Z0-1, Z0 in flight; masks of Z0-1, Z0 staged; mask of Z0+1 in registers
-  issue_plane(Z0 - 1, r0);
-  issue_plane(Z0, r1);
+  // prologue (layer Z0-1 is next): planes Z0-1 -> r1, Z0 -> r2, Z0+1 -> r3 in flight;
+  // masks of Z0-1, Z0 staged; mask of Z0+1 in registers (staged in the first layer)
+  issue_plane(Z0 - 1, r1);
+  issue_plane(Z0, r2);
   load_mask(Z0 - 1);
-  store_mask(r0);
-  load_mask(Z0);
   store_mask(r1);
+  load_mask(Z0);
+  store_mask(r2);
   load_mask(Z0 + 1);
   double s_next = (col_in && Z0 - 1 >= 0) ? __ldg(s + eidx) : 0.0;
 #pragma unroll
   for (int i = 0; i < 12; ++i) sG[i * NT + tid] = 0.0;
-  if (Z0 + 1 <= Z1) issue_plane(Z0 + 1, r2);
+  if (Z0 + 1 <= Z1) issue_plane(Z0 + 1, r3);
   else cp_async_commit();
 
   // layer ez: planes ez (slot r1), ez+1 (r2) landed; ez+2 (r3) may be in flight
