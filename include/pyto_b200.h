@@ -111,7 +111,7 @@ int pyto_version(void);
  * reference counterpart: instrumentation of the launch count). */
 long long pyto_launch_count(void);
 /* Select the tile variant of a kernel (no reference counterpart: the tile
- * choice of the project's autotuner).  PYTO_KERNEL_MATVEC variants 0..3.
+ * choice of the project's autotuner).  PYTO_KERNEL_MATVEC variants 0..3 (default 2).
  * Process-wide; not thread-safe against concurrent launches. */
 #define PYTO_KERNEL_MATVEC 0
 int pyto_tune(int kernel, int variant);

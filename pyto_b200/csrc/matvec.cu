@@ -298,10 +298,10 @@ static int launch_mv(const GridDims& g, const KHat& kh, const double* s, const u
             : launch_mv_t<TY, false, false, MINB>(L, smem, g, kh, s, mask, u, y, mode, nullptr, nullptr, nullptr, st);
 }
 
-// Tile variant of the FP64 matvec (0 = default):
+// Tile variant of the FP64 matvec (2 = default: fastest measured at 192x96x96):
 //   0: 32x8 threads, 2 CTAs/SM (128 registers)   1: 32x8, 1 CTA/SM (no register cap)
 //   2: 32x4, 3 CTAs/SM                            3: 32x16, 1 CTA/SM
-static int g_mv_variant = 0;
+static int g_mv_variant = 2;
 
 int launch_matvec64(const pyto_operator_t* op, const double* s, const uint8_t* mask, const double* u, double* y,
                     int mode, double* part, unsigned* counter, double* dot, cudaStream_t st) {

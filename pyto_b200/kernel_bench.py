@@ -40,7 +40,7 @@ def main(argv=None):
     ap.add_argument("--nel", default="192,96,96")
     ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--warm", type=int, default=3)
-    ap.add_argument("--variant", type=int, default=0, help="matvec tile variant (pyto_tune)")
+    ap.add_argument("--variant", type=int, default=2, help="matvec tile variant (pyto_tune)")
     a = ap.parse_args(argv)
     nel = tuple(int(v) for v in a.nel.split(","))
     A.call("pyto_tune", 0, a.variant)

@@ -73,7 +73,7 @@ def test_matvec_tile_variants(variant, nel):
             assert np.abs(y.cpu().numpy() - yref).max() <= 1e-13 * np.abs(yref).max()
             assert abs(dot.item() - uu @ yref) <= 1e-12 * abs(uu @ yref)
     finally:
-        A.call("pyto_tune", 0, 0)
+        A.call("pyto_tune", 0, 2)
 
 
 def test_matvec_bitwise_deterministic():
