@@ -120,11 +120,27 @@ def build(device, nel, groups, modes):
     return dict(mesh=mesh, grid=grid, rho=rho, F=F, f=f, defl=defl, ds=ds, x=x)
 
 
-def solve_step(P, rho=None):
+def solve_step(P, rho=None, form="mixed"):
     g = P["grid"]
     s, _ = g.simp(P["rho"] if rho is None else rho, 3.0, 1e-9, want_ds=False)
-    u, info = g.dpcg(s, P["F"], P["defl"], rtol=RTOL, max_iters=5000, stop_rule=0, check_every=20)
-    return u, info
+    if form == "mixed":
+        return g.dpcg_mixed(s, P["F"], P["defl"], rtol=RTOL, inner_rtol=P.get("inner_rtol", 1e-4), max_iters=8000,
+                            check_every=20)
+    return g.dpcg(s, P["F"], P["defl"], rtol=RTOL, max_iters=5000, stop_rule=0, check_every=20)
+
+
+def time_solves(P, form, steps, device):
+    """Device time of `steps` solves of one form (CUDA events on the current stream)."""
+    import torch
+    st = torch.cuda.current_stream(device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(device)
+    e0.record(st)
+    for _ in range(steps):
+        u, info = solve_step(P, form=form)
+    e1.record(st)
+    torch.cuda.synchronize(device)
+    return e0.elapsed_time(e1) / 1e3 / steps, u, info
 
 
 def time_matvec(P, reps=30):
@@ -191,6 +207,9 @@ def main():
     ap.add_argument("--modes", type=int, default=6)
     ap.add_argument("--nel", default=None, help="override grid, e.g. 96,48,48 (not a bench line)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--form", default="mixed", choices=["mixed", "fp64"],
+                    help="timed solver: FP64 refinement around FP32 deflated PCG, or plain FP64 deflated PCG")
+    ap.add_argument("--inner-rtol", type=float, default=1e-4)
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -221,7 +240,9 @@ def main():
 
     nel = tuple(int(v) for v in args.nel.split(",")) if args.nel else NEL
     P = build(device, nel, args.groups, args.modes)
+    P["inner_rtol"] = args.inner_rtol
     g = P["grid"]
+    other = "fp64" if args.form == "mixed" else "mixed"
 
     def barrier():
         if world > 1:
@@ -229,9 +250,9 @@ def main():
             dist.barrier()
 
     for _ in range(max(3, args.warmup)):
-        u, info = solve_step(P)
+        u, info = solve_step(P, form=args.form)
     torch.cuda.synchronize(device)
-    iters, trr = info.iters, info.true_rel_res
+    iters, trr, cycles = info.iters, info.true_rel_res, getattr(info, "cycles", None)
     n0 = A.lib().pyto_launch_count()
     barrier()
     torch.cuda.synchronize(device)
@@ -241,7 +262,7 @@ def main():
         e0.record(st)
         infos = []
         for _ in range(args.steps):
-            u, info = solve_step(P)
+            u, info = solve_step(P, form=args.form)
             infos.append(info)
         e1.record(st)
         torch.cuda.synchronize(device)
@@ -260,7 +281,7 @@ def main():
     u_host = torch.empty(g.ndof, dtype=torch.float64).pin_memory()
     for _ in range(2):
         r = rho_host.to(device, non_blocking=True)
-        u, _ = solve_step(P, r)
+        u, _ = solve_step(P, r, form=args.form)
         u_host.copy_(u, non_blocking=True)
     torch.cuda.synchronize(device)
     barrier()
@@ -268,7 +289,7 @@ def main():
     e2.record(st)
     for _ in range(args.steps):
         r = rho_host.to(device, non_blocking=True)
-        u, _ = solve_step(P, r)
+        u, _ = solve_step(P, r, form=args.form)
         u_host.copy_(u, non_blocking=True)
     e3.record(st)
     torch.cuda.synchronize(device)
@@ -277,6 +298,18 @@ def main():
         import torch.distributed as dist
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e = float(te.item()) / (world * args.steps)
+
+    # the other solver form on the same input, for the mixed / FP64 comparison
+    u_main = u.clone()
+    for _ in range(2):
+        solve_step(P, form=other)
+    t_other, u_other, info_other = time_solves(P, other, args.steps, device)
+    s_, _ = g.simp(P["rho"], 3.0, 1e-9, want_ds=False)
+    _, c_main = g.energy(u_main, s=s_)
+    _, c_other = g.energy(u_other, s=s_)
+    c_main, c_other = c_main.item(), c_other.item()
+    t_fp64 = t_other if other == "fp64" else value
+    t_mixed = t_other if other == "mixed" else value
 
     # roofline of the dominant kernel (FP64 matvec)
     t_mv = time_matvec(P)
@@ -294,13 +327,19 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if args.form == "mixed" else "f64",
+            "data": "synthetic",
             "config": {"workload": f"{nel[0]}x{nel[1]}x{nel[2]} hex8 cantilever, {g.ndof} DOF, "
                                    "rho = H(U[0.01,1], seed 0)/Hs r=2, SIMP p=3 Emin=1e-9",
-                       "form": "fp64 deflated PCG (Jacobi), true rel-residual <= 1e-8",
+                       "form": ("FP64 iterative refinement around FP32 deflated PCG (Jacobi), FP64 true "
+                                "rel-residual <= 1e-8" if args.form == "mixed" else
+                                "fp64 deflated PCG (Jacobi), true rel-residual <= 1e-8"),
+                       "fp64_solve_s": t_fp64, "mixed_solve_s": t_mixed, "mixed_speedup": t_fp64 / t_mixed,
+                       "compliance": c_main, "compliance_rel_diff_vs_other_form": abs(c_main - c_other) / abs(c_other),
+                       "other_form_iterations": info_other.iters,
                        "coarse_space": f"{P['ds'].ws_nGroups} node-box groups x {args.modes} rigid modes "
                                        f"(reference box partition), dense FP64 coarse inverse",
-                       "iterations": iters, "true_rel_res": trr, "l2": "inputs larger than L2 (~0.6 GB moved per "
+                       "iterations": iters, "refinement_cycles": cycles, "true_rel_res": trr, "l2": "inputs larger than L2 (~0.6 GB moved per "
                                                                           "iteration)",
                        "parallelism": f"replicas x{world}"},
             "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(rho_host.numel() * 8),

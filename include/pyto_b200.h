@@ -52,6 +52,7 @@ extern "C" {
 #define PYTO_WS_PCG 1     /* pyto_pcg_solve                                               */
 #define PYTO_WS_DPCG 2    /* pyto_dpcg_setup / pyto_dpcg_solve (coarse inverse is separate) */
 #define PYTO_WS_OC 3      /* pyto_oc_update                                               */
+#define PYTO_WS_DPCG_MIXED 4  /* pyto_dpcg_setup / pyto_dpcg_mixed_solve                      */
 
 /* The operator: grid + the element stiffness matrix, plus the data derived
  * from Ke that the kernels use (Ke rotated into the 8x8 Hadamard corner basis,
@@ -114,6 +115,7 @@ long long pyto_launch_count(void);
  * choice of the project's autotuner).  PYTO_KERNEL_MATVEC variants 0..3 (default 2).
  * Process-wide; not thread-safe against concurrent launches. */
 #define PYTO_KERNEL_MATVEC 0
+#define PYTO_KERNEL_MATVEC32 1
 int pyto_tune(int kernel, int variant);
 /* Bytes of workspace for a call of the given kind on this operator (for
  * PYTO_WS_DPCG: any coarse size up to 24576). */
@@ -154,6 +156,13 @@ int pyto_bc_mask(const pyto_operator_t* op, const int64_t* fixed_dofs, int64_t n
  * src/linear_solvers.py:136-202). */
 int pyto_matvec(const pyto_operator_t* op, const double* s, const uint8_t* mask, const double* u,
                 double* y, int mode, double* dot, void* ws, size_t ws_bytes, void* stream);
+
+/* FP32 form of pyto_matvec (FP32 s, u, y; FP32 arithmetic on the FP32 Hadamard-basis
+ * element blocks; the optional dot is accumulated in FP64).  The operator of the
+ * inner cycles of pyto_dpcg_mixed_solve; no counterpart in the reference, which
+ * assembles K in FP64 only. */
+int pyto_matvec_f32(const pyto_operator_t* op, const float* s, const uint8_t* mask, const float* u,
+                    float* y, int mode, double* dot, void* ws, size_t ws_bytes, void* stream);
 /* pyto_matvec with a non-NULL dot, for callers that cannot allocate device memory
  * (plugins whose host owns every allocation, loops where allocation is forbidden after
  * start-up).  No counterpart in the reference.  The cross-block scratch is a fixed
@@ -186,6 +195,19 @@ int pyto_dpcg_solve(const pyto_operator_t* op, const double* s, const uint8_t* m
                     const pyto_deflation_t* defl, const double* b, double* u,
                     const pyto_solve_cfg_t* cfg, pyto_solve_status_t* status, void* ws,
                     size_t ws_bytes, void* stream);
+
+/* Mixed-precision deflated PCG: FP64 iterative refinement around FP32 deflated PCG
+ * cycles.  Each cycle forms the true residual r = b - K u in FP64, solves K d = r with
+ * FP32 vectors and FP32 operator (FP64 reductions, FP64 coarse inverse from
+ * pyto_dpcg_setup) to ||r_inner|| < inner_rtol ||r||, and updates u += d in FP64; it
+ * stops when ||b - K u|| <= cfg->rtol ||b|| in FP64.  cfg->max_iters caps the total
+ * inner iterations; status->reserved returns the number of cycles.  Needs a
+ * PYTO_WS_DPCG_MIXED workspace.  Replaces DeflationSolver.deflatedPCG
+ * (src/deflation.py:504-584) where FP64 accuracy is required at lower cost. */
+int pyto_dpcg_mixed_solve(const pyto_operator_t* op, const double* s, const uint8_t* mask,
+                          const pyto_deflation_t* defl, const double* b, double* u,
+                          const pyto_solve_cfg_t* cfg, double inner_rtol, pyto_solve_status_t* status,
+                          void* ws, size_t ws_bytes, void* stream);
 
 /* ---- objectives and sensitivities ------------------------------------------------ */
 /* ce[e] = u_e^T Ke v_e (u == v gives the element energy of compliance).  If s != NULL and

@@ -19,7 +19,7 @@ OK, NOT_CONVERGED = 0, 1
 ERR_ARG, ERR_CUDA, ERR_WORKSPACE, ERR_BREAKDOWN, ERR_TOO_LARGE = -1, -2, -3, -4, -5
 MASK_IN, MASK_OUT = 1, 2
 FILTER_RAW, FILTER_DENSITY, FILTER_CHAIN, FILTER_SENS, FILTER_HS = 0, 1, 2, 3, 4
-WS_REDUCE, WS_PCG, WS_DPCG, WS_OC = 0, 1, 2, 3
+WS_REDUCE, WS_PCG, WS_DPCG, WS_OC, WS_DPCG_MIXED = 0, 1, 2, 3, 4
 
 
 class PytoLibraryError(RuntimeError):
@@ -73,6 +73,7 @@ SIGNATURES = {
     "pyto_simp": (C.c_int, [_P, _P, C.c_int64, C.c_double, C.c_double, _P, _P, _P]),
     "pyto_bc_mask": (C.c_int, [_OP, _P, C.c_int64, _P, _P]),
     "pyto_matvec": (C.c_int, [_OP, _P, _P, _P, _P, C.c_int, _P, _P, C.c_size_t, _P]),
+    "pyto_matvec_f32": (C.c_int, [_OP, _P, _P, _P, _P, C.c_int, _P, _P, C.c_size_t, _P]),
     "pyto_jacobi": (C.c_int, [_OP, _P, _P, _P, _P, _P, _P]),
     "pyto_matvec_dot_noalloc": (C.c_int, [_OP, _P, _P, _P, _P, C.c_int, _P, _P]),
     "pyto_pcg_solve": (C.c_int, [_OP, _P, _P, _P, _P, C.POINTER(SolveCfg), C.POINTER(SolveStatus), _P, C.c_size_t,
@@ -80,6 +81,8 @@ SIGNATURES = {
     "pyto_dpcg_setup": (C.c_int, [_OP, _P, _P, C.POINTER(Deflation), _P, C.c_size_t, _P]),
     "pyto_dpcg_solve": (C.c_int, [_OP, _P, _P, C.POINTER(Deflation), _P, _P, C.POINTER(SolveCfg),
                                   C.POINTER(SolveStatus), _P, C.c_size_t, _P]),
+    "pyto_dpcg_mixed_solve": (C.c_int, [_OP, _P, _P, C.POINTER(Deflation), _P, _P, C.POINTER(SolveCfg), C.c_double,
+                                        C.POINTER(SolveStatus), _P, C.c_size_t, _P]),
     "pyto_elem_energy": (C.c_int, [_OP, _P, _P, _P, _P, _P, _P, C.c_size_t, _P]),
     "pyto_stress": (C.c_int, [_OP, _P, _P, C.c_double, _P, _P, _P, _P, _P]),
     "pyto_pnorm_sum": (C.c_int, [_OP, _P, C.c_double, _P, _P, C.c_size_t, _P]),

@@ -6,9 +6,10 @@
 
 namespace pyto {
 size_t pcg_workspace_bytes(const pyto_operator_t* op);
-size_t dpcg_workspace_bytes(const pyto_operator_t* op);
+size_t dpcg_workspace_bytes(const pyto_operator_t* op, bool mixed);
 int oc_grid_blocks();
 int set_matvec_variant(int v);
+int set_matvec32_variant(int v);
 }  // namespace pyto
 
 namespace pyto {
@@ -21,6 +22,7 @@ using namespace pyto;
 extern "C" int pyto_tune(int kernel, int variant) {
   switch (kernel) {
     case PYTO_KERNEL_MATVEC: return set_matvec_variant(variant);
+    case PYTO_KERNEL_MATVEC32: return set_matvec32_variant(variant);
     default: return PYTO_ERR_ARG;
   }
 }
@@ -35,7 +37,9 @@ extern "C" size_t pyto_workspace_bytes(const pyto_operator_t* op, int kind) {
     case PYTO_WS_PCG:
       return pcg_workspace_bytes(op);
     case PYTO_WS_DPCG:
-      return dpcg_workspace_bytes(op);
+      return dpcg_workspace_bytes(op, false);
+    case PYTO_WS_DPCG_MIXED:
+      return dpcg_workspace_bytes(op, true);
     case PYTO_WS_OC:
       return 1024 + 8 * 3 * (size_t)std::max(oc_grid_blocks(), 4 * kNumSMs);
     default:

@@ -345,25 +345,25 @@ __global__ void k_negate(long long n, double* A) {
 // chunk partials in chunk order, so the result does not depend on scheduling.
 constexpr int kRestrictChunk = 2048;
 constexpr int kRestrictMaxBlocks = 65536;
+template <typename T>
 __global__ void __launch_bounds__(256) k_restrict(GridDims g, DeflP dp, const int32_t* __restrict__ gptr,
                                                   const int32_t* __restrict__ gnodes, const double* __restrict__ gc,
-                                                  const uint8_t* __restrict__ fl, const double* __restrict__ y,
-                                                  int nch, double* __restrict__ part, unsigned* counter,
-                                                  double* __restrict__ v) {
-  __shared__ double sred[8];
-  __shared__ bool s_last;
+                                                  const uint8_t* __restrict__ fl, const T* __restrict__ y,
+                                                  int nch, double* __restrict__ part) {
+  __shared__ double sred[8 * 6];
   const int grp = blockIdx.x / nch, ch = blockIdx.x % nch;
   const int beg = gptr[grp] + ch * kRestrictChunk;
   const int end = min(gptr[grp + 1], beg + kRestrictChunk);
   const double cx = gc[3 * grp], cy = gc[3 * grp + 1], cz = gc[3 * grp + 2];
   double acc[6] = {0, 0, 0, 0, 0, 0};
   for (int t = beg + threadIdx.x; t < end; t += blockDim.x) {
-    const long long n = gnodes[t];
+    const int n = gnodes[t];
     double x, yy, z;
     node_xyz(g, n, dp.hx, dp.hy, dp.hz, x, yy, z);
     const double rx = x - cx, ry = yy - cy, rz = z - cz;
     const int f = fl[n];
-    const double vx = (f & 1) ? 0.0 : y[3 * n], vy = (f & 2) ? 0.0 : y[3 * n + 1], vz = (f & 4) ? 0.0 : y[3 * n + 2];
+    const double vx = (f & 1) ? 0.0 : (double)y[3 * n], vy = (f & 2) ? 0.0 : (double)y[3 * n + 1],
+                 vz = (f & 4) ? 0.0 : (double)y[3 * n + 2];
     acc[0] += vx;
     acc[1] += vy;
     acc[2] += vz;
@@ -371,33 +371,37 @@ __global__ void __launch_bounds__(256) k_restrict(GridDims g, DeflP dp, const in
     acc[4] += rz * vx - rx * vz;
     acc[5] += -ry * vx + rx * vy;
   }
-  for (int a = 0; a < dp.modes; ++a) {
-    const double t = block_sum<256>(acc[a], sred);
-    if (threadIdx.x == 0) part[(size_t)blockIdx.x * 6 + a] = t;
+  // block reduction of the 6 sums in a fixed order (one barrier pair)
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int a = 0; a < 6; ++a) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc[a] += __shfl_down_sync(0xffffffffu, acc[a], o);
   }
-  if (threadIdx.x == 0) {
-    __threadfence();
-    s_last = (atomicAdd(counter, 1u) == gridDim.x - 1u);
-  }
+  if (lane == 0)
+#pragma unroll
+    for (int a = 0; a < 6; ++a) sred[wid * 6 + a] = acc[a];
   __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  for (int i = threadIdx.x; i < dp.ngroups * dp.modes; i += blockDim.x) {
-    const int gg = i / dp.modes, a = i % dp.modes;
+  if (threadIdx.x < 6) {
     double t = 0.0;
-    for (int c = 0; c < nch; ++c) t += __ldcg(part + ((size_t)gg * nch + c) * 6 + a);
-    v[i] = t;
+    for (int w = 0; w < 8; ++w) t += sred[w * 6 + threadIdx.x];
+    part[(size_t)blockIdx.x * 6 + threadIdx.x] = t;
   }
-  if (threadIdx.x == 0) *counter = 0u;
 }
 
-// mu = Einv v (one warp per row, v staged in shared memory)
-__global__ void __launch_bounds__(256) k_coarse_gemv(long long nc, const double* __restrict__ Einv,
-                                                     const double* __restrict__ v, double* __restrict__ mu,
+// mu = Einv v (one warp per row); v = W^T y is formed while staging it in
+// shared memory, summing each group's chunk partials in chunk order
+__global__ void __launch_bounds__(256) k_coarse_gemv(long long nc, int modes, int nch, const double* __restrict__ Einv,
+                                                     const double* __restrict__ part, double* __restrict__ mu,
                                                      const KrylovState* S) {
   extern __shared__ double sv[];
   if (S && S->done) return;
-  for (long long i = threadIdx.x; i < nc; i += blockDim.x) sv[i] = v[i];
+  for (long long i = threadIdx.x; i < nc; i += blockDim.x) {
+    const long long gg = i / modes, a = i - gg * modes;
+    double t = 0.0;
+    for (int c = 0; c < nch; ++c) t += __ldg(part + (gg * nch + c) * 6 + a);
+    sv[i] = t;
+  }
   __syncthreads();
   const int lane = threadIdx.x & 31;
   for (long long row = (long long)blockIdx.x * 8 + (threadIdx.x >> 5); row < nc; row += (long long)gridDim.x * 8) {
@@ -431,24 +435,26 @@ __device__ __forceinline__ void prolong_node(const GridDims& g, const DeflP& dp,
 }
 
 // x = W mu (masked)
+template <typename T>
 __global__ void __launch_bounds__(256) k_prolong(GridDims g, DeflP dp, const int32_t* __restrict__ ngrp,
                                                  const double* __restrict__ gc, const double* __restrict__ mu,
-                                                 const uint8_t* __restrict__ fl, double* __restrict__ x) {
+                                                 const uint8_t* __restrict__ fl, T* __restrict__ x) {
   for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < g.nnodes;
        n += (long long)gridDim.x * blockDim.x) {
     double w[3];
     prolong_node(g, dp, n, ngrp, gc, mu, w);
     const int f = fl[n];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) x[3 * n + c] = ((f >> c) & 1) ? 0.0 : w[c];
+    for (int c = 0; c < 3; ++c) x[3 * n + c] = ((f >> c) & 1) ? T(0) : (T)w[c];
   }
 }
 
-// r = b - t (masked), z = M^-1 r; reductions r.z, r.r, b.b
-__global__ void __launch_bounds__(kNodeThreads) k_dpcg_init(GridDims g, Prec pc, const double* __restrict__ b,
-                                                            const double* __restrict__ t, const double* __restrict__ w,
-                                                            const uint8_t* __restrict__ fl, double* __restrict__ r,
-                                                            double* __restrict__ z, KrylovState* S, double* part,
+// r = b - t (masked), z = M^-1 r; reductions r.z, r.r, b.b (FP64)
+template <typename T>
+__global__ void __launch_bounds__(kNodeThreads) k_dpcg_init(GridDims g, Prec pc, const T* __restrict__ b,
+                                                            const T* __restrict__ t, const double* __restrict__ w,
+                                                            const uint8_t* __restrict__ fl, T* __restrict__ r,
+                                                            T* __restrict__ z, KrylovState* S, double* part,
                                                             unsigned* counter) {
   __shared__ double sred[kNodeThreads / 32];
   double rz = 0.0, rr = 0.0, bb = 0.0;
@@ -460,14 +466,14 @@ __global__ void __launch_bounds__(kNodeThreads) k_dpcg_init(GridDims g, Prec pc,
     for (int c = 0; c < 3; ++c) {
       const long long i = 3 * n + c;
       const bool fixed = (f >> c) & 1;
-      const double bi = fixed ? 0.0 : b[i];
-      const double ri = fixed ? 0.0 : bi - t[i];
-      const double zi = jacobi_apply(ri, f, c, wn, pc);
+      const T bi = fixed ? T(0) : b[i];
+      const T ri = fixed ? T(0) : bi - t[i];
+      const T zi = (T)jacobi_apply((double)ri, f, c, wn, pc);
       r[i] = ri;
       z[i] = zi;
-      rz = fma(ri, zi, rz);
-      rr = fma(ri, ri, rr);
-      bb = fma(bi, bi, bb);
+      rz = fma((double)ri, (double)zi, rz);
+      rr = fma((double)ri, (double)ri, rr);
+      bb = fma((double)bi, (double)bi, bb);
     }
   }
   double v[3];
@@ -486,13 +492,13 @@ __global__ void __launch_bounds__(kNodeThreads) k_dpcg_init(GridDims g, Prec pc,
   });
 }
 
-// x += a p, r -= a q, z = M^-1 r (stored), reductions -> beta, convergence
+// x += a p, r -= a q, z = M^-1 r (stored), FP64 reductions -> beta, convergence
+template <typename T>
 __global__ void __launch_bounds__(kNodeThreads) k_dpcg_update1(GridDims g, Prec pc, const double* __restrict__ w,
-                                                               const uint8_t* __restrict__ fl,
-                                                               double* __restrict__ x, double* __restrict__ r,
-                                                               double* __restrict__ z, const double* __restrict__ p,
-                                                               const double* __restrict__ q, KrylovState* S,
-                                                               double* part, unsigned* counter) {
+                                                               const uint8_t* __restrict__ fl, T* __restrict__ x,
+                                                               T* __restrict__ r, T* __restrict__ z,
+                                                               const T* __restrict__ p, const T* __restrict__ q,
+                                                               KrylovState* S, double* part, unsigned* counter) {
   __shared__ double sred[kNodeThreads / 32];
   if (S->done) return;
   const double pq = S->pq, rz = S->rz;
@@ -512,13 +518,14 @@ __global__ void __launch_bounds__(kNodeThreads) k_dpcg_update1(GridDims g, Prec 
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const long long i = 3 * n + c;
-      x[i] = fma(alpha, p[i], x[i]);
-      const double ri = fma(-alpha, q[i], r[i]);
+      const T al = (T)alpha;
+      x[i] = fma(al, p[i], x[i]);
+      const T ri = fma(-al, q[i], r[i]);
       r[i] = ri;
-      const double zi = jacobi_apply(ri, f, c, wn, pc);
+      const T zi = (T)jacobi_apply((double)ri, f, c, wn, pc);
       z[i] = zi;
-      rr = fma(ri, ri, rr);
-      rzn = fma(ri, zi, rzn);
+      rr = fma((double)ri, (double)ri, rr);
+      rzn = fma((double)ri, (double)zi, rzn);
     }
   }
   double v[2];
@@ -544,11 +551,12 @@ __global__ void __launch_bounds__(kNodeThreads) k_dpcg_update1(GridDims g, Prec 
 }
 
 // p = z + beta p - W mu  (beta = 0 for the start vector)
+template <typename T>
 __global__ void __launch_bounds__(kNodeThreads) k_dpcg_update2(GridDims g, DeflP dp, const int32_t* __restrict__ ngrp,
                                                                const double* __restrict__ gc,
                                                                const double* __restrict__ mu,
                                                                const uint8_t* __restrict__ fl,
-                                                               const double* __restrict__ z, double* __restrict__ p,
+                                                               const T* __restrict__ z, T* __restrict__ p,
                                                                const KrylovState* S, int first) {
   if (!first && S->done) return;
   const double beta = first ? 0.0 : S->beta;
@@ -560,8 +568,8 @@ __global__ void __launch_bounds__(kNodeThreads) k_dpcg_update2(GridDims g, DeflP
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const long long i = 3 * n + c;
-      const double pi = first ? 0.0 : p[i];
-      p[i] = ((f >> c) & 1) ? 0.0 : fma(beta, pi, z[i]) - w[c];
+      const T pi = first ? T(0) : p[i];
+      p[i] = ((f >> c) & 1) ? T(0) : (T)(fma((T)beta, pi, z[i]) - (T)w[c]);
     }
   }
 }
@@ -607,16 +615,18 @@ struct DpcgWs {
   uint8_t* fl;
   double *cv, *mu;     // coarse vectors
   double* rpart;       // restriction partials
-  unsigned* rcounter;
   double *P, *Rp, *U;  // sweep scratch
+  // mixed-precision inner solve (FP32 vectors), carved only for the mixed solver
+  float *r32, *p32, *q32, *z32, *x32, *b32, *s32;
 };
 
 constexpr long long kMaxCoarse = 24576;  // coarse vector staged in shared memory (192 KB)
 
-static DpcgWs carve_dpcg(const pyto_operator_t* op, long long nc, void* ws, size_t bytes, size_t* need) {
+static DpcgWs carve_dpcg(const pyto_operator_t* op, long long nc, void* ws, size_t bytes, size_t* need,
+                         bool mixed = false) {
   const GridDims g = make_dims(op);
   Carver cv{(char*)ws, 0, bytes};
-  DpcgWs W;
+  DpcgWs W{};
   W.S = cv.take<KrylovState>(1);
   W.counter = cv.take<unsigned>(64);
   W.part = cv.take<double>(4 * reduce_slots(op));
@@ -626,20 +636,28 @@ static DpcgWs carve_dpcg(const pyto_operator_t* op, long long nc, void* ws, size
   W.z = cv.take<double>(3 * g.nnodes);
   W.w = cv.take<double>(g.nnodes);
   W.fl = cv.take<uint8_t>(g.nnodes);
-  W.rcounter = cv.take<unsigned>(64);
   W.rpart = cv.take<double>((size_t)6 * kRestrictMaxBlocks);
   W.cv = cv.take<double>(nc > 0 ? nc : 1);
   W.mu = cv.take<double>(nc > 0 ? nc : 1);
   W.P = cv.take<double>(kSweepB * kSweepB);
   W.Rp = cv.take<double>(kSweepB * (nc > 0 ? nc : 1));
   W.U = cv.take<double>(kSweepB * (nc > 0 ? nc : 1));
+  if (mixed) {
+    W.r32 = cv.take<float>(3 * g.nnodes);
+    W.p32 = cv.take<float>(3 * g.nnodes);
+    W.q32 = cv.take<float>(3 * g.nnodes);
+    W.z32 = cv.take<float>(3 * g.nnodes);
+    W.x32 = cv.take<float>(3 * g.nnodes);
+    W.b32 = cv.take<float>(3 * g.nnodes);
+    W.s32 = cv.take<float>(g.nelem);
+  }
   *need = cv.off + 256;
   return W;
 }
 
-size_t dpcg_workspace_bytes(const pyto_operator_t* op) {
+size_t dpcg_workspace_bytes(const pyto_operator_t* op, bool mixed) {
   size_t need = 0;
-  carve_dpcg(op, kMaxCoarse, nullptr, 0, &need);
+  carve_dpcg(op, kMaxCoarse, nullptr, 0, &need, mixed);
   return need;
 }
 
@@ -664,15 +682,16 @@ static bool defl_ok(const pyto_deflation_t* d) {
 }
 
 // mu = Einv W_f^T y
-static int coarse_solve(const GridDims& g, const DeflP& dp, const pyto_deflation_t* d, const double* y,
-                        const DpcgWs& W, const KrylovState* S, cudaStream_t st) {
+template <typename T>
+static int coarse_solve(const GridDims& g, const DeflP& dp, const pyto_deflation_t* d, const T* y, const DpcgWs& W,
+                        const KrylovState* S, cudaStream_t st) {
   const int nch = (d->max_group_nodes + kRestrictChunk - 1) / kRestrictChunk;
-  k_restrict<<<dp.ngroups * nch, 256, 0, st>>>(g, dp, d->group_ptr, d->group_nodes, d->group_center, W.fl, y, nch,
-                                               W.rpart, W.rcounter, W.cv);
+  k_restrict<T><<<dp.ngroups * nch, 256, 0, st>>>(g, dp, d->group_ptr, d->group_nodes, d->group_center, W.fl, y,
+                                                  nch, W.rpart);
   PYTO_COUNT(1);
   const size_t shm = (size_t)dp.nc * sizeof(double);
   const int nb = (int)std::min<long long>((dp.nc + 7) / 8, 4 * kNumSMs);
-  k_coarse_gemv<<<nb, 256, shm, st>>>(dp.nc, d->coarse_inv, W.cv, W.mu, S);
+  k_coarse_gemv<<<nb, 256, shm, st>>>(dp.nc, dp.modes, nch, d->coarse_inv, W.rpart, W.mu, S);
   PYTO_COUNT(1);
   PYTO_LAUNCH_CHECK();
   return PYTO_OK;
@@ -737,6 +756,98 @@ extern "C" int pyto_dpcg_setup(const pyto_operator_t* op, const double* s, const
   return PYTO_OK;
 }
 
+namespace pyto {
+
+template <typename T>
+struct DVec {
+  T *r, *p, *q, *z;
+};
+
+int launch_matvec32(const pyto_operator_t* op, const float* s, const uint8_t* mask, const float* u, float* y,
+                    int mode, double* part, unsigned* counter, double* dot, cudaStream_t st);
+
+static int matvec_t(const pyto_operator_t* op, const double* s, const uint8_t* mask, const double* u, double* y,
+                    double* part, unsigned* counter, double* dot, cudaStream_t st) {
+  return launch_matvec64(op, s, mask, u, y, PYTO_MASK_IN | PYTO_MASK_OUT, part, counter, dot, st);
+}
+static int matvec_t(const pyto_operator_t* op, const float* s, const uint8_t* mask, const float* u, float* y,
+                    double* part, unsigned* counter, double* dot, cudaStream_t st) {
+  return launch_matvec32(op, s, mask, u, y, PYTO_MASK_IN | PYTO_MASK_OUT, part, counter, dot, st);
+}
+
+// One deflated PCG run (src/deflation.py:504-584) in vector precision T;
+// scalars, reductions and the coarse space are FP64.  Jacobi data (W.w, W.fl)
+// must be set.  On return *hs holds the final device state.
+template <typename T>
+static int dpcg_run(const pyto_operator_t* op, const T* s, const uint8_t* mask, const pyto_deflation_t* defl,
+                    const T* b, T* u, DVec<T> V, const DpcgWs& W, double rtol, int max_iters, int stop_rule,
+                    int every, KrylovState* hs, cudaStream_t st) {
+  const DeflP dp = make_deflp(op, defl);
+  const GridDims g = make_dims(op);
+  const Prec pc = make_prec(op);
+  int rc;
+  k_state_init2<<<1, 1, 0, st>>>(W.S, rtol, max_iters, stop_rule);
+  PYTO_COUNT(1);
+  // coarse start: x = W Einv W_f^T b   (src/deflation.py:532-537)
+  if ((rc = coarse_solve(g, dp, defl, b, W, nullptr, st))) return rc;
+  k_prolong<T><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center, W.mu, W.fl, u);
+  PYTO_COUNT(1);
+  // r = b - K x, z = M r
+  if ((rc = matvec_t(op, s, mask, u, V.q, nullptr, nullptr, nullptr, st))) return rc;
+  k_dpcg_init<T><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, pc, b, V.q, W.w, W.fl, V.r, V.z, W.S, W.part, W.counter);
+  PYTO_COUNT(1);
+  // p0 = z - W Einv W^T K z
+  if ((rc = matvec_t(op, s, mask, V.z, V.q, nullptr, nullptr, nullptr, st))) return rc;
+  if ((rc = coarse_solve(g, dp, defl, V.q, W, nullptr, st))) return rc;
+  k_dpcg_update2<T><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center, W.mu, W.fl,
+                                                          V.z, V.p, W.S, 1);
+  PYTO_COUNT(1);
+  PYTO_LAUNCH_CHECK();
+  PYTO_CUDA(cudaMemcpyAsync(hs, W.S, sizeof(*hs), cudaMemcpyDeviceToHost, st));
+  PYTO_CUDA(cudaStreamSynchronize(st));
+  while (!hs->done && hs->iters < max_iters) {
+    for (int k = 0; k < every; ++k) {
+      if ((rc = matvec_t(op, s, mask, V.p, V.q, W.part, W.counter, &W.S->pq, st))) return rc;
+      k_dpcg_update1<T><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, pc, W.w, W.fl, u, V.r, V.z, V.p, V.q, W.S, W.part,
+                                                              W.counter);
+      PYTO_COUNT(1);
+      // K z -> q (q is free again), mu = Einv W^T K z, p = z + beta p - W mu
+      if ((rc = matvec_t(op, s, mask, V.z, V.q, nullptr, nullptr, nullptr, st))) return rc;
+      if ((rc = coarse_solve(g, dp, defl, V.q, W, W.S, st))) return rc;
+      k_dpcg_update2<T><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center, W.mu,
+                                                              W.fl, V.z, V.p, W.S, 0);
+      PYTO_COUNT(1);
+    }
+    PYTO_LAUNCH_CHECK();
+    PYTO_CUDA(cudaMemcpyAsync(hs, W.S, sizeof(*hs), cudaMemcpyDeviceToHost, st));
+    PYTO_CUDA(cudaStreamSynchronize(st));
+  }
+  return PYTO_OK;
+}
+
+template <typename A, typename B>
+__global__ void k_cast(long long n, const A* __restrict__ a, B* __restrict__ b) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    b[i] = (B)a[i];
+}
+
+// b32 = (float)(b - t)  (fixed entries are masked by the inner solver)
+__global__ void k_residual_f32(long long n, const double* __restrict__ b, const double* __restrict__ t,
+                               float* __restrict__ b32) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    b32[i] = (float)(b[i] - t[i]);
+}
+
+// u += (double) x
+__global__ void k_add_f32(long long n, const float* __restrict__ x, double* __restrict__ u) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    u[i] += (double)x[i];
+}
+
+}  // namespace pyto
+
+using namespace pyto;
+
 extern "C" int pyto_dpcg_solve(const pyto_operator_t* op, const double* s, const uint8_t* mask,
                                const pyto_deflation_t* defl, const double* b, double* u, const pyto_solve_cfg_t* cfg,
                                pyto_solve_status_t* status, void* ws, size_t ws_bytes, void* stream) {
@@ -750,60 +861,15 @@ extern "C" int pyto_dpcg_solve(const pyto_operator_t* op, const double* s, const
   if (!ws || ws_bytes < need) return PYTO_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
   const GridDims g = make_dims(op);
-  const Prec pc = make_prec(op);
-  const int mm = PYTO_MASK_IN | PYTO_MASK_OUT;
   PYTO_CUDA(cudaMemsetAsync(W.counter, 0, 64 * sizeof(unsigned), st));
-  PYTO_CUDA(cudaMemsetAsync(W.rcounter, 0, 64 * sizeof(unsigned), st));
-  k_state_init2<<<1, 1, 0, st>>>(W.S, cfg->rtol, cfg->max_iters, cfg->stop_rule);
-  PYTO_COUNT(1);
-  rc = pyto_jacobi(op, s, mask, W.w, W.fl, nullptr, stream);
-  if (rc) return rc;
-  // coarse start: x = W Einv W_f^T b   (src/deflation.py:532-537)
-  rc = coarse_solve(g, dp, defl, b, W, nullptr, st);
-  if (rc) return rc;
-  k_prolong<<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center, W.mu, W.fl, u);
-  PYTO_COUNT(1);
-  // r = b - K x, z = M r
-  rc = launch_matvec64(op, s, mask, u, W.q, mm, nullptr, nullptr, nullptr, st);
-  if (rc) return rc;
-  k_dpcg_init<<<kNodeBlocks, kNodeThreads, 0, st>>>(g, pc, b, W.q, W.w, W.fl, W.r, W.z, W.S, W.part, W.counter);
-  PYTO_COUNT(1);
-  // p0 = z - W Einv W^T K z
-  rc = launch_matvec64(op, s, mask, W.z, W.q, mm, nullptr, nullptr, nullptr, st);
-  if (rc) return rc;
-  rc = coarse_solve(g, dp, defl, W.q, W, nullptr, st);
-  if (rc) return rc;
-  k_dpcg_update2<<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center, W.mu, W.fl, W.z,
-                                                       W.p, W.S, 1);
-  PYTO_COUNT(1);
-  PYTO_LAUNCH_CHECK();
-  const int every = std::max(1, cfg->check_every);
+  if ((rc = pyto_jacobi(op, s, mask, W.w, W.fl, nullptr, stream))) return rc;
   KrylovState hs{};
-  PYTO_CUDA(cudaMemcpyAsync(&hs, W.S, sizeof(hs), cudaMemcpyDeviceToHost, st));
-  PYTO_CUDA(cudaStreamSynchronize(st));
-  while (!hs.done && hs.iters < cfg->max_iters) {
-    for (int k = 0; k < every; ++k) {
-      rc = launch_matvec64(op, s, mask, W.p, W.q, mm, W.part, W.counter, &W.S->pq, st);
-      if (rc) return rc;
-      k_dpcg_update1<<<kNodeBlocks, kNodeThreads, 0, st>>>(g, pc, W.w, W.fl, u, W.r, W.z, W.p, W.q, W.S, W.part,
-                                                           W.counter);
-      PYTO_COUNT(1);
-      // K z -> q (q is free again), mu = Einv W^T K z, p = z + beta p - W mu
-      rc = launch_matvec64(op, s, mask, W.z, W.q, mm, nullptr, nullptr, nullptr, st);
-      if (rc) return rc;
-      rc = coarse_solve(g, dp, defl, W.q, W, W.S, st);
-      if (rc) return rc;
-      k_dpcg_update2<<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center, W.mu, W.fl,
-                                                           W.z, W.p, W.S, 0);
-      PYTO_COUNT(1);
-    }
-    PYTO_LAUNCH_CHECK();
-    PYTO_CUDA(cudaMemcpyAsync(&hs, W.S, sizeof(hs), cudaMemcpyDeviceToHost, st));
-    PYTO_CUDA(cudaStreamSynchronize(st));
-  }
-  const KrylovState before = hs;
-  rc = launch_matvec64(op, s, mask, u, W.q, mm, nullptr, nullptr, nullptr, st);
+  rc = dpcg_run<double>(op, s, mask, defl, b, u, DVec<double>{W.r, W.p, W.q, W.z}, W, cfg->rtol, cfg->max_iters,
+                        cfg->stop_rule, std::max(1, cfg->check_every), &hs, st);
   if (rc) return rc;
+  const KrylovState before = hs;
+  if ((rc = launch_matvec64(op, s, mask, u, W.q, PYTO_MASK_IN | PYTO_MASK_OUT, nullptr, nullptr, nullptr, st)))
+    return rc;
   k_true_residual2<<<kNodeBlocks, kNodeThreads, 0, st>>>(g, b, W.q, W.fl, W.S, W.part, W.counter);
   PYTO_COUNT(1);
   PYTO_LAUNCH_CHECK();
@@ -817,4 +883,71 @@ extern "C" int pyto_dpcg_solve(const pyto_operator_t* op, const double* s, const
   status->true_rel_res = hs.bb > 0 ? sqrt(hs.true_rr / hs.bb) : 0.0;
   if (hs.breakdown) return PYTO_ERR_BREAKDOWN;
   return hs.converged ? PYTO_OK : PYTO_NOT_CONVERGED;
+}
+
+extern "C" int pyto_dpcg_mixed_solve(const pyto_operator_t* op, const double* s, const uint8_t* mask,
+                                     const pyto_deflation_t* defl, const double* b, double* u,
+                                     const pyto_solve_cfg_t* cfg, double inner_rtol, pyto_solve_status_t* status,
+                                     void* ws, size_t ws_bytes, void* stream) {
+  if (!op || !s || !b || !u || !cfg || !status || !defl_ok(defl)) return PYTO_ERR_ARG;
+  if (!(cfg->rtol > 0.0) || !(inner_rtol > 0.0) || !(inner_rtol < 1.0) || cfg->max_iters < 0) return PYTO_ERR_ARG;
+  const DeflP dp = make_deflp(op, defl);
+  int rc = gemv_smem_ok(dp.nc);
+  if (rc) return rc;
+  size_t need = 0;
+  DpcgWs W = carve_dpcg(op, dp.nc, ws, ws_bytes, &need, true);
+  if (!ws || ws_bytes < need) return PYTO_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  const GridDims g = make_dims(op);
+  const long long nd = 3 * g.nnodes;
+  const int nb = (int)std::min<long long>((nd + 255) / 256, 8 * kNumSMs);
+  PYTO_CUDA(cudaMemsetAsync(W.counter, 0, 64 * sizeof(unsigned), st));
+  if ((rc = pyto_jacobi(op, s, mask, W.w, W.fl, nullptr, stream))) return rc;
+  k_cast<double, float><<<nb, 256, 0, st>>>(g.nelem, s, W.s32);
+  PYTO_COUNT(1);
+  PYTO_CUDA(cudaMemsetAsync(u, 0, nd * sizeof(double), st));
+  // FP64 outer loop: r = b - K u in FP64, FP32 deflated PCG on K d = r, u += d
+  KrylovState hs{}, inner{};
+  int total = 0, cycles = 0;
+  double rel = 1.0;
+  bool conv = false, brk = false;
+  for (;;) {
+    if (cycles == 0) {
+      PYTO_CUDA(cudaMemsetAsync(W.q, 0, nd * sizeof(double), st));
+    } else if ((rc = launch_matvec64(op, s, mask, u, W.q, PYTO_MASK_IN | PYTO_MASK_OUT, nullptr, nullptr, nullptr,
+                                     st))) {
+      return rc;
+    }
+    k_true_residual2<<<kNodeBlocks, kNodeThreads, 0, st>>>(g, b, W.q, W.fl, W.S, W.part, W.counter);
+    PYTO_COUNT(1);
+    PYTO_LAUNCH_CHECK();
+    PYTO_CUDA(cudaMemcpyAsync(&hs, W.S, sizeof(hs), cudaMemcpyDeviceToHost, st));
+    PYTO_CUDA(cudaStreamSynchronize(st));
+    rel = hs.bb > 0 ? sqrt(hs.true_rr / hs.bb) : 0.0;
+    if (rel <= cfg->rtol || hs.bb == 0.0) {
+      conv = true;
+      break;
+    }
+    if (total >= cfg->max_iters || brk) break;
+    // r (FP64) = b - K u, formed in FP32 as the inner right-hand side
+    k_residual_f32<<<nb, 256, 0, st>>>(nd, b, W.q, W.b32);
+    PYTO_COUNT(1);
+    rc = dpcg_run<float>(op, W.s32, mask, defl, W.b32, W.x32, DVec<float>{W.r32, W.p32, W.q32, W.z32}, W,
+                         inner_rtol, cfg->max_iters - total, 0, std::max(1, cfg->check_every), &inner, st);
+    if (rc) return rc;
+    total += inner.iters;
+    brk = inner.breakdown != 0;
+    k_add_f32<<<nb, 256, 0, st>>>(nd, W.x32, u);
+    PYTO_COUNT(1);
+    ++cycles;
+    if (inner.iters == 0) break;  // no progress possible
+  }
+  status->converged = conv ? 1 : 0;
+  status->iters = total;
+  status->breakdown = brk ? 1 : 0;
+  status->reserved = cycles;
+  status->rel_res = rel;
+  status->true_rel_res = rel;
+  if (brk && !conv) return PYTO_ERR_BREAKDOWN;
+  return conv ? PYTO_OK : PYTO_NOT_CONVERGED;
 }

@@ -24,35 +24,40 @@ namespace pyto {
 // Four plane slots are in flight: ez-1 (output: BC mask and u for the fused
 // dot), ez and ez+1 (compute), ez+2 (being staged).
 // ---------------------------------------------------------------------------
-template <int TY>
+template <typename T, int TY>
 struct MvSmem {
   static constexpr int TX = 32, NT = TX * TY, PX = TX + 1, PY = TY + 1, PLANE = PX * PY, RING = 5;
-  static constexpr size_t su = RING * 3 * PLANE;  // doubles
-  static constexpr size_t sG = 12 * NT;           // doubles
-  static constexpr size_t sc = 2 * 3 * TY * TX;   // doubles
-  static constexpr size_t bytes = 8 * (su + sG + sc) + RING * PLANE + 16;
+  static constexpr size_t su = RING * 3 * PLANE;  // T
+  static constexpr size_t sG = 12 * NT;           // T
+  static constexpr size_t sc = 2 * 3 * TY * TX;   // T
+  static constexpr size_t bytes = sizeof(T) * (su + sG + sc) + RING * PLANE + 16;
 };
 
-__device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc, bool valid) {
+// asynchronous global->shared copy of one T (4 or 8 bytes); zero-fill when !valid
+template <typename T>
+__device__ __forceinline__ void cp_async_t(T* sdst, const T* gsrc, bool valid) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
-  const int n = valid ? 8 : 0;  // 0: zero-fill, the source is not read
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gsrc), "r"(n) : "memory");
+  const int n = valid ? (int)sizeof(T) : 0;  // 0: zero-fill, the source is not read
+  if (sizeof(T) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gsrc), "r"(n) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(gsrc), "r"(n) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-template <int TY, bool DOT, bool MASKIN, int MINB>
+template <typename T, int TY, bool DOT, bool MASKIN, int MINB>
 __global__ void __launch_bounds__(32 * TY, MINB)
-    k_matvec64(GridDims g, KHat kh, const double* __restrict__ s, const uint8_t* __restrict__ mask,
-               const double* __restrict__ u, double* __restrict__ y, int zc, int mode, double* part,
-               unsigned* counter, double* dot_out) {
-  using M = MvSmem<TY>;
+    k_matvec(GridDims g, KHat kh, const T* __restrict__ s, const uint8_t* __restrict__ mask,
+             const T* __restrict__ u, T* __restrict__ y, int zc, int mode, double* part, unsigned* counter,
+             double* dot_out) {
+  using M = MvSmem<T, TY>;
   constexpr int TX = M::TX, NT = M::NT, PX = M::PX, PLANE = M::PLANE;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double* su = reinterpret_cast<double*>(smem_raw);  // [RING][3][PLANE]
-  double* sG = su + M::su;                           // [12][NT] pending top-face accumulators
-  double* sc = sG + M::sG;                           // [2][3][TY][TX] y-combine partials
+  T* su = reinterpret_cast<T*>(smem_raw);  // [RING][3][PLANE]
+  T* sG = su + M::su;                      // [12][NT] pending top-face accumulators
+  T* sc = sG + M::sG;                      // [2][3][TY][TX] y-combine partials
   uint8_t* smk = reinterpret_cast<uint8_t*>(sc + M::sc);  // [RING][PLANE] BC mask
   __shared__ double sred[NT / 32];
 
@@ -93,19 +98,19 @@ __global__ void __launch_bounds__(32 * TY, MINB)
   // plane k is issued into the slot held by `slot`; n_off: its first node of the plane
   auto issue_plane = [&](int k, int slot) {
     const bool kin = k >= 0 && k < g.sz;
-    double* d = su + slot * (3 * PLANE);
+    T* d = su + slot * (3 * PLANE);
     const int nb = kin ? pn * k : 0;
     {
       const bool v = kin && offm >= 0;
-      const double* src = u + 3 * (v ? nb + offm : 0);
+      const T* src = u + 3 * (v ? nb + offm : 0);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) cp_async8(d + c * PLANE + sim, src + c, v);
+      for (int c = 0; c < 3; ++c) cp_async_t(d + c * PLANE + sim, src + c, v);
     }
     if (has_e) {
       const bool v = kin && offe >= 0;
-      const double* src = u + 3 * (v ? nb + offe : 0);
+      const T* src = u + 3 * (v ? nb + offe : 0);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) cp_async8(d + c * PLANE + sie, src + c, v);
+      for (int c = 0; c < 3; ++c) cp_async_t(d + c * PLANE + sie, src + c, v);
     }
     cp_async_commit();
   };
@@ -123,8 +128,8 @@ __global__ void __launch_bounds__(32 * TY, MINB)
     d[sim] = (uint8_t)mm;
     if (has_e) d[sie] = (uint8_t)me;
   };
-  auto face = [&](int slot, double (&F)[3][4]) {
-    const double* b = su + slot * (3 * PLANE) + sim;
+  auto face = [&](int slot, T (&F)[3][4]) {
+    const T* b = su + slot * (3 * PLANE) + sim;
     int m00 = 0, m10 = 0, m01 = 0, m11 = 0;
     if (MASKIN) {
       const uint8_t* mb = smk + slot * PLANE + sim;
@@ -135,13 +140,13 @@ __global__ void __launch_bounds__(32 * TY, MINB)
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const double* bc = b + c * PLANE;
-      double a00 = bc[0], a10 = bc[1], a01 = bc[PX], a11 = bc[PX + 1];
+      const T* bc = b + c * PLANE;
+      T a00 = bc[0], a10 = bc[1], a01 = bc[PX], a11 = bc[PX + 1];
       if (MASKIN) {
-        if ((m00 >> c) & 1) a00 = 0.0;
-        if ((m10 >> c) & 1) a10 = 0.0;
-        if ((m01 >> c) & 1) a01 = 0.0;
-        if ((m11 >> c) & 1) a11 = 0.0;
+        if ((m00 >> c) & 1) a00 = T(0);
+        if ((m10 >> c) & 1) a10 = T(0);
+        if ((m01 >> c) & 1) a01 = T(0);
+        if ((m11 >> c) & 1) a11 = T(0);
       }
       face_fwd(a00, a10, a01, a11, F[c]);
     }
@@ -149,21 +154,21 @@ __global__ void __launch_bounds__(32 * TY, MINB)
   const bool owner = tx < TX - 1 && ty < TY - 1 && (X0 + tx) < g.sx && (Y0 + ty) < g.sy;
   const int li = (ty + 1) * PX + tx + 1;  // owned node in the tile
   double dot = 0.0;
-  double cT[3] = {0.0, 0.0, 0.0};
+  T cT[3] = {T(0), T(0), T(0)};
   auto output = [&](int k, int slot) {  // owned node of plane k
     if (!owner) return;
     const int mk = mask_out ? (int)smk[slot * PLANE + li] : 0;
     const int dof = 3 * ((X0 + tx) + g.sx * (Y0 + ty) + pn * k);
-    const double* scb = sc + (k & 1) * (3 * TY * TX) + (ty + 1) * TX + tx;
+    const T* scb = sc + (k & 1) * (3 * TY * TX) + (ty + 1) * TX + tx;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      double v = cT[c] + scb[c * TY * TX];
-      if ((mk >> c) & 1) v = 0.0;
+      T v = cT[c] + scb[c * TY * TX];
+      if ((mk >> c) & 1) v = T(0);
       y[dof + c] = v;
       if (DOT) {
-        double uv = su[slot * (3 * PLANE) + c * PLANE + li];
-        if (MASKIN && ((smk[slot * PLANE + li] >> c) & 1)) uv = 0.0;
-        dot = fma(uv, v, dot);
+        T uv = su[slot * (3 * PLANE) + c * PLANE + li];
+        if (MASKIN && ((smk[slot * PLANE + li] >> c) & 1)) uv = T(0);
+        dot = fma((double)uv, (double)v, dot);
       }
     }
   };
@@ -179,9 +184,9 @@ __global__ void __launch_bounds__(32 * TY, MINB)
   load_mask(Z0);
   store_mask(r2);
   load_mask(Z0 + 1);
-  double s_next = (col_in && Z0 - 1 >= 0) ? __ldg(s + eidx) : 0.0;
+  T s_next = (col_in && Z0 - 1 >= 0) ? __ldg(s + eidx) : T(0);
 #pragma unroll
-  for (int i = 0; i < 12; ++i) sG[i * NT + tid] = 0.0;
+  for (int i = 0; i < 12; ++i) sG[i * NT + tid] = T(0);
   if (Z0 + 1 <= Z1) issue_plane(Z0 + 1, r3);
   else cp_async_commit();
 
@@ -194,11 +199,11 @@ __global__ void __launch_bounds__(32 * TY, MINB)
     load_mask(ez + 3);
     if (ez + 3 <= Z1) issue_plane(ez + 3, r4);
     else cp_async_commit();
-    const double se = s_next;
+    const T se = s_next;
     eidx += pe;
-    s_next = (col_in && ez + 1 < Z1 && ez + 1 < g.nz) ? __ldg(s + eidx) : 0.0;
-    const double sv = (ez >= 0 && ez < g.nz) ? se : 0.0;
-    double Fb[3][4], Ft[3][4], Gs[3][4];
+    s_next = (col_in && ez + 1 < Z1 && ez + 1 < g.nz) ? __ldg(s + eidx) : T(0);
+    const T sv = (ez >= 0 && ez < g.nz) ? se : T(0);
+    T Fb[3][4], Ft[3][4], Gs[3][4];
     face(r1, Fb);
     face(r2, Ft);
 #pragma unroll
@@ -208,29 +213,30 @@ __global__ void __launch_bounds__(32 * TY, MINB)
     // classes in pairs (qp, qp^4): after a pair, its three top-face entries are final
 #pragma unroll
     for (int qp = 0; qp < 4; ++qp) {
-      double gt[3];
+      T gt[3];
       bool gt_set[3] = {false, false, false};
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int q = qp + 4 * h;
-        double v[3];
+        T v[3];
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
           const int m = member_mode(q, d);
           const int f = m & 3;
-          v[d] = (m == 0) ? 0.0 : ((m & 4) ? sv * (Ft[d][f] - Fb[d][f]) : sv * (Ft[d][f] + Fb[d][f]));
+          v[d] = (m == 0) ? T(0) : ((m & 4) ? sv * (Ft[d][f] - Fb[d][f]) : sv * (Ft[d][f] + Fb[d][f]));
         }
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
           const int m = member_mode(q, c);
           if (m == 0) continue;
           const int f = m & 3;
-          double o = 0.0;
+          T o = T(0);
           bool first = true;
 #pragma unroll
           for (int d = 0; d < 3; ++d) {
             if (member_mode(q, d) == 0) continue;
-            o = first ? kh.b[q][3 * c + d] * v[d] : fma(kh.b[q][3 * c + d], v[d], o);
+            const T kc = (T)kh.b[q][3 * c + d];
+            o = first ? kc * v[d] : fma(kc, v[d], o);
             first = false;
           }
           Gs[c][f] += (m & 4) ? -o : o;
@@ -239,13 +245,13 @@ __global__ void __launch_bounds__(32 * TY, MINB)
         }
       }
 #pragma unroll
-      for (int c = 0; c < 3; ++c) sG[(c * 4 + ((qp ^ (1 << c)) & 3)) * NT + tid] = gt_set[c] ? gt[c] : 0.0;
+      for (int c = 0; c < 3; ++c) sG[(c * 4 + ((qp ^ (1 << c)) & 3)) * NT + tid] = gt_set[c] ? gt[c] : T(0);
     }
     if (ez >= Z0) {
-      double* scb = sc + (ez & 1) * (3 * TY * TX) + ty * TX + tx;
+      T* scb = sc + (ez & 1) * (3 * TY * TX) + ty * TX + tx;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        double c00, c10, c01, c11;
+        T c00, c10, c01, c11;
         face_inv(Gs[c], c00, c10, c01, c11);
         cT[c] = c11 + __shfl_down_sync(0xffffffffu, c01, 1);
         scb[c * TY * TX] = c10 + __shfl_down_sync(0xffffffffu, c00, 1);
@@ -269,49 +275,65 @@ __global__ void __launch_bounds__(32 * TY, MINB)
   }
 }
 
-template <int TY, bool DOT, bool MI, int MINB>
-static int launch_mv_t(const MvLaunch& L, size_t smem, const GridDims& g, const KHat& kh, const double* s,
-                       const uint8_t* mask, const double* u, double* y, int mode, double* part, unsigned* counter,
-                       double* dot, cudaStream_t st) {
+template <typename T, int TY, bool DOT, bool MI, int MINB>
+static int launch_mv_t(const MvLaunch& L, size_t smem, const GridDims& g, const KHat& kh, const T* s,
+                       const uint8_t* mask, const T* u, T* y, int mode, double* part, unsigned* counter, double* dot,
+                       cudaStream_t st) {
   static bool attr = false;
   if (!attr) {
-    PYTO_CUDA(cudaFuncSetAttribute(k_matvec64<TY, DOT, MI, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    PYTO_CUDA(cudaFuncSetAttribute(k_matvec<T, TY, DOT, MI, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem));
     attr = true;
   }
-  k_matvec64<TY, DOT, MI, MINB><<<L.grid, 32 * TY, smem, st>>>(g, kh, s, mask, u, y, L.zc, mode, part, counter, dot);
+  k_matvec<T, TY, DOT, MI, MINB><<<L.grid, 32 * TY, smem, st>>>(g, kh, s, mask, u, y, L.zc, mode, part, counter, dot);
   PYTO_COUNT(1);
   PYTO_LAUNCH_CHECK();
   return PYTO_OK;
 }
 
-template <int TY, int MINB>
-static int launch_mv(const GridDims& g, const KHat& kh, const double* s, const uint8_t* mask, const double* u,
-                     double* y, int mode, double* part, unsigned* counter, double* dot, cudaStream_t st) {
-  const size_t smem = MvSmem<TY>::bytes;
+template <typename T, int TY, int MINB>
+static int launch_mv(const GridDims& g, const KHat& kh, const T* s, const uint8_t* mask, const T* u, T* y, int mode,
+                     double* part, unsigned* counter, double* dot, cudaStream_t st) {
+  const size_t smem = MvSmem<T, TY>::bytes;
   const MvLaunch L = matvec_launch<32, TY>(g);
   const bool mi = (mode & PYTO_MASK_IN) && mask != nullptr;
   if (dot)
-    return mi ? launch_mv_t<TY, true, true, MINB>(L, smem, g, kh, s, mask, u, y, mode, part, counter, dot, st)
-              : launch_mv_t<TY, true, false, MINB>(L, smem, g, kh, s, mask, u, y, mode, part, counter, dot, st);
-  return mi ? launch_mv_t<TY, false, true, MINB>(L, smem, g, kh, s, mask, u, y, mode, nullptr, nullptr, nullptr, st)
-            : launch_mv_t<TY, false, false, MINB>(L, smem, g, kh, s, mask, u, y, mode, nullptr, nullptr, nullptr, st);
+    return mi ? launch_mv_t<T, TY, true, true, MINB>(L, smem, g, kh, s, mask, u, y, mode, part, counter, dot, st)
+              : launch_mv_t<T, TY, true, false, MINB>(L, smem, g, kh, s, mask, u, y, mode, part, counter, dot, st);
+  return mi ? launch_mv_t<T, TY, false, true, MINB>(L, smem, g, kh, s, mask, u, y, mode, nullptr, nullptr, nullptr,
+                                                    st)
+            : launch_mv_t<T, TY, false, false, MINB>(L, smem, g, kh, s, mask, u, y, mode, nullptr, nullptr, nullptr,
+                                                     st);
 }
 
 // Tile variant of the FP64 matvec (2 = default: fastest measured at 192x96x96):
 //   0: 32x8 threads, 2 CTAs/SM (128 registers)   1: 32x8, 1 CTA/SM (no register cap)
 //   2: 32x4, 3 CTAs/SM                            3: 32x16, 1 CTA/SM
 static int g_mv_variant = 2;
+// Tile variant of the FP32 matvec (same numbering; 0 = default)
+static int g_mv32_variant = 0;
 
 int launch_matvec64(const pyto_operator_t* op, const double* s, const uint8_t* mask, const double* u, double* y,
                     int mode, double* part, unsigned* counter, double* dot, cudaStream_t st) {
   const GridDims g = make_dims(op);
   const KHat kh = make_khat(op);
   switch (g_mv_variant) {
-    case 1: return launch_mv<8, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
-    case 2: return launch_mv<4, 3>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
-    case 3: return launch_mv<16, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
-    default: return launch_mv<8, 2>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
+    case 1: return launch_mv<double, 8, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
+    case 2: return launch_mv<double, 4, 3>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
+    case 3: return launch_mv<double, 16, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
+    default: return launch_mv<double, 8, 2>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
+  }
+}
+
+int launch_matvec32(const pyto_operator_t* op, const float* s, const uint8_t* mask, const float* u, float* y,
+                    int mode, double* part, unsigned* counter, double* dot, cudaStream_t st) {
+  const GridDims g = make_dims(op);
+  const KHat kh = make_khat(op);
+  switch (g_mv32_variant) {
+    case 1: return launch_mv<float, 8, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
+    case 2: return launch_mv<float, 4, 3>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
+    case 3: return launch_mv<float, 16, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
+    default: return launch_mv<float, 8, 2>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
   }
 }
 
@@ -321,6 +343,12 @@ long long matvec_blocks(const pyto_operator_t* op) { return matvec_launch<32, 4>
 int set_matvec_variant(int v) {
   if (v < 0 || v > 3) return PYTO_ERR_ARG;
   g_mv_variant = v;
+  return PYTO_OK;
+}
+
+int set_matvec32_variant(int v) {
+  if (v < 0 || v > 3) return PYTO_ERR_ARG;
+  g_mv32_variant = v;
   return PYTO_OK;
 }
 
@@ -434,4 +462,19 @@ extern "C" int pyto_matvec(const pyto_operator_t* op, const double* s, const uin
     PYTO_CUDA(cudaMemsetAsync(counter, 0, 64 * sizeof(unsigned), (cudaStream_t)stream));
   }
   return launch_matvec64(op, s, mask, u, y, mode, part, counter, dot, (cudaStream_t)stream);
+}
+
+extern "C" int pyto_matvec_f32(const pyto_operator_t* op, const float* s, const uint8_t* mask, const float* u,
+                               float* y, int mode, double* dot, void* ws, size_t ws_bytes, void* stream) {
+  if (!op || !s || !u || !y || u == y) return PYTO_ERR_ARG;
+  double* part = nullptr;
+  unsigned* counter = nullptr;
+  if (dot) {
+    Carver cv{(char*)ws, 0, ws_bytes};
+    counter = cv.take<unsigned>(64);
+    part = cv.take<double>((size_t)matvec_blocks(op));
+    if (!cv.ok()) return PYTO_ERR_WORKSPACE;
+    PYTO_CUDA(cudaMemsetAsync(counter, 0, 64 * sizeof(unsigned), (cudaStream_t)stream));
+  }
+  return launch_matvec32(op, s, mask, u, y, mode, part, counter, dot, (cudaStream_t)stream);
 }

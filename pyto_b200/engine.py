@@ -50,7 +50,6 @@ class HexGrid:
         self.mask = torch.zeros(_round4(self.nnodes), dtype=torch.uint8, device=self.device)
         self.active = None
         self.n_active = self.nelem
-        self._scalars = torch.zeros(8, dtype=F64, device=self.device)
 
     # ---- helpers -------------------------------------------------------------
     @property
@@ -103,11 +102,18 @@ class HexGrid:
     def matvec(self, s, u, mode=A.MASK_IN | A.MASK_OUT, out=None, dot=False):
         """y = K(s) u on full-length vectors (Dirichlet masking per mode)."""
         y = out if out is not None else torch.empty(self.ndof, dtype=F64, device=self.device)
-        d = self._scalars[0:1] if dot else None
+        d = torch.empty(1, dtype=F64, device=self.device) if dot else None
         wsp, wsn = self._ws(A.WS_REDUCE, "reduce") if dot else (None, 0)
         A.call("pyto_matvec", self.opp, A.ptr(s), A.ptr(self.mask), A.ptr(u), A.ptr(y), int(mode), A.ptr(d), wsp, wsn,
                self._st())
         return (y, d) if dot else y
+
+    def matvec_f32(self, s32, u32, mode=A.MASK_IN | A.MASK_OUT, out=None):
+        """FP32 y = K(s) u (the operator of the mixed-precision inner cycles)."""
+        y = out if out is not None else torch.empty(self.ndof, dtype=torch.float32, device=self.device)
+        A.call("pyto_matvec_f32", self.opp, A.ptr(s32), A.ptr(self.mask), A.ptr(u32), A.ptr(y), int(mode), None,
+               None, 0, self._st())
+        return y
 
     def jacobi(self, s):
         winv = torch.empty(self.nnodes, dtype=F64, device=self.device)
@@ -153,12 +159,32 @@ class HexGrid:
         return u, SolveInfo(bool(stt.converged), int(stt.iters), bool(stt.breakdown), float(stt.rel_res),
                             float(stt.true_rel_res), rc)
 
+    def dpcg_mixed(self, s, b, defl, rtol=1e-8, inner_rtol=1e-4, max_iters=4000, check_every=25, out=None,
+                   setup=True):
+        """Deflated PCG in mixed precision: FP64 iterative refinement (true residual
+        ||b - K u|| <= rtol ||b|| in FP64) around FP32 deflated PCG cycles that each
+        reduce the residual by inner_rtol.  info.cycles is the number of cycles."""
+        wsp, wsn = self._ws(A.WS_DPCG_MIXED, "krylov")
+        if setup:
+            A.call("pyto_dpcg_setup", self.opp, A.ptr(s), A.ptr(self.mask), C.byref(defl.struct), wsp, wsn,
+                   self._st())
+        u = out if out is not None else torch.empty(self.ndof, dtype=F64, device=self.device)
+        cfg = self._cfg(rtol, max_iters, 0, check_every, False)
+        stt = A.SolveStatus()
+        rc = A.call("pyto_dpcg_mixed_solve", self.opp, A.ptr(s), A.ptr(self.mask), C.byref(defl.struct), A.ptr(b),
+                    A.ptr(u), C.byref(cfg), float(inner_rtol), C.byref(stt), wsp, wsn, self._st(),
+                    allow=(A.OK, A.NOT_CONVERGED, A.ERR_BREAKDOWN))
+        info = SolveInfo(bool(stt.converged), int(stt.iters), bool(stt.breakdown), float(stt.rel_res),
+                         float(stt.true_rel_res), rc)
+        info.cycles = int(stt.reserved)
+        return u, info
+
     # ---- element quantities ---------------------------------------------------------------
     def energy(self, u, v=None, s=None):
         """ce_e = u_e^T Ke v_e; with s also returns sum_e s_e ce_e (device scalar)."""
         v = u if v is None else v
         ce = torch.empty(self.nelem, dtype=F64, device=self.device)
-        tot = self._scalars[1:2] if s is not None else None
+        tot = torch.empty(1, dtype=F64, device=self.device) if s is not None else None
         wsp, wsn = self._ws(A.WS_REDUCE, "reduce") if s is not None else (None, 0)
         A.call("pyto_elem_energy", self.opp, A.ptr(u), A.ptr(v), A.ptr(s), A.ptr(ce), A.ptr(tot), wsp, wsn,
                self._st())
@@ -176,7 +202,7 @@ class HexGrid:
         return out
 
     def pow_sum(self, vm, P):
-        out = self._scalars[2:3]
+        out = torch.empty(1, dtype=F64, device=self.device)
         wsp, wsn = self._ws(A.WS_REDUCE, "reduce")
         A.call("pyto_pnorm_sum", self.opp, A.ptr(vm), float(P), A.ptr(out), wsp, wsn, self._st())
         return out
@@ -198,7 +224,7 @@ class HexGrid:
 
     def oc_update(self, x, dc, volfrac, move=0.2, xmin=0.001, xmax=1.0):
         """In-place OC update of x; returns max |dx| as a device scalar."""
-        ch = self._scalars[3:4]
+        ch = torch.empty(1, dtype=F64, device=self.device)
         wsp, wsn = self._ws(A.WS_OC, "oc")
         A.call("pyto_oc_update", self.opp, A.ptr(x), A.ptr(dc), A.ptr(self.active), int(self.n_active),
                float(volfrac), float(move), float(xmin), float(xmax), A.ptr(ch), wsp, wsn, self._st())

@@ -35,15 +35,20 @@ def _timeit(fn, reps, warm=3):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--kernel", default="matvec", choices=["matvec", "energy", "filter", "jacobi", "stress", "dpcg", "pcg"])
+    ap.add_argument("--kernel", default="matvec", choices=["matvec", "matvec32", "energy", "filter", "jacobi", "stress", "dpcg",
+                                                          "mixed", "pcg"])
     ap.add_argument("--groups", type=int, default=432, help="deflation groups for --kernel dpcg")
     ap.add_argument("--nel", default="192,96,96")
     ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--warm", type=int, default=3)
     ap.add_argument("--variant", type=int, default=2, help="matvec tile variant (pyto_tune)")
+    ap.add_argument("--variant32", type=int, default=None, help="FP32 matvec tile variant (pyto_tune)")
+    ap.add_argument("--inner-rtol", type=float, default=1e-4, help="inner tolerance for --kernel mixed")
     a = ap.parse_args(argv)
     nel = tuple(int(v) for v in a.nel.split(","))
     A.call("pyto_tune", 0, a.variant)
+    if a.variant32 is not None:
+        A.call("pyto_tune", 1, a.variant32)
     mesh = HexMesher()
     mesh.grid_mesh(nel, (1.0, 1.0, 1.0))
     f, fixed = cantilever(mesh)
@@ -54,6 +59,10 @@ def main(argv=None):
     y = torch.empty_like(u)
     if a.kernel == "matvec":
         fn, nbytes = (lambda: g.matvec(s, u, out=y)), 48 * g.nnodes + 8 * g.nelem + g.nnodes
+    elif a.kernel == "matvec32":
+        s32, u32 = s.float(), u.float()
+        y32 = torch.empty_like(u32)
+        fn, nbytes = (lambda: g.matvec_f32(s32, u32, out=y32)), 24 * g.nnodes + 4 * g.nelem + g.nnodes
     elif a.kernel == "energy":
         fn, nbytes = (lambda: g.energy(u, s=s)), 24 * g.nnodes + 16 * g.nelem
     elif a.kernel == "filter":
@@ -61,21 +70,25 @@ def main(argv=None):
         fn, nbytes = (lambda: g.filter(2.0, A.FILTER_DENSITY, s, out=out)), 16 * g.nelem
     elif a.kernel == "jacobi":
         fn, nbytes = (lambda: g.jacobi(s)), 8 * g.nelem + 33 * g.nnodes
-    elif a.kernel in ("dpcg", "pcg"):
+    elif a.kernel in ("dpcg", "mixed", "pcg"):
         from .deflation import DeflationSolver
         F = g.tensor(f)
-        if a.kernel == "dpcg":
+        if a.kernel in ("dpcg", "mixed"):
             ds = DeflationSolver(shift=1e-14, shift_relative=True)
             ds.create_deflation_groups(mesh, a.groups)
             defl = ds.device_deflation(g)
-            fn = lambda: g.dpcg(s, F, defl, rtol=1e-8, max_iters=5000, stop_rule=0, check_every=20)
+            if a.kernel == "dpcg":
+                fn = lambda: g.dpcg(s, F, defl, rtol=1e-8, max_iters=5000, stop_rule=0, check_every=20)
+            else:
+                fn = lambda: g.dpcg_mixed(s, F, defl, rtol=1e-8, inner_rtol=a.inner_rtol, max_iters=8000,
+                                          check_every=20)
         else:
             fn = lambda: g.pcg(s, F, rtol=1e-8, check_every=20)
         nbytes = 0
     else:
         fn, nbytes = (lambda: g.stress(u, s, 0.5, want=("vm",))), 24 * g.nnodes + 16 * g.nelem
     t = _timeit(fn, a.reps, a.warm)
-    if a.kernel in ("dpcg", "pcg"):
+    if a.kernel in ("dpcg", "mixed", "pcg"):
         _, info = fn()
         print(json.dumps({"kernel": a.kernel, "nel": nel, "ms": t * 1e3, "iters": info.iters,
                           "true_rel_res": info.true_rel_res}))

@@ -193,6 +193,64 @@ def test_dpcg_coarse_spaces_converge(modes, agg):
     assert info.iters < info2.iters
 
 
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+def test_matvec_f32_matches_fp64(variant):
+    """FP32 operator: relative error of K(s)u against the FP64 operator at FP32 rounding."""
+    from pyto_b200 import _capi as A
+    nel = (33, 9, 17)
+    m = O.grid_mesh(*nel)
+    _, fixed = O.cantilever_bc(m)
+    g = _grid(nel, fixed=fixed)
+    rng = np.random.default_rng(7)
+    s64 = _dev(rng.uniform(1e-3, 1.0, m["num_elems"]))
+    u64 = _dev(rng.normal(size=3 * m["num_nodes"]))
+    s32, u32 = s64.float(), u64.float()
+    A.call("pyto_tune", 1, variant)
+    try:
+        y32 = g.matvec_f32(s32, u32)
+    finally:
+        A.call("pyto_tune", 1, 0)
+    y64 = g.matvec(s32.double(), u32.double())
+    err = (y32.double() - y64).abs().max().item()
+    assert err <= 2e-6 * y64.abs().max().item(), err
+
+
+@pytest.mark.parametrize("nel,rtol", [((12, 6, 6), 1e-10), ((32, 16, 16), 1e-8)])
+def test_dpcg_mixed_reaches_fp64_accuracy(nel, rtol):
+    """FP64 refinement around FP32 deflated PCG: the FP64 true residual meets rtol and the
+    compliance agrees with a tighter FP64 Jacobi PCG solve."""
+    from pyto_b200.engine import DeviceDeflation
+    m = O.grid_mesh(*nel)
+    f, fixed = O.cantilever_bc(m)
+    g = _grid(nel, fixed=fixed)
+    rng = np.random.default_rng(1)
+    s, _ = g.simp(_dev(rng.uniform(0.01, 1.0, m["num_elems"])), 3.0, 1e-9)
+    grp, cnt, cen = O.deflation_groups(m["node_xyz"], 8 if nel[0] == 12 else 40)
+    defl = DeviceDeflation(g, grp, cen, modes=6, shift=1e-14, shift_relative=True)
+    b = _dev(f)
+    u, info = g.dpcg_mixed(s, b, defl, rtol=rtol)
+    assert info.converged and info.true_rel_res <= rtol, info
+    r = b - g.matvec(s, u)
+    r[torch.as_tensor(fixed, device="cuda")] = 0
+    assert r.norm().item() <= rtol * b.norm().item() * 1.0000001
+    u2, info2 = g.pcg(s, b, rtol=rtol * 1e-2)
+    assert info2.converged
+    _, C = g.energy(u, s=s)
+    _, C2 = g.energy(u2, s=s)
+    assert abs(C.item() - C2.item()) <= 10 * rtol * abs(C2.item())
+
+
+def test_dpcg_mixed_golden_compliance():
+    from pyto_b200.engine import DeviceDeflation
+    d, m, g, s, ds = _cantilever_case("cantilever_12x6x6_direct.npz", (12, 6, 6), (1.0, 1.0, 1.0))
+    grp, cnt, cen = O.deflation_groups(m["node_xyz"], 8)
+    defl = DeviceDeflation(g, grp, cen, modes=6, shift=1e-10, shift_relative=False)
+    u, info = g.dpcg_mixed(s, _dev(d["f"]), defl, rtol=1e-11)
+    assert info.converged and info.cycles >= 2
+    _, C = g.energy(u, s=s)
+    assert abs(C.item() - float(d["C"])) <= 1e-10 * float(d["C"])
+
+
 def test_stress_vm_pnorm():
     d, m, g, s, ds = _cantilever_case("cantilever_12x6x6_direct.npz", (12, 6, 6), (1.0, 1.0, 1.0))
     u = _dev(d["u"])
