@@ -90,7 +90,7 @@ typedef struct pyto_solve_status {
 typedef struct pyto_deflation {
   int32_t ngroups;
   int32_t modes;               /* 3 or 6 */
-  const int32_t* node_group;   /* [nnodes] group of each node */
+  const int32_t* node_group;   /* [nnodes] group of each node (16-byte aligned) */
   const int32_t* group_ptr;    /* [ngroups+1] CSR offsets of group_nodes */
   const int32_t* group_nodes;  /* [nnodes] node ids sorted by group */
   const double* group_center;  /* [ngroups*3] centroid of each group */
@@ -104,6 +104,14 @@ typedef struct pyto_deflation {
   const int32_t* nbr_list;     /* groups sharing an element with each group (incl. itself), ascending */
   int32_t max_nbr;             /* largest neighbour list (<= 128) */
   int32_t reserved;
+  /* Optional boundary element lists (NULL: the solver applies K to z with a full
+   * matvec before restricting, as src/deflation.py:560-566 does).  A rigid mode of
+   * a group is in the null space of every element whose 8 corners lie in that
+   * group and are free, so W_f^T K z only needs, per group, the elements with a
+   * corner in the group and a corner in another group or on a fixed DOF; the
+   * lists must be rebuilt when the fixed DOFs change. */
+  const int32_t* bel_ptr;      /* [ngroups+1] CSR offsets of bel_list */
+  const int32_t* bel_list;     /* boundary elements of each group, ascending element ids */
 } pyto_deflation_t;
 
 /* ---- version / workspace ------------------------------------------------- */
@@ -190,23 +198,29 @@ int pyto_pcg_solve(const pyto_operator_t* op, const double* s, const uint8_t* ma
 int pyto_dpcg_setup(const pyto_operator_t* op, const double* s, const uint8_t* mask,
                     pyto_deflation_t* defl, void* ws, size_t ws_bytes, void* stream);
 /* Deflated PCG (src/deflation.py:504-584): coarse start, p0 = z - W mu, per iteration
- * one coarse correction; stopping rule per cfg.  Replaces DeflationSolver.deflatedPCG. */
+ * one coarse correction; stopping rule per cfg.  b and u must be 16-byte aligned.  With
+ * boundary lists in defl, W_f^T K z is formed from the group-boundary elements instead
+ * of a second full matvec per iteration.  Replaces DeflationSolver.deflatedPCG. */
 int pyto_dpcg_solve(const pyto_operator_t* op, const double* s, const uint8_t* mask,
                     const pyto_deflation_t* defl, const double* b, double* u,
                     const pyto_solve_cfg_t* cfg, pyto_solve_status_t* status, void* ws,
                     size_t ws_bytes, void* stream);
 
-/* Mixed-precision deflated PCG: FP64 iterative refinement around FP32 deflated PCG
- * cycles.  Each cycle forms the true residual r = b - K u in FP64, solves K d = r with
- * FP32 vectors and FP32 operator (FP64 reductions, FP64 coarse inverse from
- * pyto_dpcg_setup) to ||r_inner|| < inner_rtol ||r||, and updates u += d in FP64; it
- * stops when ||b - K u|| <= cfg->rtol ||b|| in FP64.  cfg->max_iters caps the total
- * inner iterations; status->reserved returns the number of cycles.  Needs a
- * PYTO_WS_DPCG_MIXED workspace.  Replaces DeflationSolver.deflatedPCG
- * (src/deflation.py:504-584) where FP64 accuracy is required at lower cost. */
+/* Mixed-precision deflated PCG with reliable updates.  The Krylov recurrence runs
+ * on FP32 vectors with the FP32 operator (FP64 dot-product reductions and scalars,
+ * the FP64 coarse inverse of pyto_dpcg_setup); the solution is held in FP64.  The
+ * start is the FP64 coarse solve u = W E^-1 W_f^T b.  Whenever the FP32 recursive
+ * residual has dropped by `delta` (0 < delta < 1) since the last update, or meets
+ * cfg->rtol, the FP32 iterate is added to u in FP64 and the residual is replaced by
+ * b - K u computed in FP64; the search direction is kept, so no Krylov information
+ * is discarded.  Convergence is ||b - K u|| <= cfg->rtol ||b||, tested in FP64.
+ * cfg->max_iters caps the FP32 iterations; status->reserved returns the number of
+ * FP64 residual updates.  Needs a PYTO_WS_DPCG_MIXED workspace.  Replaces
+ * DeflationSolver.deflatedPCG (src/deflation.py:504-584) where FP64 accuracy is
+ * required at lower cost. */
 int pyto_dpcg_mixed_solve(const pyto_operator_t* op, const double* s, const uint8_t* mask,
                           const pyto_deflation_t* defl, const double* b, double* u,
-                          const pyto_solve_cfg_t* cfg, double inner_rtol, pyto_solve_status_t* status,
+                          const pyto_solve_cfg_t* cfg, double delta, pyto_solve_status_t* status,
                           void* ws, size_t ws_bytes, void* stream);
 
 /* ---- objectives and sensitivities ------------------------------------------------ */

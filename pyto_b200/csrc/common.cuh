@@ -106,14 +106,17 @@ __device__ __forceinline__ double warp_sum_partials(const double* p, int n) {
 }
 
 // Cross-block reduction: every block deposits its value(s) (thread 0 holds
-// them), the last block to arrive sums all partials in block order and calls
-// `fin(totals)` in its thread 0.  Deterministic: the summation order does not
-// depend on scheduling.  The counter is reset by the last block, so it can be
-// reused by the next launch on the same stream.
+// them), the last block to arrive sums all partials and calls `fin(totals)` in
+// its thread 0.  The last block sums with all its threads (thread t takes
+// partials t, t+blockDim, ... in order; warps combine by xor butterfly; warp
+// sums are added in warp order), so the result is deterministic: the order
+// does not depend on scheduling.  The counter is reset by the last block, so it
+// can be reused by the next launch on the same stream.
 template <int K, typename Fin>
 __device__ __forceinline__ void grid_reduce(const double (&v)[K], double* part /*[K][nblocks]*/,
                                             unsigned* counter, int nblocks, Fin fin) {
   __shared__ bool s_last;
+  __shared__ double s_w[K][32];
   const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
   if (threadIdx.x == 0) {
 #pragma unroll
@@ -123,16 +126,33 @@ __device__ __forceinline__ void grid_reduce(const double (&v)[K], double* part /
     s_last = (t == (unsigned)nblocks - 1u);
   }
   __syncthreads();
-  if (s_last && threadIdx.x < 32) {
-    __threadfence();
+  if (!s_last) return;
+  __threadfence();
+  double acc[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) acc[k] = 0.0;
+  for (int i = threadIdx.x; i < nblocks; i += blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] += __ldcg(part + (size_t)k * nblocks + i);
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+    if (lane == 0) s_w[k][wid] = acc[k];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
     double tot[K];
 #pragma unroll
-    for (int k = 0; k < K; ++k) tot[k] = warp_sum_partials(part + (size_t)k * nblocks, nblocks);
-    if (threadIdx.x == 0) {
-      fin(tot);
-      *counter = 0u;
-      __threadfence();
+    for (int k = 0; k < K; ++k) {
+      tot[k] = 0.0;
+      for (int w = 0; w < nw; ++w) tot[k] += s_w[k][w];
     }
+    fin(tot);
+    *counter = 0u;
+    __threadfence();
   }
 }
 

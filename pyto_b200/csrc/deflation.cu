@@ -247,7 +247,9 @@ __global__ void __launch_bounds__(1024) k_sweep_pivot(long long n, int k0, int b
   }
 }
 
-// Rp = A_K: (copy), U = P Rp   (16 columns per block)
+// Rp = A_K: (copy), U = P Rp   (16 columns per block).  Only the lower tiles
+// (and the full diagonal tiles) of A are current, so row K right of the pivot
+// block is read from column K below it.
 __global__ void __launch_bounds__(256) k_sweep_panel(long long n, int k0, int bk, const double* __restrict__ A,
                                                      const double* __restrict__ P, double* __restrict__ Rp,
                                                      double* __restrict__ U) {
@@ -259,7 +261,7 @@ __global__ void __launch_bounds__(256) k_sweep_panel(long long n, int k0, int bk
     const int i = t / 16, jj = t % 16;
     const long long j = j0 + jj;
     double v = 0.0;
-    if (i < bk && j < n) v = A[(k0 + i) * n + j];
+    if (i < bk && j < n) v = (j < k0 + kSweepB) ? A[(k0 + i) * n + j] : A[j * n + (k0 + i)];
     sR[i][jj] = v;
     if (i < bk && j < n) Rp[i * n + j] = v;
   }
@@ -274,13 +276,19 @@ __global__ void __launch_bounds__(256) k_sweep_panel(long long n, int k0, int bk
   }
 }
 
-// tile update, 64x64 tiles, 256 threads x (4x4) outputs, k in chunks of 32
+// tile update of the lower 64x64 tiles (ti >= tj, one CTA each, 1-D grid),
+// 256 threads x (4x4) outputs, k in chunks of 32
 __global__ void __launch_bounds__(256) k_sweep_update(long long n, int k0, int bk, double* __restrict__ A,
                                                       const double* __restrict__ P, const double* __restrict__ Rp,
                                                       const double* __restrict__ U) {
   __shared__ double sL[32][65];  // A_iK for the tile rows: Rp[k][i]
   __shared__ double sU[32][65];  // U_Kj for the tile cols
-  const long long i0 = (long long)blockIdx.y * 64, j0 = (long long)blockIdx.x * 64;
+  const long long b = blockIdx.x;
+  long long ti = (long long)((sqrt(8.0 * (double)b + 1.0) - 1.0) * 0.5);
+  while (ti * (ti + 1) / 2 > b) --ti;
+  while ((ti + 1) * (ti + 2) / 2 <= b) ++ti;
+  const long long tj = b - ti * (ti + 1) / 2;
+  const long long i0 = ti * 64, j0 = tj * 64;
   const bool rowK = (i0 == k0), colK = (j0 == k0);
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
   if (rowK || colK) {
@@ -332,9 +340,17 @@ __global__ void __launch_bounds__(256) k_sweep_update(long long n, int k0, int b
     }
 }
 
-__global__ void k_negate(long long n, double* A) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    A[i] = -A[i];
+// E^-1 = -A: negate the lower tiles (diagonal tiles in full) and mirror them
+// into the upper tiles; each entry pair is handled by one thread
+__global__ void k_negate_sym(long long n, double* A) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n * n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long i = t / n, j = t - i * n;
+    if ((i >> 6) < (j >> 6)) continue;  // upper tile: written from its mirror
+    const double v = -A[t];
+    A[t] = v;
+    if ((i >> 6) > (j >> 6)) A[j * n + i] = v;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -389,6 +405,204 @@ __global__ void __launch_bounds__(256) k_restrict(GridDims g, DeflP dp, const in
   }
 }
 
+// v = W_f^T K(s) z from the boundary elements of each group.  For element e of
+// group G's list, y_e = s_e Ke z_e in the Hadamard basis (as in the matvec, in
+// the vector precision T), then the rigid modes of G are contracted with y_e at
+// the corners of e that lie in G, free DOFs only, accumulating in FP64.
+// Elements whose corners all lie in G and are free contribute
+// w_e^T Ke z_e = (Ke w_e)^T z_e = 0 and are not listed.
+//
+// Each group's list is cut into chunks of kRkChunk entries, one CTA per chunk
+// (kRkThreads threads, two entries each); cptr is the CSR of chunks per group
+// and cgrp the group of each chunk.  A CTA writes its partial sums; the last
+// CTA of a group to finish (per-group counter) adds the group's partials in
+// chunk order, so the result does not depend on scheduling, and resets the
+// counter.  Output: v[G*modes + a].
+constexpr int kRkThreads = 128;
+constexpr int kRkChunk = 2 * kRkThreads;
+constexpr int kRkMaxChunks = 65536;
+
+// cptr[G] = sum_{G' < G} ceil(len(G') / kRkChunk), cgrp[c] = group of chunk c
+// (one block of 1024 threads)
+__global__ void __launch_bounds__(1024) k_chunk_ptr(int ngroups, const int32_t* __restrict__ bptr,
+                                                    int32_t* __restrict__ cptr, int32_t* __restrict__ cgrp) {
+  __shared__ int sc[1024];
+  const int per = (ngroups + 1023) / 1024;
+  const int g0 = threadIdx.x * per, g1 = min(ngroups, g0 + per);
+  int loc = 0;
+  for (int gg = g0; gg < g1; ++gg) loc += (bptr[gg + 1] - bptr[gg] + kRkChunk - 1) / kRkChunk;
+  sc[threadIdx.x] = loc;
+  __syncthreads();
+  for (int o = 1; o < 1024; o <<= 1) {  // inclusive scan
+    const int v = threadIdx.x >= o ? sc[threadIdx.x - o] : 0;
+    __syncthreads();
+    sc[threadIdx.x] += v;
+    __syncthreads();
+  }
+  int run = sc[threadIdx.x] - loc;
+  for (int gg = g0; gg < g1; ++gg) {
+    cptr[gg] = run;
+    const int nch = (bptr[gg + 1] - bptr[gg] + kRkChunk - 1) / kRkChunk;
+    for (int c = 0; c < nch; ++c) cgrp[run + c] = gg;
+    run += nch;
+  }
+  if (threadIdx.x == 1023) cptr[ngroups] = sc[1023];
+}
+
+// adds the contribution of boundary element e to the 6 mode sums of group G
+template <typename T>
+__device__ __forceinline__ void rk_element(const GridDims& g, const KHat& kh, const DeflP& dp, int e, int G, T se,
+                                           const uint8_t* __restrict__ fl, const int32_t* __restrict__ ngrp,
+                                           double c0, double c1, double c2, const T* __restrict__ z,
+                                           double (&acc)[6]) {
+  const int r = e / g.nx;
+  const int ex = e - r * g.nx;
+  const int ez = r / g.ny;
+  const int ey = r - ez * g.ny;
+  const int n0 = ex + g.sx * (ey + g.sy * ez);
+  const int pn = g.sx * g.sy;
+  int gr[8], mk[8];
+  T u[3][8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int nd = n0 + (k & 1) + g.sx * ((k >> 1) & 1) + pn * (k >> 2);
+    gr[k] = ngrp[nd];
+    mk[k] = fl[nd] & 7;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) u[c][k] = ((mk[k] >> c) & 1) ? T(0) : z[3 * (long long)nd + c];
+  }
+  T Fb[3][4], Ft[3][4], Gb[3][4], Gt[3][4];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    face_fwd(u[c][0], u[c][1], u[c][2], u[c][3], Fb[c]);
+    face_fwd(u[c][4], u[c][5], u[c][6], u[c][7], Ft[c]);
+#pragma unroll
+    for (int f = 0; f < 4; ++f) Gb[c][f] = Gt[c][f] = T(0);
+  }
+  hex8_core<T>(kh, se, Fb, Ft, Gb, Gt);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    face_inv(Gb[c], u[c][0], u[c][1], u[c][2], u[c][3]);
+    face_inv(Gt[c], u[c][4], u[c][5], u[c][6], u[c][7]);
+  }
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    if (gr[k] != G) continue;
+    const double yx = (mk[k] & 1) ? 0.0 : (double)u[0][k], yy = (mk[k] & 2) ? 0.0 : (double)u[1][k],
+                 yz = (mk[k] & 4) ? 0.0 : (double)u[2][k];
+    const double rx = dp.hx * (ex + (k & 1)) - c0, ry = dp.hy * (ey + ((k >> 1) & 1)) - c1,
+                 rz = dp.hz * (ez + (k >> 2)) - c2;
+    acc[0] += yx;
+    acc[1] += yy;
+    acc[2] += yz;
+    acc[3] += -rz * yy + ry * yz;
+    acc[4] += rz * yx - rx * yz;
+    acc[5] += -ry * yx + rx * yy;
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRkThreads, sizeof(T) == 4 ? 6 : 4) k_restrict_K(GridDims g, KHat kh, DeflP dp, const T* __restrict__ s,
+                                                           const uint8_t* __restrict__ fl,
+                                                           const int32_t* __restrict__ ngrp,
+                                                           const double* __restrict__ gc,
+                                                           const int32_t* __restrict__ bptr,
+                                                           const int32_t* __restrict__ blist,
+                                                           const int32_t* __restrict__ cptr,
+                                                           const int32_t* __restrict__ cgrp, const T* __restrict__ z,
+                                                           double* __restrict__ part, unsigned* __restrict__ gcount,
+                                                           double* __restrict__ v, const KrylovState* S) {
+  __shared__ double sred[kRkThreads / 32 * 6];
+  __shared__ int s_last;
+  if (S && S->done) return;
+  const int ch = blockIdx.x;
+  if (ch >= cptr[dp.ngroups]) return;
+  const int G = cgrp[ch];
+  const int c0g = cptr[G], nch = cptr[G + 1] - c0g;
+  const int end = bptr[G + 1];
+  const int t0 = bptr[G] + (ch - c0g) * kRkChunk + threadIdx.x;
+  const double c0 = gc[3 * G], c1 = gc[3 * G + 1], c2 = gc[3 * G + 2];
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  const int e0 = t0 < end ? blist[t0] : -1;
+  const int e1 = t0 + kRkThreads < end ? blist[t0 + kRkThreads] : -1;
+  const T s0 = e0 >= 0 ? s[e0] : T(0);
+  const T s1 = e1 >= 0 ? s[e1] : T(0);
+  if (s0 != T(0)) rk_element<T>(g, kh, dp, e0, G, s0, fl, ngrp, c0, c1, c2, z, acc);
+  if (s1 != T(0)) rk_element<T>(g, kh, dp, e1, G, s1, fl, ngrp, c0, c1, c2, z, acc);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int a = 0; a < 6; ++a) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc[a] += __shfl_down_sync(0xffffffffu, acc[a], o);
+  }
+  if (lane == 0)
+#pragma unroll
+    for (int a = 0; a < 6; ++a) sred[wid * 6 + a] = acc[a];
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    double tt = 0.0;
+#pragma unroll
+    for (int w = 0; w < kRkThreads / 32; ++w) tt += sred[w * 6 + threadIdx.x];
+    if (nch == 1) {  // single chunk: it is the group's sum
+      if (threadIdx.x < dp.modes) v[(size_t)G * dp.modes + threadIdx.x] = tt;
+    } else {
+      part[(size_t)ch * 6 + threadIdx.x] = tt;
+    }
+  }
+  if (nch == 1) return;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = (atomicAdd(&gcount[G], 1u) == (unsigned)(nch - 1));
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (threadIdx.x < dp.modes) {
+    double tt = 0.0;
+    for (int c = c0g; c < c0g + nch; ++c) tt += __ldcg(part + (size_t)c * 6 + threadIdx.x);
+    v[(size_t)G * dp.modes + threadIdx.x] = tt;
+  }
+  if (threadIdx.x == 0) gcount[G] = 0;
+}
+
+// mu = Einv v for a compact coarse vector v (nc entries), one warp per row with
+// 16-byte loads (nc even) and four independent partial sums per lane.
+__global__ void __launch_bounds__(256) k_gemv(long long nc, const double* __restrict__ Einv,
+                                              const double* __restrict__ v, double* __restrict__ mu,
+                                              const KrylovState* S) {
+  extern __shared__ double sv[];
+  if (S && S->done) return;
+  for (long long i = threadIdx.x; i < nc; i += blockDim.x) sv[i] = v[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  for (long long row = (long long)blockIdx.x * 8 + (threadIdx.x >> 5); row < nc; row += (long long)gridDim.x * 8) {
+    const double* a = Einv + row * nc;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    if ((nc & 1) == 0) {
+      const double2* a2p = reinterpret_cast<const double2*>(a);
+      const long long h = nc >> 1;
+      long long j = lane;
+      for (; j + 32 < h; j += 64) {
+        const double2 e0 = __ldg(a2p + j), e1 = __ldg(a2p + j + 32);
+        a0 = fma(e0.x, sv[2 * j], a0);
+        a1 = fma(e0.y, sv[2 * j + 1], a1);
+        a2 = fma(e1.x, sv[2 * j + 64], a2);
+        a3 = fma(e1.y, sv[2 * j + 65], a3);
+      }
+      if (j < h) {
+        const double2 e0 = __ldg(a2p + j);
+        a0 = fma(e0.x, sv[2 * j], a0);
+        a1 = fma(e0.y, sv[2 * j + 1], a1);
+      }
+    } else {
+      for (long long j = lane; j < nc; j += 32) a0 = fma(__ldg(a + j), sv[j], a0);
+    }
+    double acc = (a0 + a1) + (a2 + a3);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) mu[row] = acc;
+  }
+}
+
 // mu = Einv v (one warp per row); v = W^T y is formed while staging it in
 // shared memory, summing each group's chunk partials in chunk order
 __global__ void __launch_bounds__(256) k_coarse_gemv(long long nc, int modes, int nch, const double* __restrict__ Einv,
@@ -406,8 +620,16 @@ __global__ void __launch_bounds__(256) k_coarse_gemv(long long nc, int modes, in
   const int lane = threadIdx.x & 31;
   for (long long row = (long long)blockIdx.x * 8 + (threadIdx.x >> 5); row < nc; row += (long long)gridDim.x * 8) {
     const double* a = Einv + row * nc;
-    double acc = 0.0;
-    for (long long j = lane; j < nc; j += 32) acc = fma(__ldg(a + j), sv[j], acc);
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    long long j = lane;
+    for (; j + 96 < nc; j += 128) {
+      a0 = fma(__ldg(a + j), sv[j], a0);
+      a1 = fma(__ldg(a + j + 32), sv[j + 32], a1);
+      a2 = fma(__ldg(a + j + 64), sv[j + 64], a2);
+      a3 = fma(__ldg(a + j + 96), sv[j + 96], a3);
+    }
+    for (; j < nc; j += 32) a0 = fma(__ldg(a + j), sv[j], a0);
+    double acc = (a0 + a1) + (a2 + a3);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if (lane == 0) mu[row] = acc;
@@ -434,8 +656,8 @@ __device__ __forceinline__ void prolong_node(const GridDims& g, const DeflP& dp,
   }
 }
 
-// x = W mu (masked)
-template <typename T>
+// x = W mu (masked); ADD: x += W mu
+template <typename T, bool ADD = false>
 __global__ void __launch_bounds__(256) k_prolong(GridDims g, DeflP dp, const int32_t* __restrict__ ngrp,
                                                  const double* __restrict__ gc, const double* __restrict__ mu,
                                                  const uint8_t* __restrict__ fl, T* __restrict__ x) {
@@ -445,8 +667,21 @@ __global__ void __launch_bounds__(256) k_prolong(GridDims g, DeflP dp, const int
     prolong_node(g, dp, n, ngrp, gc, mu, w);
     const int f = fl[n];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) x[3 * n + c] = ((f >> c) & 1) ? T(0) : (T)w[c];
+    for (int c = 0; c < 3; ++c) {
+      const T v = ((f >> c) & 1) ? T(0) : (T)w[c];
+      if (ADD)
+        x[3 * n + c] += v;
+      else
+        x[3 * n + c] = v;
+    }
   }
+}
+
+// r = b - t (FP64, fixed DOFs masked)
+__global__ void k_residual64(long long n, const double* __restrict__ b, const double* __restrict__ t,
+                             const uint8_t* __restrict__ fl, double* __restrict__ r) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    r[i] = ((fl[i / 3] >> (i % 3)) & 1) ? 0.0 : b[i] - t[i];
 }
 
 // r = b - t (masked), z = M^-1 r; reductions r.z, r.r, b.b (FP64)
@@ -494,6 +729,19 @@ __global__ void __launch_bounds__(kNodeThreads) k_dpcg_init(GridDims g, Prec pc,
 
 // x += a p, r -= a q, z = M^-1 r (stored), FP64 reductions -> beta, convergence
 template <typename T>
+__device__ __forceinline__ void update1_dof(const Prec& pc, int f, int c, double wn, T al, T& x, T& r, T& z, T p,
+                                            T q, double& rr, double& rzn) {
+  x = fma(al, p, x);
+  r = fma(-al, q, r);
+  z = (T)jacobi_apply((double)r, f, c, wn, pc);
+  rr = fma((double)r, (double)r, rr);
+  rzn = fma((double)r, (double)z, rzn);
+}
+
+// alpha = r.z / p.q; x += alpha p; r -= alpha q; z = M^-1 r; r.r, r.z (FP64).
+// Threads take quads of 4 nodes (12 DOFs, 16-byte loads); the < 4 nodes after
+// the last full quad are done one DOF at a time.
+template <typename T>
 __global__ void __launch_bounds__(kNodeThreads) k_dpcg_update1(GridDims g, Prec pc, const double* __restrict__ w,
                                                                const uint8_t* __restrict__ fl, T* __restrict__ x,
                                                                T* __restrict__ r, T* __restrict__ z,
@@ -510,22 +758,38 @@ __global__ void __launch_bounds__(kNodeThreads) k_dpcg_update1(GridDims g, Prec 
     }
     return;
   }
+  const T al = (T)alpha;
   double rr = 0.0, rzn = 0.0;
-  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < g.nnodes;
-       n += (long long)gridDim.x * blockDim.x) {
+  const long long nq = g.nnodes / 4;
+  const long long gt = blockIdx.x * (long long)blockDim.x + threadIdx.x, gs = (long long)gridDim.x * blockDim.x;
+  for (long long t = gt; t < nq; t += gs) {
+    T xv[12], rv[12], pv[12], qv[12], zv[12];
+    ld12(x + 12 * t, xv);
+    ld12(r + 12 * t, rv);
+    ld12(p + 12 * t, pv);
+    ld12(q + 12 * t, qv);
+    double wn[4];
+    unsigned f4;
+    ld_quad_node(w, fl, t, wn, f4);
+#pragma unroll
+    for (int k = 0; k < 12; ++k)
+      update1_dof<T>(pc, (f4 >> (8 * (k / 3))) & 0xff, k % 3, wn[k / 3], al, xv[k], rv[k], zv[k], pv[k], qv[k], rr,
+                     rzn);
+    st12(x + 12 * t, xv);
+    st12(r + 12 * t, rv);
+    st12(z + 12 * t, zv);
+  }
+  if (gt < g.nnodes - 4 * nq) {
+    const long long n = 4 * nq + gt;
     const int f = fl[n];
-    const double wn = w[n];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const long long i = 3 * n + c;
-      const T al = (T)alpha;
-      x[i] = fma(al, p[i], x[i]);
-      const T ri = fma(-al, q[i], r[i]);
+      T xi = x[i], ri = r[i], zi;
+      update1_dof<T>(pc, f, c, w[n], al, xi, ri, zi, p[i], q[i], rr, rzn);
+      x[i] = xi;
       r[i] = ri;
-      const T zi = (T)jacobi_apply((double)ri, f, c, wn, pc);
       z[i] = zi;
-      rr = fma((double)ri, (double)ri, rr);
-      rzn = fma((double)ri, (double)zi, rzn);
     }
   }
   double v[2];
@@ -552,6 +816,30 @@ __global__ void __launch_bounds__(kNodeThreads) k_dpcg_update1(GridDims g, Prec 
 
 // p = z + beta p - W mu  (beta = 0 for the start vector)
 template <typename T>
+__device__ __forceinline__ void update2_node(const GridDims& g, const DeflP& dp, long long n, int grp, int f,
+                                             const double* __restrict__ gc, const double* __restrict__ mu, T beta,
+                                             const T* zv, T* pv, bool first) {
+  double x, y, zz;
+  node_xyz(g, n, dp.hx, dp.hy, dp.hz, x, y, zz);
+  const double* c = gc + 3 * (long long)grp;
+  const double rx = x - c[0], ry = y - c[1], rz = zz - c[2];
+  const double* m = mu + (long long)grp * dp.modes;
+  double w0 = m[0], w1 = m[1], w2 = m[2];
+  if (dp.modes == 6) {
+    w0 += rz * m[4] - ry * m[5];
+    w1 += -rz * m[3] + rx * m[5];
+    w2 += ry * m[3] - rx * m[4];
+  }
+  const double wv[3] = {w0, w1, w2};
+#pragma unroll
+  for (int c2 = 0; c2 < 3; ++c2) {
+    const T pi = first ? T(0) : pv[c2];
+    pv[c2] = ((f >> c2) & 1) ? T(0) : (T)(fma(beta, pi, zv[c2]) - (T)wv[c2]);
+  }
+}
+
+// p = z + beta p - W mu (first: p = z - W mu); quads of 4 nodes as in update1
+template <typename T>
 __global__ void __launch_bounds__(kNodeThreads) k_dpcg_update2(GridDims g, DeflP dp, const int32_t* __restrict__ ngrp,
                                                                const double* __restrict__ gc,
                                                                const double* __restrict__ mu,
@@ -559,18 +847,30 @@ __global__ void __launch_bounds__(kNodeThreads) k_dpcg_update2(GridDims g, DeflP
                                                                const T* __restrict__ z, T* __restrict__ p,
                                                                const KrylovState* S, int first) {
   if (!first && S->done) return;
-  const double beta = first ? 0.0 : S->beta;
-  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < g.nnodes;
-       n += (long long)gridDim.x * blockDim.x) {
-    double w[3];
-    prolong_node(g, dp, n, ngrp, gc, mu, w);
-    const int f = fl[n];
+  const T beta = first ? T(0) : (T)S->beta;
+  const long long nq = g.nnodes / 4;
+  const long long gt = blockIdx.x * (long long)blockDim.x + threadIdx.x, gs = (long long)gridDim.x * blockDim.x;
+  for (long long t = gt; t < nq; t += gs) {
+    T zv[12], pv[12];
+    ld12(z + 12 * t, zv);
+    if (!first) ld12(p + 12 * t, pv);
+    const int4 gq = __ldg(reinterpret_cast<const int4*>(ngrp + 4 * t));
+    const unsigned f4 = __ldg(reinterpret_cast<const unsigned*>(fl + 4 * t));
+    const int gr[4] = {gq.x, gq.y, gq.z, gq.w};
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const long long i = 3 * n + c;
-      const T pi = first ? T(0) : p[i];
-      p[i] = ((f >> c) & 1) ? T(0) : (T)(fma((T)beta, pi, z[i]) - (T)w[c]);
-    }
+    for (int j = 0; j < 4; ++j)
+      update2_node<T>(g, dp, 4 * t + j, gr[j], (f4 >> (8 * j)) & 0xff, gc, mu, beta, zv + 3 * j, pv + 3 * j,
+                      first != 0);
+    st12(p + 12 * t, pv);
+  }
+  if (gt < g.nnodes - 4 * nq) {
+    const long long n = 4 * nq + gt;
+    T zv[3] = {z[3 * n], z[3 * n + 1], z[3 * n + 2]};
+    T pv[3] = {p[3 * n], p[3 * n + 1], p[3 * n + 2]};
+    update2_node<T>(g, dp, n, ngrp[n], fl[n], gc, mu, beta, zv, pv, first != 0);
+    p[3 * n] = pv[0];
+    p[3 * n + 1] = pv[1];
+    p[3 * n + 2] = pv[2];
   }
 }
 
@@ -615,6 +915,9 @@ struct DpcgWs {
   uint8_t* fl;
   double *cv, *mu;     // coarse vectors
   double* rpart;       // restriction partials
+  int32_t* cptr;       // boundary-list chunk table [ngroups+1]
+  int32_t* cgrp;       // group of each chunk [kRkMaxChunks]
+  unsigned* gcount;    // per-group chunk counters [ngroups]
   double *P, *Rp, *U;  // sweep scratch
   // mixed-precision inner solve (FP32 vectors), carved only for the mixed solver
   float *r32, *p32, *q32, *z32, *x32, *b32, *s32;
@@ -637,7 +940,10 @@ static DpcgWs carve_dpcg(const pyto_operator_t* op, long long nc, void* ws, size
   W.w = cv.take<double>(g.nnodes);
   W.fl = cv.take<uint8_t>(g.nnodes);
   W.rpart = cv.take<double>((size_t)6 * kRestrictMaxBlocks);
-  W.cv = cv.take<double>(nc > 0 ? nc : 1);
+  W.cptr = cv.take<int32_t>((size_t)kMaxCoarse + 1);
+  W.cgrp = cv.take<int32_t>((size_t)kRkMaxChunks);
+  W.gcount = cv.take<unsigned>((size_t)kMaxCoarse);
+  W.cv = cv.take<double>(2 * (nc > 0 ? nc : 1));  // k_restrict_K writes 6 slots per group
   W.mu = cv.take<double>(nc > 0 ? nc : 1);
   W.P = cv.take<double>(kSweepB * kSweepB);
   W.Rp = cv.take<double>(kSweepB * (nc > 0 ? nc : 1));
@@ -697,10 +1003,50 @@ static int coarse_solve(const GridDims& g, const DeflP& dp, const pyto_deflation
   return PYTO_OK;
 }
 
+// p = z + beta p - W Einv W_f^T K(s) z from the boundary element lists (chunk
+// tables built by chunk_setup for the current solve); first: p = z - W Einv W_f^T K z
+template <typename T>
+static int coarse_update_K(const pyto_operator_t* op, const GridDims& g, const DeflP& dp, const pyto_deflation_t* d,
+                           const T* s, const T* z, T* p, const DpcgWs& W, int nchunks, const KrylovState* S,
+                           int first, cudaStream_t st) {
+  k_restrict_K<T><<<nchunks, kRkThreads, 0, st>>>(g, make_khat(op), dp, s, W.fl, d->node_group, d->group_center,
+                                                  d->bel_ptr, d->bel_list, W.cptr, W.cgrp, z, W.rpart, W.gcount,
+                                                  W.cv, S);
+  PYTO_COUNT(1);
+  const size_t shm = (size_t)dp.nc * sizeof(double);
+  const int nb = (int)std::min<long long>((dp.nc + 7) / 8, 8 * kNumSMs);
+  k_gemv<<<nb, 256, shm, st>>>(dp.nc, d->coarse_inv, W.cv, W.mu, first ? nullptr : S);
+  PYTO_COUNT(1);
+  k_dpcg_update2<T><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, d->node_group, d->group_center, W.mu, W.fl, z, p,
+                                                          S, first);
+  PYTO_COUNT(1);
+  PYTO_LAUNCH_CHECK();
+  return PYTO_OK;
+}
+
+// Chunk table of the boundary lists; returns the chunk count (0: no lists) or a
+// negative status.  The group counters are zeroed here and left at zero by
+// every k_restrict_K launch.
+static int chunk_setup(const pyto_deflation_t* d, const DpcgWs& W, cudaStream_t st) {
+  if (!d->bel_ptr || !d->bel_list) return 0;
+  int total = 0;
+  PYTO_CUDA(cudaMemcpyAsync(&total, d->bel_ptr + d->ngroups, sizeof(int), cudaMemcpyDeviceToHost, st));
+  PYTO_CUDA(cudaStreamSynchronize(st));
+  const long long bound = (long long)total / kRkChunk + d->ngroups;  // >= number of chunks
+  if (total < 0 || bound > kRkMaxChunks) return PYTO_ERR_TOO_LARGE;
+  k_chunk_ptr<<<1, 1024, 0, st>>>(d->ngroups, d->bel_ptr, W.cptr, W.cgrp);
+  PYTO_COUNT(1);
+  PYTO_CUDA(cudaMemsetAsync(W.gcount, 0, (size_t)d->ngroups * sizeof(unsigned), st));
+  PYTO_LAUNCH_CHECK();
+  return (int)std::max<long long>(bound, 1);
+}
+
 static int gemv_smem_ok(long long nc) {
   static bool done = false;
   if (!done) {
     if (cudaFuncSetAttribute(k_coarse_gemv, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(kMaxCoarse * sizeof(double))) != cudaSuccess ||
+        cudaFuncSetAttribute(k_gemv, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(kMaxCoarse * sizeof(double))) != cudaSuccess)
       return PYTO_ERR_CUDA;
     done = true;
@@ -747,10 +1093,10 @@ extern "C" int pyto_dpcg_setup(const pyto_operator_t* op, const double* s, const
     PYTO_COUNT(1);
     k_sweep_panel<<<(int)((n + 15) / 16), 256, 0, st>>>(n, (int)k0, bk, E, W.P, W.Rp, W.U);
     PYTO_COUNT(1);
-    k_sweep_update<<<dim3(tiles, tiles), 256, 0, st>>>(n, (int)k0, bk, E, W.P, W.Rp, W.U);
+    k_sweep_update<<<(int)((long long)tiles * (tiles + 1) / 2), 256, 0, st>>>(n, (int)k0, bk, E, W.P, W.Rp, W.U);
     PYTO_COUNT(1);
   }
-  k_negate<<<(int)std::min<long long>((n * n + 255) / 256, 8 * kNumSMs), 256, 0, st>>>(n * n, E);
+  k_negate_sym<<<(int)std::min<long long>((n * n + 255) / 256, 8 * kNumSMs), 256, 0, st>>>(n, E);
   PYTO_COUNT(1);
   PYTO_LAUNCH_CHECK();
   return PYTO_OK;
@@ -797,11 +1143,18 @@ static int dpcg_run(const pyto_operator_t* op, const T* s, const uint8_t* mask, 
   k_dpcg_init<T><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, pc, b, V.q, W.w, W.fl, V.r, V.z, W.S, W.part, W.counter);
   PYTO_COUNT(1);
   // p0 = z - W Einv W^T K z
-  if ((rc = matvec_t(op, s, mask, V.z, V.q, nullptr, nullptr, nullptr, st))) return rc;
-  if ((rc = coarse_solve(g, dp, defl, V.q, W, nullptr, st))) return rc;
-  k_dpcg_update2<T><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center, W.mu, W.fl,
-                                                          V.z, V.p, W.S, 1);
-  PYTO_COUNT(1);
+  const int nchunks = chunk_setup(defl, W, st);
+  if (nchunks < 0) return nchunks;
+  const bool lists = nchunks > 0;
+  if (lists) {
+    if ((rc = coarse_update_K(op, g, dp, defl, s, V.z, V.p, W, nchunks, W.S, 1, st))) return rc;
+  } else {
+    if ((rc = matvec_t(op, s, mask, V.z, V.q, nullptr, nullptr, nullptr, st))) return rc;
+    if ((rc = coarse_solve(g, dp, defl, V.q, W, nullptr, st))) return rc;
+    k_dpcg_update2<T><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center, W.mu,
+                                                            W.fl, V.z, V.p, W.S, 1);
+    PYTO_COUNT(1);
+  }
   PYTO_LAUNCH_CHECK();
   PYTO_CUDA(cudaMemcpyAsync(hs, W.S, sizeof(*hs), cudaMemcpyDeviceToHost, st));
   PYTO_CUDA(cudaStreamSynchronize(st));
@@ -811,12 +1164,16 @@ static int dpcg_run(const pyto_operator_t* op, const T* s, const uint8_t* mask, 
       k_dpcg_update1<T><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, pc, W.w, W.fl, u, V.r, V.z, V.p, V.q, W.S, W.part,
                                                               W.counter);
       PYTO_COUNT(1);
-      // K z -> q (q is free again), mu = Einv W^T K z, p = z + beta p - W mu
-      if ((rc = matvec_t(op, s, mask, V.z, V.q, nullptr, nullptr, nullptr, st))) return rc;
-      if ((rc = coarse_solve(g, dp, defl, V.q, W, W.S, st))) return rc;
-      k_dpcg_update2<T><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center, W.mu,
-                                                              W.fl, V.z, V.p, W.S, 0);
-      PYTO_COUNT(1);
+      // mu = Einv W^T K z (from the boundary lists, or K z -> q then W^T q), p = z + beta p - W mu
+      if (lists) {
+        if ((rc = coarse_update_K(op, g, dp, defl, s, V.z, V.p, W, nchunks, W.S, 0, st))) return rc;
+      } else {
+        if ((rc = matvec_t(op, s, mask, V.z, V.q, nullptr, nullptr, nullptr, st))) return rc;
+        if ((rc = coarse_solve(g, dp, defl, V.q, W, W.S, st))) return rc;
+        k_dpcg_update2<T><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center, W.mu,
+                                                                W.fl, V.z, V.p, W.S, 0);
+        PYTO_COUNT(1);
+      }
     }
     PYTO_LAUNCH_CHECK();
     PYTO_CUDA(cudaMemcpyAsync(hs, W.S, sizeof(*hs), cudaMemcpyDeviceToHost, st));
@@ -831,11 +1188,50 @@ __global__ void k_cast(long long n, const A* __restrict__ a, B* __restrict__ b) 
     b[i] = (B)a[i];
 }
 
-// b32 = (float)(b - t)  (fixed entries are masked by the inner solver)
-__global__ void k_residual_f32(long long n, const double* __restrict__ b, const double* __restrict__ t,
-                               float* __restrict__ b32) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    b32[i] = (float)(b[i] - t[i]);
+// Reliable update of the mixed solver: r = b - t (t = K u in FP64, fixed DOFs
+// masked), r32 = (float) r, z32 = M^-1 r32.  The last block sets rr = true_rr =
+// ||r||^2 (FP64), rz = r32.z32, bb = ||b||^2, clears the breakdown flag and sets
+// converged/done from the FP64 residual.
+__global__ void __launch_bounds__(kNodeThreads) k_reliable(GridDims g, Prec pc, const double* __restrict__ b,
+                                                           const double* __restrict__ t, const double* __restrict__ w,
+                                                           const uint8_t* __restrict__ fl, float* __restrict__ r32,
+                                                           float* __restrict__ z32, KrylovState* S, double* part,
+                                                           unsigned* counter) {
+  __shared__ double sred[kNodeThreads / 32];
+  double rz = 0.0, rr = 0.0, bb = 0.0;
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < g.nnodes;
+       n += (long long)gridDim.x * blockDim.x) {
+    const int f = fl[n];
+    const double wn = w[n];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const long long i = 3 * n + c;
+      const bool fixed = (f >> c) & 1;
+      const double bi = fixed ? 0.0 : b[i];
+      const double ri = fixed ? 0.0 : bi - t[i];
+      const float rf = (float)ri;
+      const float zf = (float)jacobi_apply((double)rf, f, c, wn, pc);
+      r32[i] = rf;
+      z32[i] = zf;
+      rz = fma((double)rf, (double)zf, rz);
+      rr = fma(ri, ri, rr);
+      bb = fma(bi, bi, bb);
+    }
+  }
+  double v[3];
+  v[0] = block_sum<kNodeThreads>(rz, sred);
+  v[1] = block_sum<kNodeThreads>(rr, sred);
+  v[2] = block_sum<kNodeThreads>(bb, sred);
+  grid_reduce<3>(v, part, counter, gridDim.x, [&](const double* tot) {
+    S->rz = tot[0];
+    S->rr = tot[1];
+    S->true_rr = tot[1];
+    S->bb = tot[2];
+    S->breakdown = 0;
+    const int conv = (tot[2] == 0.0 || sqrt(tot[1]) <= S->rtol * sqrt(tot[2])) ? 1 : 0;
+    S->converged = conv;
+    S->done = conv;
+  });
 }
 
 // u += (double) x
@@ -853,6 +1249,7 @@ extern "C" int pyto_dpcg_solve(const pyto_operator_t* op, const double* s, const
                                pyto_solve_status_t* status, void* ws, size_t ws_bytes, void* stream) {
   if (!op || !s || !b || !u || !cfg || !status || !defl_ok(defl)) return PYTO_ERR_ARG;
   if (!(cfg->rtol >= 0.0) || cfg->max_iters < 0 || cfg->stop_rule < 0 || cfg->stop_rule > 1) return PYTO_ERR_ARG;
+  if (((uintptr_t)b | (uintptr_t)u | (uintptr_t)defl->node_group) & 15) return PYTO_ERR_ARG;
   const DeflP dp = make_deflp(op, defl);
   int rc = gemv_smem_ok(dp.nc);
   if (rc) return rc;
@@ -887,10 +1284,11 @@ extern "C" int pyto_dpcg_solve(const pyto_operator_t* op, const double* s, const
 
 extern "C" int pyto_dpcg_mixed_solve(const pyto_operator_t* op, const double* s, const uint8_t* mask,
                                      const pyto_deflation_t* defl, const double* b, double* u,
-                                     const pyto_solve_cfg_t* cfg, double inner_rtol, pyto_solve_status_t* status,
+                                     const pyto_solve_cfg_t* cfg, double delta, pyto_solve_status_t* status,
                                      void* ws, size_t ws_bytes, void* stream) {
   if (!op || !s || !b || !u || !cfg || !status || !defl_ok(defl)) return PYTO_ERR_ARG;
-  if (!(cfg->rtol > 0.0) || !(inner_rtol > 0.0) || !(inner_rtol < 1.0) || cfg->max_iters < 0) return PYTO_ERR_ARG;
+  if (!(cfg->rtol > 0.0) || !(delta > 0.0) || !(delta < 1.0) || cfg->max_iters < 0) return PYTO_ERR_ARG;
+  if (((uintptr_t)b | (uintptr_t)u | (uintptr_t)defl->node_group) & 15) return PYTO_ERR_ARG;
   const DeflP dp = make_deflp(op, defl);
   int rc = gemv_smem_ok(dp.nc);
   if (rc) return rc;
@@ -899,55 +1297,110 @@ extern "C" int pyto_dpcg_mixed_solve(const pyto_operator_t* op, const double* s,
   if (!ws || ws_bytes < need) return PYTO_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
   const GridDims g = make_dims(op);
+  const Prec pc = make_prec(op);
   const long long nd = 3 * g.nnodes;
   const int nb = (int)std::min<long long>((nd + 255) / 256, 8 * kNumSMs);
+  const int every = std::max(1, cfg->check_every);
   PYTO_CUDA(cudaMemsetAsync(W.counter, 0, 64 * sizeof(unsigned), st));
   if ((rc = pyto_jacobi(op, s, mask, W.w, W.fl, nullptr, stream))) return rc;
   k_cast<double, float><<<nb, 256, 0, st>>>(g.nelem, s, W.s32);
   PYTO_COUNT(1);
-  PYTO_CUDA(cudaMemsetAsync(u, 0, nd * sizeof(double), st));
-  // FP64 outer loop: r = b - K u in FP64, FP32 deflated PCG on K d = r, u += d
-  KrylovState hs{}, inner{};
-  int total = 0, cycles = 0;
-  double rel = 1.0;
-  bool conv = false, brk = false;
-  for (;;) {
-    if (cycles == 0) {
-      PYTO_CUDA(cudaMemsetAsync(W.q, 0, nd * sizeof(double), st));
-    } else if ((rc = launch_matvec64(op, s, mask, u, W.q, PYTO_MASK_IN | PYTO_MASK_OUT, nullptr, nullptr, nullptr,
-                                     st))) {
-      return rc;
+  const int nchunks = chunk_setup(defl, W, st);
+  if (nchunks < 0) return nchunks;
+  const bool lists = nchunks > 0;
+  k_state_init2<<<1, 1, 0, st>>>(W.S, cfg->rtol, cfg->max_iters, 0);
+  PYTO_COUNT(1);
+  // coarse start in FP64: u = W Einv W_f^T b   (src/deflation.py:532-537)
+  if ((rc = coarse_solve(g, dp, defl, b, W, nullptr, st))) return rc;
+  k_prolong<double><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center, W.mu, W.fl, u);
+  PYTO_COUNT(1);
+
+  // r = b - K u in FP64, handed to the FP32 recurrence; the FP32 iterate x32 restarts at 0.
+  // The DEF2 recurrence never changes W_f^T r (W_f^T K p = 0 for every direction),
+  // so a residual update first removes its coarse part: u += W Einv W_f^T (b - K u).
+  auto reliable = [&](bool coarse) -> int {
+    int e;
+    if (coarse) {
+      if ((e = launch_matvec64(op, s, mask, u, W.q, PYTO_MASK_IN | PYTO_MASK_OUT, nullptr, nullptr, nullptr, st)))
+        return e;
+      k_residual64<<<nb, 256, 0, st>>>(nd, b, W.q, W.fl, W.r);
+      PYTO_COUNT(1);
+      if ((e = coarse_solve(g, dp, defl, (const double*)W.r, W, nullptr, st))) return e;
+      k_prolong<double, true><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center,
+                                                                    W.mu, W.fl, u);
+      PYTO_COUNT(1);
     }
-    k_true_residual2<<<kNodeBlocks, kNodeThreads, 0, st>>>(g, b, W.q, W.fl, W.S, W.part, W.counter);
+    if ((e = launch_matvec64(op, s, mask, u, W.q, PYTO_MASK_IN | PYTO_MASK_OUT, nullptr, nullptr, nullptr, st)))
+      return e;
+    k_reliable<<<kNodeBlocks, kNodeThreads, 0, st>>>(g, pc, b, W.q, W.w, W.fl, W.r32, W.z32, W.S, W.part,
+                                                     W.counter);
     PYTO_COUNT(1);
+    PYTO_CUDA(cudaMemsetAsync(W.x32, 0, nd * sizeof(float), st));
+    return PYTO_OK;
+  };
+  auto restart_p = [&]() -> int {  // p = z - W Einv W^T K z
+    int e;
+    if (lists) {
+      if ((e = coarse_update_K(op, g, dp, defl, W.s32, W.z32, W.p32, W, nchunks, W.S, 1, st))) return e;
+    } else {
+      if ((e = matvec_t(op, W.s32, mask, W.z32, W.q32, nullptr, nullptr, nullptr, st))) return e;
+      if ((e = coarse_solve(g, dp, defl, W.q32, W, nullptr, st))) return e;
+      k_dpcg_update2<float><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center,
+                                                                  W.mu, W.fl, W.z32, W.p32, W.S, 1);
+      PYTO_COUNT(1);
+    }
+    return PYTO_OK;
+  };
+  if ((rc = reliable(false))) return rc;
+  if ((rc = restart_p())) return rc;
+  PYTO_LAUNCH_CHECK();
+  KrylovState hs{};
+  PYTO_CUDA(cudaMemcpyAsync(&hs, W.S, sizeof(hs), cudaMemcpyDeviceToHost, st));
+  PYTO_CUDA(cudaStreamSynchronize(st));
+  double rr_ref = hs.rr;
+  int updates = 1, restarts = 0;
+  const double d2 = delta * delta;
+  while (!hs.converged && hs.iters < cfg->max_iters) {
+    for (int k = 0; k < every; ++k) {
+      if ((rc = matvec_t(op, W.s32, mask, W.p32, W.q32, W.part, W.counter, &W.S->pq, st))) return rc;
+      k_dpcg_update1<float><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, pc, W.w, W.fl, W.x32, W.r32, W.z32, W.p32,
+                                                                  W.q32, W.S, W.part, W.counter);
+      PYTO_COUNT(1);
+      if (lists) {
+        if ((rc = coarse_update_K(op, g, dp, defl, W.s32, W.z32, W.p32, W, nchunks, W.S, 0, st))) return rc;
+      } else {
+        if ((rc = matvec_t(op, W.s32, mask, W.z32, W.q32, nullptr, nullptr, nullptr, st))) return rc;
+        if ((rc = coarse_solve(g, dp, defl, W.q32, W, W.S, st))) return rc;
+        k_dpcg_update2<float><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center,
+                                                                    W.mu, W.fl, W.z32, W.p32, W.S, 0);
+        PYTO_COUNT(1);
+      }
+    }
     PYTO_LAUNCH_CHECK();
     PYTO_CUDA(cudaMemcpyAsync(&hs, W.S, sizeof(hs), cudaMemcpyDeviceToHost, st));
     PYTO_CUDA(cudaStreamSynchronize(st));
-    rel = hs.bb > 0 ? sqrt(hs.true_rr / hs.bb) : 0.0;
-    if (rel <= cfg->rtol || hs.bb == 0.0) {
-      conv = true;
-      break;
-    }
-    if (total >= cfg->max_iters || brk) break;
-    // r (FP64) = b - K u, formed in FP32 as the inner right-hand side
-    k_residual_f32<<<nb, 256, 0, st>>>(nd, b, W.q, W.b32);
-    PYTO_COUNT(1);
-    rc = dpcg_run<float>(op, W.s32, mask, defl, W.b32, W.x32, DVec<float>{W.r32, W.p32, W.q32, W.z32}, W,
-                         inner_rtol, cfg->max_iters - total, 0, std::max(1, cfg->check_every), &inner, st);
-    if (rc) return rc;
-    total += inner.iters;
-    brk = inner.breakdown != 0;
+    if (!(hs.done || hs.rr <= d2 * rr_ref)) continue;
+    // fold the FP32 iterate into u and replace the recursive residual by the true one
     k_add_f32<<<nb, 256, 0, st>>>(nd, W.x32, u);
     PYTO_COUNT(1);
-    ++cycles;
-    if (inner.iters == 0) break;  // no progress possible
+    const bool brk = hs.breakdown != 0;
+    if ((rc = reliable(true))) return rc;
+    ++updates;
+    if (brk) {  // p.Kp <= 0 in FP32: restart the search direction from the new residual
+      if (++restarts > 8) break;
+      if ((rc = restart_p())) return rc;
+    }
+    PYTO_LAUNCH_CHECK();
+    PYTO_CUDA(cudaMemcpyAsync(&hs, W.S, sizeof(hs), cudaMemcpyDeviceToHost, st));
+    PYTO_CUDA(cudaStreamSynchronize(st));
+    rr_ref = hs.rr;
   }
-  status->converged = conv ? 1 : 0;
-  status->iters = total;
-  status->breakdown = brk ? 1 : 0;
-  status->reserved = cycles;
-  status->rel_res = rel;
-  status->true_rel_res = rel;
-  if (brk && !conv) return PYTO_ERR_BREAKDOWN;
-  return conv ? PYTO_OK : PYTO_NOT_CONVERGED;
+  status->converged = hs.converged;
+  status->iters = hs.iters;
+  status->breakdown = restarts > 8 ? 1 : 0;
+  status->reserved = updates;
+  status->rel_res = hs.bb > 0 ? sqrt(hs.rr / hs.bb) : 0.0;
+  status->true_rel_res = hs.bb > 0 ? sqrt(hs.true_rr / hs.bb) : 0.0;
+  if (status->breakdown && !hs.converged) return PYTO_ERR_BREAKDOWN;
+  return hs.converged ? PYTO_OK : PYTO_NOT_CONVERGED;
 }

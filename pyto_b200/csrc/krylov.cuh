@@ -5,7 +5,8 @@
 
 namespace pyto {
 
-constexpr int kNodeBlocks = 4 * kNumSMs;  // grid of node-wise kernels (grid-stride)
+constexpr int kNodeBlocks = 16 * kNumSMs;  // grid of node-wise kernels (grid-stride; 3 partials each fit the
+                                           // 4 * reduce_slots partial array)
 constexpr int kNodeThreads = 256;
 
 struct KrylovState {
@@ -37,6 +38,47 @@ __device__ __forceinline__ double jacobi_apply(double r, int fl, int c, double w
 __device__ __forceinline__ bool krylov_converged(const KrylovState& S, double rr, double rz_new) {
   if (S.stop_rule == 0) return sqrt(rr) < S.rtol * sqrt(S.bb);
   return sqrt(rz_new / S.rz0) <= S.rtol;
+}
+
+// 12 consecutive values (the 3 DOFs of 4 nodes) with 16-byte accesses; the
+// address must be 16-byte aligned (node quads of 16-byte aligned vectors).
+__device__ __forceinline__ void ld12(const float* p, float (&v)[12]) {
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float4 t = __ldg(reinterpret_cast<const float4*>(p) + k);
+    v[4 * k] = t.x;
+    v[4 * k + 1] = t.y;
+    v[4 * k + 2] = t.z;
+    v[4 * k + 3] = t.w;
+  }
+}
+__device__ __forceinline__ void ld12(const double* p, double (&v)[12]) {
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    const double2 t = __ldg(reinterpret_cast<const double2*>(p) + k);
+    v[2 * k] = t.x;
+    v[2 * k + 1] = t.y;
+  }
+}
+__device__ __forceinline__ void st12(float* p, const float (&v)[12]) {
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+    reinterpret_cast<float4*>(p)[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+}
+__device__ __forceinline__ void st12(double* p, const double (&v)[12]) {
+#pragma unroll
+  for (int k = 0; k < 6; ++k) reinterpret_cast<double2*>(p)[k] = make_double2(v[2 * k], v[2 * k + 1]);
+}
+// Jacobi weights and flags of the 4 nodes of quad t (w, fl: 16- and 4-byte aligned bases)
+__device__ __forceinline__ void ld_quad_node(const double* w, const uint8_t* fl, long long t, double (&wn)[4],
+                                             unsigned& f4) {
+  const double2 a = __ldg(reinterpret_cast<const double2*>(w + 4 * t));
+  const double2 b = __ldg(reinterpret_cast<const double2*>(w + 4 * t) + 1);
+  wn[0] = a.x;
+  wn[1] = a.y;
+  wn[2] = b.x;
+  wn[3] = b.y;
+  f4 = __ldg(reinterpret_cast<const unsigned*>(fl + 4 * t));
 }
 
 int launch_matvec64(const pyto_operator_t* op, const double* s, const uint8_t* mask, const double* u, double* y,

@@ -50,6 +50,7 @@ class HexGrid:
         self.mask = torch.zeros(_round4(self.nnodes), dtype=torch.uint8, device=self.device)
         self.active = None
         self.n_active = self.nelem
+        self.mask_version = 0
 
     # ---- helpers -------------------------------------------------------------
     @property
@@ -76,6 +77,7 @@ class HexGrid:
                          else fixed_dofs, dtype=torch.int64)
         A.call("pyto_bc_mask", self.opp, A.ptr(fd) if fd.numel() else None, int(fd.numel()), A.ptr(self.mask),
                self._st())
+        self.mask_version += 1
         return self
 
     def set_active(self, active):
@@ -142,6 +144,7 @@ class HexGrid:
                             float(stt.true_rel_res), rc)
 
     def dpcg_setup(self, s, defl):
+        defl.sync(self)
         wsp, wsn = self._ws(A.WS_DPCG, "krylov")
         A.call("pyto_dpcg_setup", self.opp, A.ptr(s), A.ptr(self.mask), C.byref(defl.struct), wsp, wsn, self._st())
 
@@ -149,6 +152,7 @@ class HexGrid:
         """Deflated PCG (coarse inverse rebuilt for s when setup=True)."""
         if setup:
             self.dpcg_setup(s, defl)
+        defl.sync(self)
         u = out if out is not None else torch.empty(self.ndof, dtype=F64, device=self.device)
         cfg = self._cfg(rtol, max_iters, stop_rule, check_every, False)
         stt = A.SolveStatus()
@@ -159,12 +163,14 @@ class HexGrid:
         return u, SolveInfo(bool(stt.converged), int(stt.iters), bool(stt.breakdown), float(stt.rel_res),
                             float(stt.true_rel_res), rc)
 
-    def dpcg_mixed(self, s, b, defl, rtol=1e-8, inner_rtol=1e-4, max_iters=4000, check_every=25, out=None,
+    def dpcg_mixed(self, s, b, defl, rtol=1e-8, delta=1e-2, max_iters=4000, check_every=10, out=None,
                    setup=True):
-        """Deflated PCG in mixed precision: FP64 iterative refinement (true residual
-        ||b - K u|| <= rtol ||b|| in FP64) around FP32 deflated PCG cycles that each
-        reduce the residual by inner_rtol.  info.cycles is the number of cycles."""
+        """Deflated PCG in mixed precision: an FP32 recurrence whose residual is replaced
+        by the FP64 true residual b - K u (u held in FP64) each time it has dropped by
+        `delta`; converged when ||b - K u|| <= rtol ||b|| in FP64.  info.cycles is the
+        number of FP64 residual updates."""
         wsp, wsn = self._ws(A.WS_DPCG_MIXED, "krylov")
+        defl.sync(self)
         if setup:
             A.call("pyto_dpcg_setup", self.opp, A.ptr(s), A.ptr(self.mask), C.byref(defl.struct), wsp, wsn,
                    self._st())
@@ -172,7 +178,7 @@ class HexGrid:
         cfg = self._cfg(rtol, max_iters, 0, check_every, False)
         stt = A.SolveStatus()
         rc = A.call("pyto_dpcg_mixed_solve", self.opp, A.ptr(s), A.ptr(self.mask), C.byref(defl.struct), A.ptr(b),
-                    A.ptr(u), C.byref(cfg), float(inner_rtol), C.byref(stt), wsp, wsn, self._st(),
+                    A.ptr(u), C.byref(cfg), float(delta), C.byref(stt), wsp, wsn, self._st(),
                     allow=(A.OK, A.NOT_CONVERGED, A.ERR_BREAKDOWN))
         info = SolveInfo(bool(stt.converged), int(stt.iters), bool(stt.breakdown), float(stt.rel_res),
                          float(stt.true_rel_res), rc)
@@ -264,7 +270,9 @@ class DeviceDeflation:
         n0 = (ex + sx * (ey + sy * ez)).ravel()
         pairs = []
         corner = [0, 1, sx, sx + 1, sx * sy, sx * sy + 1, sx * sy + sx, sx * sy + sx + 1]
-        cg = np.stack([node_group[n0 + c] for c in corner], 1)
+        self._corner_nodes = np.stack([n0 + c for c in corner], 1).astype(np.int32)
+        cg = node_group[self._corner_nodes]
+        self._spans = (cg != cg[:, :1]).any(1)
         for a in range(8):
             for b in range(8):
                 pairs.append(cg[:, a].astype(np.int64) * ng + cg[:, b])
@@ -288,4 +296,31 @@ class DeviceDeflation:
         self.struct = A.Deflation(ng, self.modes, A.ptr(self.node_group), A.ptr(self.group_ptr),
                                   A.ptr(self.group_nodes), A.ptr(self.group_center), A.ptr(self.coarse_inv),
                                   float(shift), 1 if shift_relative else 0, int(counts.max()), A.ptr(self.group_box),
-                                  A.ptr(self.nbr_ptr), A.ptr(self.nbr_list), self.max_nbr, 0)
+                                  A.ptr(self.nbr_ptr), A.ptr(self.nbr_list), self.max_nbr, 0, None, None)
+        self._node_group_np = node_group
+        self.use_boundary_lists = True
+        self.mask_version = None
+        self.sync(grid)
+
+    def sync(self, grid: HexGrid):
+        """(Re)build the per-group boundary element lists for the grid's current fixed
+        DOFs: elements with a corner in the group and a corner in another group or on a
+        fixed DOF (W_f^T K z is formed from these elements only)."""
+        if not self.use_boundary_lists:
+            self.struct.bel_ptr = self.struct.bel_list = None
+            return self
+        if self.mask_version == grid.mask_version:
+            self.struct.bel_ptr, self.struct.bel_list = A.ptr(self.bel_ptr), A.ptr(self.bel_list)
+            return self
+        mask = grid.mask[:grid.nnodes].cpu().numpy()
+        fixed_el = ((mask[self._corner_nodes] & 7) != 0).any(1)
+        el = np.flatnonzero(self._spans | fixed_el)
+        cg = self._node_group_np[self._corner_nodes[el]].astype(np.int64)
+        key = np.unique((cg * grid.nelem + el[:, None]).ravel())
+        grp, elem = key // grid.nelem, key % grid.nelem
+        bptr = np.concatenate([[0], np.cumsum(np.bincount(grp, minlength=self.ngroups))]).astype(np.int32)
+        self.bel_ptr = torch.as_tensor(bptr, device=grid.device)
+        self.bel_list = torch.as_tensor(elem.astype(np.int32), device=grid.device)
+        self.struct.bel_ptr, self.struct.bel_list = A.ptr(self.bel_ptr), A.ptr(self.bel_list)
+        self.mask_version = grid.mask_version
+        return self

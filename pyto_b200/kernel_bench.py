@@ -43,7 +43,7 @@ def main(argv=None):
     ap.add_argument("--warm", type=int, default=3)
     ap.add_argument("--variant", type=int, default=2, help="matvec tile variant (pyto_tune)")
     ap.add_argument("--variant32", type=int, default=None, help="FP32 matvec tile variant (pyto_tune)")
-    ap.add_argument("--inner-rtol", type=float, default=1e-4, help="inner tolerance for --kernel mixed")
+    ap.add_argument("--delta", type=float, default=1e-2, help="reliable-update threshold for --kernel mixed")
     a = ap.parse_args(argv)
     nel = tuple(int(v) for v in a.nel.split(","))
     A.call("pyto_tune", 0, a.variant)
@@ -80,7 +80,7 @@ def main(argv=None):
             if a.kernel == "dpcg":
                 fn = lambda: g.dpcg(s, F, defl, rtol=1e-8, max_iters=5000, stop_rule=0, check_every=20)
             else:
-                fn = lambda: g.dpcg_mixed(s, F, defl, rtol=1e-8, inner_rtol=a.inner_rtol, max_iters=8000,
+                fn = lambda: g.dpcg_mixed(s, F, defl, rtol=1e-8, delta=a.delta, max_iters=8000,
                                           check_every=20)
         else:
             fn = lambda: g.pcg(s, F, rtol=1e-8, check_every=20)
