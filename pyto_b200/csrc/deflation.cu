@@ -25,6 +25,11 @@
 namespace pyto {
 
 constexpr int kSweepB = 64;
+// boundary-list chunks: kRkChunk list entries per CTA of the K-restriction and
+// of the coarse assembly
+constexpr int kRkThreads = 128;
+constexpr int kRkChunk = 2 * kRkThreads;
+constexpr int kRkMaxChunks = 65536;
 
 // node ids fit in int32 (checked by pyto_operator_init), so 32-bit division suffices
 __device__ __forceinline__ void node_xyz(const GridDims& g, long long n, double hx, double hy, double hz, double& x,
@@ -182,6 +187,147 @@ __global__ void __launch_bounds__(kAsmThreads) k_coarse_rows(GridDims g, KHat kh
   }
 }
 
+// Hadamard transform (8 corner modes, the ordering of hex8_core) of component c
+// of rigid mode a of group Gs restricted to the element's corners in Gs with
+// free DOF c; rel0: corner 0 relative to the group centre, h: element size.
+__device__ __forceinline__ void mode_comp_hat(const int (&gr)[8], const int (&mk)[8], int Gs, int c, int a,
+                                              const double (&rel0)[3], const double (&h)[3], double (&H)[8]) {
+  double v[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    double w = 0.0;
+    if (gr[k] == Gs && !((mk[k] >> c) & 1)) {
+      const double rx = rel0[0] + ((k & 1) ? h[0] : 0.0), ry = rel0[1] + (((k >> 1) & 1) ? h[1] : 0.0),
+                   rz = rel0[2] + ((k >> 2) ? h[2] : 0.0);
+      // component c of mode a: [tx,ty,tz, rx:(0,-z,y), ry:(z,0,-x), rz:(-y,x,0)]
+      if (a < 3) w = (a == c) ? 1.0 : 0.0;
+      else if (a == 3) w = (c == 1) ? -rz : (c == 2) ? ry : 0.0;
+      else if (a == 4) w = (c == 0) ? rz : (c == 2) ? -rx : 0.0;
+      else w = (c == 0) ? -ry : (c == 1) ? rx : 0.0;
+    }
+    v[k] = w;
+  }
+  double Fb[4], Ft[4];
+  face_fwd(v[0], v[1], v[2], v[3], Fb);
+  face_fwd(v[4], v[5], v[6], v[7], Ft);
+#pragma unroll
+  for (int f = 0; f < 4; ++f) {
+    H[f] = Ft[f] + Fb[f];
+    H[f + 4] = Ft[f] - Fb[f];
+  }
+}
+
+// Row blocks E[G, :] from the boundary element lists: one CTA per list chunk
+// (chunk tables as for k_restrict_K), one entry per thread per pass.  For entry
+// (G, e) and every group H at a corner of e, s_e (Phi W_G|e)^T K^ (Phi W_H|e) is
+// added into a shared-memory accumulator of G's neighbour slots (the sums of
+// one CTA are formed with shared-memory atomics, so their order varies), which
+// is then added into E with global atomics.
+constexpr int kCrThreads = 128;
+__global__ void __launch_bounds__(kCrThreads) k_coarse_rows2(GridDims g, KHat kh, DeflP dp,
+                                                             const double* __restrict__ s,
+                                                             const uint8_t* __restrict__ mask,
+                                                             const int32_t* __restrict__ ngrp,
+                                                             const double* __restrict__ gc,
+                                                             const int32_t* __restrict__ bptr,
+                                                             const int32_t* __restrict__ blist,
+                                                             const int32_t* __restrict__ cptr,
+                                                             const int32_t* __restrict__ cgrp,
+                                                             const int32_t* __restrict__ nptr,
+                                                             const int32_t* __restrict__ nlist,
+                                                             double* __restrict__ E) {
+  extern __shared__ double acc[];  // [nnb][36]
+  __shared__ int snb[128];
+  const int ch = blockIdx.x;
+  if (ch >= cptr[dp.ngroups]) return;
+  const int G = cgrp[ch];
+  const int nb0 = nptr[G], nnb = nptr[G + 1] - nb0;
+  for (int t = threadIdx.x; t < nnb; t += blockDim.x) snb[t] = nlist[nb0 + t];
+  for (int t = threadIdx.x; t < nnb * 36; t += blockDim.x) acc[t] = 0.0;
+  __syncthreads();
+  const int M = dp.modes;
+  const double h[3] = {dp.hx, dp.hy, dp.hz};
+  const int end = bptr[G + 1];
+  const int pn = g.sx * g.sy;
+  for (int r = 0; r < kRkChunk / kCrThreads; ++r) {
+    const int t = bptr[G] + (ch - cptr[G]) * kRkChunk + r * kCrThreads + threadIdx.x;
+    if (t >= end) continue;
+    const int e = blist[t];
+    const double se = s[e];
+    if (se == 0.0) continue;
+    const int rr = e / g.nx;
+    const int ex = e - rr * g.nx;
+    const int ez = rr / g.ny;
+    const int ey = rr - ez * g.ny;
+    const int n0 = ex + g.sx * (ey + g.sy * ez);
+    int gr[8], mk[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int nd = n0 + (k & 1) + g.sx * ((k >> 1) & 1) + pn * (k >> 2);
+      gr[k] = ngrp[nd];
+      mk[k] = mask ? (mask[nd] & 7) : 0;
+    }
+    // distinct corner groups and their slots in G's neighbour list
+    int Hs[8], Sl[8], nh = 0;
+    for (int k = 0; k < 8; ++k) {
+      bool seen = false;
+      for (int q = 0; q < nh; ++q) seen |= (Hs[q] == gr[k]);
+      if (seen) continue;
+      int slot = 0;
+      while (slot < nnb && snb[slot] != gr[k]) ++slot;
+      if (slot == nnb) continue;  // not possible for a consistent neighbour list
+      Hs[nh] = gr[k];
+      Sl[nh] = slot;
+      ++nh;
+    }
+    const double relG[3] = {dp.hx * ex - gc[3 * G], dp.hy * ey - gc[3 * G + 1], dp.hz * ez - gc[3 * G + 2]};
+    for (int a = 0; a < M; ++a) {
+      double Hg[3][8];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) mode_comp_hat(gr, mk, G, c, a, relG, h, Hg[c]);
+      // Z = s_e K^ Hg (rows m = 0 vanish)
+      double Z[3][8];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        Z[c][0] = 0.0;
+#pragma unroll
+        for (int m = 1; m < 8; ++m) {
+          const int q = m ^ (1 << c);
+          double o = 0.0;
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            const int md = member_mode(q, d);
+            if (md == 0) continue;
+            o = fma(kh.b[q][3 * c + d], Hg[d][md], o);
+          }
+          Z[c][m] = se * o;
+        }
+      }
+      for (int hi = 0; hi < nh; ++hi) {
+        const int H = Hs[hi];
+        const double relH[3] = {dp.hx * ex - gc[3 * H], dp.hy * ey - gc[3 * H + 1], dp.hz * ez - gc[3 * H + 2]};
+        for (int b = 0; b < M; ++b) {
+          double v = 0.0;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            double Hh[8];
+            mode_comp_hat(gr, mk, H, c, b, relH, h, Hh);
+#pragma unroll
+            for (int m = 1; m < 8; ++m) v = fma(Z[c][m], Hh[m], v);
+          }
+          if (v != 0.0) atomicAdd(&acc[Sl[hi] * 36 + a * 6 + b], v);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < nnb * M * M; t += blockDim.x) {
+    const int slot = t / (M * M), a = (t / M) % M, b = t % M;
+    const double v = acc[slot * 36 + a * 6 + b];
+    if (v != 0.0) atomicAdd(&E[((long long)G * M + a) * dp.nc + (long long)snb[slot] * M + b], v);
+  }
+}
+
 // mean |diag(E)| (one block) -> *out
 __global__ void k_diag_mean(long long nc, const double* __restrict__ E, double* out) {
   __shared__ double sred[8];
@@ -212,39 +358,60 @@ __global__ void k_coarse_finish(long long nc, double* E, double shift, const dou
 // blocked sweep inversion: after all pivot blocks A = -E^-1
 //   P = A_KK^-1, U = P A_K:, A_ij -= A_iK U_Kj, A_Kj = U_Kj, A_iK = U_Ki^T, A_KK = -P
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024) k_sweep_pivot(long long n, int k0, int bk, const double* __restrict__ A,
-                                                      double* __restrict__ P) {
-  __shared__ double M[kSweepB][kSweepB + 1];
-  for (int t = threadIdx.x; t < kSweepB * kSweepB; t += blockDim.x) {
-    const int i = t / kSweepB, j = t % kSweepB;
-    M[i][j] = (i < bk && j < bk) ? A[(k0 + i) * n + (k0 + j)] : (i == j ? 1.0 : 0.0);
-  }
-  __syncthreads();
-  // in-place sweep of the small block (result -M^-1): each thread owns 4 entries
+// In-place sweep of the bk x bk diagonal block (result -M^-1).  256 threads, each
+// holding a 4 x 4 set of entries (rows ty + 16a, columns tx + 16b) in registers;
+// per pivot step only the pivot row and column pass through shared memory
+// (double-buffered, one barrier per step).
+__global__ void __launch_bounds__(256) k_sweep_pivot(long long n, int k0, int bk, const double* __restrict__ A,
+                                                     double* __restrict__ P) {
+  __shared__ double s_row[2][kSweepB], s_col[2][kSweepB];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double R[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int i = ty + 16 * a, j = tx + 16 * b;
+      R[a][b] = (i < bk && j < bk) ? A[(k0 + i) * n + (k0 + j)] : (i == j ? 1.0 : 0.0);
+    }
   for (int p = 0; p < bk; ++p) {
-    double nv[4];
-    const double ipiv = 1.0 / M[p][p];
+    const int buf = p & 1, pa = p >> 4, pr = p & 15;
+    if (ty == pr) {
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const int t = threadIdx.x + r * 1024;
-      const int i = t / kSweepB, j = t % kSweepB;
-      if (i == p && j == p) nv[r] = -ipiv;
-      else if (i == p) nv[r] = M[p][j] * ipiv;
-      else if (j == p) nv[r] = M[i][p] * ipiv;
-      else nv[r] = fma(-M[i][p], M[p][j] * ipiv, M[i][j]);
+      for (int a = 0; a < 4; ++a)
+        if (a == pa)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) s_row[buf][tx + 16 * b] = R[a][b];
+    }
+    if (tx == pr) {
+#pragma unroll
+      for (int b = 0; b < 4; ++b)
+        if (b == pa)
+#pragma unroll
+          for (int a = 0; a < 4; ++a) s_col[buf][ty + 16 * a] = R[a][b];
     }
     __syncthreads();
+    const double ipiv = 1.0 / s_row[buf][p];
+    double rv[4], cv[4];
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      const int t = threadIdx.x + r * 1024;
-      M[t / kSweepB][t % kSweepB] = nv[r];
-    }
-    __syncthreads();
+    for (int b = 0; b < 4; ++b) rv[b] = s_row[buf][tx + 16 * b] * ipiv;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) cv[a] = s_col[buf][ty + 16 * a];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        const bool ip = (ty + 16 * a == p), jp = (tx + 16 * b == p);
+        if (ip && jp) R[a][b] = -ipiv;
+        else if (ip) R[a][b] = rv[b];
+        else if (jp) R[a][b] = cv[a] * ipiv;
+        else R[a][b] = fma(-cv[a], rv[b], R[a][b]);
+      }
   }
-  for (int t = threadIdx.x; t < kSweepB * kSweepB; t += blockDim.x) {
-    const int i = t / kSweepB, j = t % kSweepB;
-    P[t] = -M[i][j];  // P = A_KK^-1
-  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) P[(ty + 16 * a) * kSweepB + tx + 16 * b] = -R[a][b];  // P = A_KK^-1
 }
 
 // Rp = A_K: (copy), U = P Rp   (16 columns per block).  Only the lower tiles
@@ -418,9 +585,6 @@ __global__ void __launch_bounds__(256) k_restrict(GridDims g, DeflP dp, const in
 // CTA of a group to finish (per-group counter) adds the group's partials in
 // chunk order, so the result does not depend on scheduling, and resets the
 // counter.  Output: v[G*modes + a].
-constexpr int kRkThreads = 128;
-constexpr int kRkChunk = 2 * kRkThreads;
-constexpr int kRkMaxChunks = 65536;
 
 // cptr[G] = sum_{G' < G} ceil(len(G') / kRkChunk), cgrp[c] = group of chunk c
 // (one block of 1024 threads)
@@ -485,20 +649,25 @@ __device__ __forceinline__ void rk_element(const GridDims& g, const KHat& kh, co
     face_inv(Gb[c], u[c][0], u[c][1], u[c][2], u[c][3]);
     face_inv(Gt[c], u[c][4], u[c][5], u[c][6], u[c][7]);
   }
+  // contraction with the rigid modes of G in the vector precision, per element;
+  // the element sums are accumulated in FP64
+  const T bx = (T)(dp.hx * ex - c0), by = (T)(dp.hy * ey - c1), bz = (T)(dp.hz * ez - c2);
+  const T hx = (T)dp.hx, hy = (T)dp.hy, hz = (T)dp.hz;
+  T em[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
     if (gr[k] != G) continue;
-    const double yx = (mk[k] & 1) ? 0.0 : (double)u[0][k], yy = (mk[k] & 2) ? 0.0 : (double)u[1][k],
-                 yz = (mk[k] & 4) ? 0.0 : (double)u[2][k];
-    const double rx = dp.hx * (ex + (k & 1)) - c0, ry = dp.hy * (ey + ((k >> 1) & 1)) - c1,
-                 rz = dp.hz * (ez + (k >> 2)) - c2;
-    acc[0] += yx;
-    acc[1] += yy;
-    acc[2] += yz;
-    acc[3] += -rz * yy + ry * yz;
-    acc[4] += rz * yx - rx * yz;
-    acc[5] += -ry * yx + rx * yy;
+    const T yx = (mk[k] & 1) ? T(0) : u[0][k], yy = (mk[k] & 2) ? T(0) : u[1][k], yz = (mk[k] & 4) ? T(0) : u[2][k];
+    const T rx = (k & 1) ? bx + hx : bx, ry = ((k >> 1) & 1) ? by + hy : by, rz = (k >> 2) ? bz + hz : bz;
+    em[0] += yx;
+    em[1] += yy;
+    em[2] += yz;
+    em[3] += -rz * yy + ry * yz;
+    em[4] += rz * yx - rx * yz;
+    em[5] += -ry * yx + rx * yy;
   }
+#pragma unroll
+  for (int a = 0; a < 6; ++a) acc[a] += (double)em[a];
 }
 
 template <typename T>
@@ -742,7 +911,7 @@ __device__ __forceinline__ void update1_dof(const Prec& pc, int f, int c, double
 // Threads take quads of 4 nodes (12 DOFs, 16-byte loads); the < 4 nodes after
 // the last full quad are done one DOF at a time.
 template <typename T>
-__global__ void __launch_bounds__(kNodeThreads) k_dpcg_update1(GridDims g, Prec pc, const double* __restrict__ w,
+__global__ void __launch_bounds__(kNodeThreads, 4) k_dpcg_update1(GridDims g, Prec pc, const double* __restrict__ w,
                                                                const uint8_t* __restrict__ fl, T* __restrict__ x,
                                                                T* __restrict__ r, T* __restrict__ z,
                                                                const T* __restrict__ p, const T* __restrict__ q,
@@ -762,22 +931,30 @@ __global__ void __launch_bounds__(kNodeThreads) k_dpcg_update1(GridDims g, Prec 
   double rr = 0.0, rzn = 0.0;
   const long long nq = g.nnodes / 4;
   const long long gt = blockIdx.x * (long long)blockDim.x + threadIdx.x, gs = (long long)gridDim.x * blockDim.x;
+  using CK = Chunk<T>;
+  constexpr int NK = 12 / CK::N;  // 16-byte chunks per quad
   for (long long t = gt; t < nq; t += gs) {
-    T xv[12], rv[12], pv[12], qv[12], zv[12];
-    ld12(x + 12 * t, xv);
-    ld12(r + 12 * t, rv);
-    ld12(p + 12 * t, pv);
-    ld12(q + 12 * t, qv);
     double wn[4];
     unsigned f4;
     ld_quad_node(w, fl, t, wn, f4);
 #pragma unroll
-    for (int k = 0; k < 12; ++k)
-      update1_dof<T>(pc, (f4 >> (8 * (k / 3))) & 0xff, k % 3, wn[k / 3], al, xv[k], rv[k], zv[k], pv[k], qv[k], rr,
-                     rzn);
-    st12(x + 12 * t, xv);
-    st12(r + 12 * t, rv);
-    st12(z + 12 * t, zv);
+    for (int k = 0; k < NK; ++k) {
+      const long long ck = NK * t + k;
+      T xv[CK::N], rv[CK::N], pv[CK::N], qv[CK::N], zv[CK::N];
+      CK::ld(x, ck, xv);
+      CK::ld(r, ck, rv);
+      CK::ld(p, ck, pv);
+      CK::ld(q, ck, qv);
+#pragma unroll
+      for (int j = 0; j < CK::N; ++j) {
+        const int d = k * CK::N + j;  // DOF within the quad
+        update1_dof<T>(pc, (f4 >> (8 * (d / 3))) & 0xff, d % 3, wn[d / 3], al, xv[j], rv[j], zv[j], pv[j], qv[j],
+                       rr, rzn);
+      }
+      CK::st(x, ck, xv);
+      CK::st(r, ck, rv);
+      CK::st(z, ck, zv);
+    }
   }
   if (gt < g.nnodes - 4 * nq) {
     const long long n = 4 * nq + gt;
@@ -1062,7 +1239,8 @@ extern "C" int pyto_dpcg_setup(const pyto_operator_t* op, const double* s, const
                                pyto_deflation_t* defl, void* ws, size_t ws_bytes, void* stream) {
   if (!op || !s || !defl_ok(defl)) return PYTO_ERR_ARG;
   const DeflP dp = make_deflp(op, defl);
-  if (dp.nc > kMaxCoarse) return PYTO_ERR_TOO_LARGE;
+  int rc0 = gemv_smem_ok(dp.nc);
+  if (rc0) return rc0;
   size_t need = 0;
   DpcgWs W = carve_dpcg(op, dp.nc, ws, ws_bytes, &need);
   if (!ws || ws_bytes < need) return PYTO_ERR_WORKSPACE;
@@ -1071,8 +1249,15 @@ extern "C" int pyto_dpcg_setup(const pyto_operator_t* op, const double* s, const
   double* E = defl->coarse_inv;
   const long long n = dp.nc;
   PYTO_CUDA(cudaMemsetAsync(E, 0, (size_t)n * n * sizeof(double), st));
-  {
-    const size_t shm = (size_t)defl->max_nbr * 36 * sizeof(double);
+  const int nchunks = chunk_setup(defl, W, st);
+  if (nchunks < 0) return nchunks;
+  const size_t shm = (size_t)defl->max_nbr * 36 * sizeof(double);
+  if (nchunks > 0) {
+    k_coarse_rows2<<<nchunks, kCrThreads, shm, st>>>(g, make_khat(op), dp, s, mask, defl->node_group,
+                                                     defl->group_center, defl->bel_ptr, defl->bel_list, W.cptr,
+                                                     W.cgrp, defl->nbr_ptr, defl->nbr_list, E);
+    PYTO_COUNT(1);
+  } else {
     k_coarse_rows<<<dp.ngroups, kAsmThreads, shm, st>>>(g, make_khat(op), dp, s, mask, defl->node_group,
                                                          defl->group_center, defl->group_box, defl->nbr_ptr,
                                                          defl->nbr_list, E);
@@ -1089,7 +1274,7 @@ extern "C" int pyto_dpcg_setup(const pyto_operator_t* op, const double* s, const
   const int tiles = (int)((n + 63) / 64);
   for (long long k0 = 0; k0 < n; k0 += kSweepB) {
     const int bk = (int)std::min<long long>(kSweepB, n - k0);
-    k_sweep_pivot<<<1, 1024, 0, st>>>(n, (int)k0, bk, E, W.P);
+    k_sweep_pivot<<<1, 256, 0, st>>>(n, (int)k0, bk, E, W.P);
     PYTO_COUNT(1);
     k_sweep_panel<<<(int)((n + 15) / 16), 256, 0, st>>>(n, (int)k0, bk, E, W.P, W.Rp, W.U);
     PYTO_COUNT(1);

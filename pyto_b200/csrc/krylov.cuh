@@ -69,6 +69,36 @@ __device__ __forceinline__ void st12(double* p, const double (&v)[12]) {
 #pragma unroll
   for (int k = 0; k < 6; ++k) reinterpret_cast<double2*>(p)[k] = make_double2(v[2 * k], v[2 * k + 1]);
 }
+// One 16-byte chunk (4 floats or 2 doubles) of vector v at chunk index k
+template <typename T>
+struct Chunk;
+template <>
+struct Chunk<float> {
+  static constexpr int N = 4;
+  __device__ __forceinline__ static void ld(const float* p, long long k, float (&v)[4]) {
+    const float4 t = __ldg(reinterpret_cast<const float4*>(p) + k);
+    v[0] = t.x;
+    v[1] = t.y;
+    v[2] = t.z;
+    v[3] = t.w;
+  }
+  __device__ __forceinline__ static void st(float* p, long long k, const float (&v)[4]) {
+    reinterpret_cast<float4*>(p)[k] = make_float4(v[0], v[1], v[2], v[3]);
+  }
+};
+template <>
+struct Chunk<double> {
+  static constexpr int N = 2;
+  __device__ __forceinline__ static void ld(const double* p, long long k, double (&v)[2]) {
+    const double2 t = __ldg(reinterpret_cast<const double2*>(p) + k);
+    v[0] = t.x;
+    v[1] = t.y;
+  }
+  __device__ __forceinline__ static void st(double* p, long long k, const double (&v)[2]) {
+    reinterpret_cast<double2*>(p)[k] = make_double2(v[0], v[1]);
+  }
+};
+
 // Jacobi weights and flags of the 4 nodes of quad t (w, fl: 16- and 4-byte aligned bases)
 __device__ __forceinline__ void ld_quad_node(const double* w, const uint8_t* fl, long long t, double (&wn)[4],
                                              unsigned& f4) {
