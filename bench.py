@@ -124,7 +124,7 @@ def solve_step(P, rho=None, form="mixed"):
     g = P["grid"]
     s, _ = g.simp(P["rho"] if rho is None else rho, 3.0, 1e-9, want_ds=False)
     if form == "mixed":
-        return g.dpcg_mixed(s, P["F"], P["defl"], rtol=RTOL, delta=P.get("delta", 1e-2), max_iters=8000,
+        return g.dpcg_mixed(s, P["F"], P["defl"], rtol=RTOL, delta=P.get("delta", 1e-1), max_iters=8000,
                             check_every=20)
     return g.dpcg(s, P["F"], P["defl"], rtol=RTOL, max_iters=5000, stop_rule=0, check_every=20)
 
@@ -209,7 +209,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--form", default="mixed", choices=["mixed", "fp64"],
                     help="timed solver: FP64 refinement around FP32 deflated PCG, or plain FP64 deflated PCG")
-    ap.add_argument("--delta", type=float, default=1e-2, help="mixed form: FP64 residual update each time the FP32 residual drops by this factor")
+    ap.add_argument("--delta", type=float, default=1e-1, help="mixed form: FP64 residual update each time the FP32 residual drops by this factor")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

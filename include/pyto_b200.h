@@ -70,7 +70,8 @@ typedef struct pyto_operator {
 typedef struct pyto_solve_cfg {
   double rtol;          /* relative tolerance of the stopping rule */
   int32_t max_iters;    /* iteration cap */
-  int32_t stop_rule;    /* 0: ||r||_2 < rtol ||b||_2 (scipy cg); 1: sqrt(r.z / r0.z0) <= rtol (PyTO DPCG) */
+  int32_t stop_rule;    /* 0: ||r||_2 < rtol ||b||_2 (scipy cg); 1: sqrt(r.z / r0.z0) <= rtol (PyTO DPCG);
+                           2 (pyto_dpcg_solve only): FP64 residual replacement, see there */
   int32_t check_every;  /* host polls convergence every this many iterations (>=1) */
   int32_t x0_given;     /* 1: u holds the initial guess on entry; 0: start from zero */
 } pyto_solve_cfg_t;
@@ -198,7 +199,11 @@ int pyto_pcg_solve(const pyto_operator_t* op, const double* s, const uint8_t* ma
 int pyto_dpcg_setup(const pyto_operator_t* op, const double* s, const uint8_t* mask,
                     pyto_deflation_t* defl, void* ws, size_t ws_bytes, void* stream);
 /* Deflated PCG (src/deflation.py:504-584): coarse start, p0 = z - W mu, per iteration
- * one coarse correction; stopping rule per cfg.  b and u must be 16-byte aligned.  With
+ * one coarse correction; stopping rule per cfg (0: scipy, 1: PyTO).  cfg->stop_rule = 2
+ * selects FP64 residual replacement: the recurrence of rule 0, but whenever ||r|| has
+ * dropped 100-fold the coarse part of the true residual is removed and r is replaced by
+ * b - K u; converged when ||b - K u|| <= rtol ||b|| (robust at tight tolerances where the
+ * recurrence alone drifts).  b and u must be 16-byte aligned.  With
  * boundary lists in defl, W_f^T K z is formed from the group-boundary elements instead
  * of a second full matvec per iteration.  Replaces DeflationSolver.deflatedPCG. */
 int pyto_dpcg_solve(const pyto_operator_t* op, const double* s, const uint8_t* mask,

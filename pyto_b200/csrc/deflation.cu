@@ -1101,6 +1101,9 @@ struct DpcgWs {
 };
 
 constexpr long long kMaxCoarse = 24576;  // coarse vector staged in shared memory (192 KB)
+constexpr double kReliableDelta = 1e-2;  // FP64 residual replacement each time ||r|| drops 100-fold
+constexpr int kReliableSegment = 100;    // and at least every this many iterations
+constexpr int kMaxRestarts = 64;         // direction restarts before giving up
 
 static DpcgWs carve_dpcg(const pyto_operator_t* op, long long nc, void* ws, size_t bytes, size_t* need,
                          bool mixed = false) {
@@ -1373,16 +1376,50 @@ __global__ void k_cast(long long n, const A* __restrict__ a, B* __restrict__ b) 
     b[i] = (B)a[i];
 }
 
-// Reliable update of the mixed solver: r = b - t (t = K u in FP64, fixed DOFs
-// masked), r32 = (float) r, z32 = M^-1 r32.  The last block sets rr = true_rr =
-// ||r||^2 (FP64), rz = r32.z32, bb = ||b||^2, clears the breakdown flag and sets
-// converged/done from the FP64 residual.
+// Reliable update: r = b - t in FP64 (t = K u, fixed DOFs masked).  With
+// scaled = 1 the recurrence vectors are normalised: r_T = r / ||r||, z_T =
+// M^-1 r_T, and the state records rscale2 = ||r||^2 (the FP32 recurrence then
+// works on O(1) values whatever the magnitude of b); otherwise r_T = r.  Two
+// passes: the first forms ||r||^2 and ||b||^2, the second writes r_T, z_T and
+// r_T.z_T.  The last block of the second pass sets rr (recurrence units),
+// true_rr = ||r||^2, bb, rz, clears the breakdown flag and sets converged/done
+// from the FP64 residual.
+__global__ void __launch_bounds__(kNodeThreads) k_residual_norms(GridDims g, const double* __restrict__ b,
+                                                                 const double* __restrict__ t,
+                                                                 const uint8_t* __restrict__ fl, KrylovState* S,
+                                                                 double* part, unsigned* counter) {
+  __shared__ double sred[kNodeThreads / 32];
+  double rr = 0.0, bb = 0.0;
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < g.nnodes;
+       n += (long long)gridDim.x * blockDim.x) {
+    const int f = fl[n];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      if ((f >> c) & 1) continue;
+      const double bi = b[3 * n + c], ri = bi - t[3 * n + c];
+      rr = fma(ri, ri, rr);
+      bb = fma(bi, bi, bb);
+    }
+  }
+  double v[2] = {block_sum<kNodeThreads>(rr, sred), block_sum<kNodeThreads>(bb, sred)};
+  grid_reduce<2>(v, part, counter, gridDim.x, [&](const double* tot) {
+    S->true_rr = tot[0];
+    S->bb = tot[1];
+    S->rscale2_prev = S->rscale2;
+    S->rscale2 = tot[0] > 0.0 ? tot[0] : 1.0;
+  });
+}
+
+template <typename T>
 __global__ void __launch_bounds__(kNodeThreads) k_reliable(GridDims g, Prec pc, const double* __restrict__ b,
                                                            const double* __restrict__ t, const double* __restrict__ w,
-                                                           const uint8_t* __restrict__ fl, float* __restrict__ r32,
-                                                           float* __restrict__ z32, KrylovState* S, double* part,
-                                                           unsigned* counter) {
+                                                           const uint8_t* __restrict__ fl, T* __restrict__ r32,
+                                                           T* __restrict__ z32, T* __restrict__ p, KrylovState* S,
+                                                           double* part, unsigned* counter, int scaled) {
   __shared__ double sred[kNodeThreads / 32];
+  const double isc = scaled ? 1.0 / sqrt(S->rscale2) : 1.0;
+  // the kept search direction moves to the units of the new residual
+  const T psc = (scaled && p && S->rscale2_prev > 0.0) ? (T)sqrt(S->rscale2_prev / S->rscale2) : T(1);
   double rz = 0.0, rr = 0.0, bb = 0.0;
   for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < g.nnodes;
        n += (long long)gridDim.x * blockDim.x) {
@@ -1393,11 +1430,12 @@ __global__ void __launch_bounds__(kNodeThreads) k_reliable(GridDims g, Prec pc, 
       const long long i = 3 * n + c;
       const bool fixed = (f >> c) & 1;
       const double bi = fixed ? 0.0 : b[i];
-      const double ri = fixed ? 0.0 : bi - t[i];
-      const float rf = (float)ri;
-      const float zf = (float)jacobi_apply((double)rf, f, c, wn, pc);
+      const double ri = (fixed ? 0.0 : bi - t[i]) * isc;
+      const T rf = (T)ri;
+      const T zf = (T)jacobi_apply((double)rf, f, c, wn, pc);
       r32[i] = rf;
       z32[i] = zf;
+      if (psc != T(1)) p[i] *= psc;
       rz = fma((double)rf, (double)zf, rz);
       rr = fma(ri, ri, rr);
       bb = fma(bi, bi, bb);
@@ -1408,32 +1446,222 @@ __global__ void __launch_bounds__(kNodeThreads) k_reliable(GridDims g, Prec pc, 
   v[1] = block_sum<kNodeThreads>(rr, sred);
   v[2] = block_sum<kNodeThreads>(bb, sred);
   grid_reduce<3>(v, part, counter, gridDim.x, [&](const double* tot) {
+    // tot[1] = ||r_T||^2, tot[2] = ||b||^2 (b is not scaled)
     S->rz = tot[0];
     S->rr = tot[1];
-    S->true_rr = tot[1];
+    if (!scaled) {
+      S->true_rr = tot[1];
+      S->rscale2 = 0.0;
+    }
     S->bb = tot[2];
     S->breakdown = 0;
-    const int conv = (tot[2] == 0.0 || sqrt(tot[1]) <= S->rtol * sqrt(tot[2])) ? 1 : 0;
+    const int conv = (tot[2] == 0.0 || sqrt(S->true_rr) <= S->rtol * sqrt(tot[2])) ? 1 : 0;
     S->converged = conv;
     S->done = conv;
   });
 }
 
-// u += (double) x
-__global__ void k_add_f32(long long n, const float* __restrict__ x, double* __restrict__ u) {
+// u += sqrt(S->rscale2) (double) x   (the FP32 iterate is in the units of the
+// normalised residual)
+__global__ void k_add_f32(long long n, const float* __restrict__ x, const KrylovState* S, double* __restrict__ u) {
+  const double sc = S->rscale2 > 0.0 ? sqrt(S->rscale2) : 1.0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    u[i] += (double)x[i];
+    u[i] = fma(sc, (double)x[i], u[i]);
 }
 
 }  // namespace pyto
 
 using namespace pyto;
 
+
+// Deflated PCG with reliable updates, vectors in precision T (float: the
+// mixed solver; double: the FP64 solver with residual replacement).  The
+// recurrence runs on T vectors with the T operator (FP64 reductions, scalars and
+// coarse inverse); u is FP64.  Whenever the recursive residual has dropped by
+// delta since the last update, or meets rtol, the iterate is folded into u,
+// the coarse part of the true residual is removed (u += W Einv W_f^T (b - K u):
+// the DEF2 recurrence never changes W_f^T r), and the residual is replaced by
+// b - K u computed in FP64; the search direction is kept.
+template <typename T>
+struct RelVec;
+template <>
+struct RelVec<float> {
+  static float* r(const DpcgWs& W) { return W.r32; }
+  static float* p(const DpcgWs& W) { return W.p32; }
+  static float* q(const DpcgWs& W) { return W.q32; }
+  static float* z(const DpcgWs& W) { return W.z32; }
+};
+template <>
+struct RelVec<double> {
+  static double* r(const DpcgWs& W) { return W.r; }
+  static double* p(const DpcgWs& W) { return W.p; }
+  static double* q(const DpcgWs& W) { return W.q; }
+  static double* z(const DpcgWs& W) { return W.z; }
+};
+
+template <typename T>
+static int dpcg_reliable(const pyto_operator_t* op, const double* s, const uint8_t* mask,
+                         const pyto_deflation_t* defl, const double* b, double* u, const pyto_solve_cfg_t* cfg,
+                         double delta, pyto_solve_status_t* status, const DpcgWs& W, cudaStream_t st) {
+  constexpr bool F32 = sizeof(T) == 4;
+  const DeflP dp = make_deflp(op, defl);
+  const GridDims g = make_dims(op);
+  const Prec pc = make_prec(op);
+  const long long nd = 3 * g.nnodes;
+  const int nb = (int)std::min<long long>((nd + 255) / 256, 8 * kNumSMs);
+  const int every = std::max(1, cfg->check_every);
+  T* r = RelVec<T>::r(W);
+  T* p = RelVec<T>::p(W);
+  T* q = RelVec<T>::q(W);
+  T* z = RelVec<T>::z(W);
+  T* x = nullptr;  // iterate of the recurrence: FP32 accumulator, or u itself
+  const T* sT = nullptr;
+  if constexpr (F32) {
+    x = W.x32;
+    sT = W.s32;
+  } else {
+    x = u;
+    sT = s;
+  }
+  int rc;
+  PYTO_CUDA(cudaMemsetAsync(W.counter, 0, 64 * sizeof(unsigned), st));
+  if ((rc = pyto_jacobi(op, s, mask, W.w, W.fl, nullptr, st))) return rc;
+  if constexpr (F32) {
+    k_cast<double, float><<<nb, 256, 0, st>>>(g.nelem, s, W.s32);
+    PYTO_COUNT(1);
+  }
+  const int nchunks = chunk_setup(defl, W, st);
+  if (nchunks < 0) return nchunks;
+  const bool lists = nchunks > 0;
+  k_state_init2<<<1, 1, 0, st>>>(W.S, cfg->rtol, cfg->max_iters, 0);
+  PYTO_COUNT(1);
+  // coarse start in FP64: u = W Einv W_f^T b   (src/deflation.py:532-537)
+  if ((rc = coarse_solve(g, dp, defl, b, W, nullptr, st))) return rc;
+  k_prolong<double><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center, W.mu, W.fl, u);
+  PYTO_COUNT(1);
+
+  auto reliable = [&](bool coarse) -> int {
+    int e;
+    if (coarse) {
+      if ((e = launch_matvec64(op, s, mask, u, W.q, PYTO_MASK_IN | PYTO_MASK_OUT, nullptr, nullptr, nullptr, st)))
+        return e;
+      // the FP64 residual goes to W.r: free at this point (for T = double it is the
+      // recurrence residual, replaced below); W.q (K u) is likewise dead here
+      k_residual64<<<nb, 256, 0, st>>>(nd, b, W.q, W.fl, W.r);
+      PYTO_COUNT(1);
+      if ((e = coarse_solve(g, dp, defl, (const double*)W.r, W, nullptr, st))) return e;
+      k_prolong<double, true><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center,
+                                                                    W.mu, W.fl, u);
+      PYTO_COUNT(1);
+    }
+    if ((e = launch_matvec64(op, s, mask, u, W.q, PYTO_MASK_IN | PYTO_MASK_OUT, nullptr, nullptr, nullptr, st)))
+      return e;
+    if constexpr (F32) {
+      k_residual_norms<<<kNodeBlocks, kNodeThreads, 0, st>>>(g, b, W.q, W.fl, W.S, W.part, W.counter);
+      PYTO_COUNT(1);
+    }
+    k_reliable<T><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, pc, b, W.q, W.w, W.fl, r, z, coarse ? p : nullptr, W.S,
+                                                        W.part, W.counter, F32 ? 1 : 0);
+    PYTO_COUNT(1);
+    if constexpr (F32) PYTO_CUDA(cudaMemsetAsync(W.x32, 0, nd * sizeof(float), st));
+    return PYTO_OK;
+  };
+  auto restart_p = [&]() -> int {  // p = z - W Einv W^T K z
+    int e;
+    if (lists) {
+      if ((e = coarse_update_K(op, g, dp, defl, sT, (const T*)z, p, W, nchunks, W.S, 1, st))) return e;
+    } else {
+      if ((e = matvec_t(op, sT, mask, z, q, nullptr, nullptr, nullptr, st))) return e;
+      if ((e = coarse_solve(g, dp, defl, (const T*)q, W, nullptr, st))) return e;
+      k_dpcg_update2<T><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center, W.mu,
+                                                              W.fl, z, p, W.S, 1);
+      PYTO_COUNT(1);
+    }
+    return PYTO_OK;
+  };
+  if ((rc = reliable(false))) return rc;
+  if ((rc = restart_p())) return rc;
+  PYTO_LAUNCH_CHECK();
+  KrylovState hs{};
+  PYTO_CUDA(cudaMemcpyAsync(&hs, W.S, sizeof(hs), cudaMemcpyDeviceToHost, st));
+  PYTO_CUDA(cudaStreamSynchronize(st));
+  double rr_ref = hs.rr;
+  double true_prev = hs.true_rr;  // true ||r||^2 at the previous update
+  int updates = 1, restarts = 0, seg0 = 0;
+  const double d2 = delta * delta;
+  while (!hs.converged && hs.iters < cfg->max_iters) {
+    for (int k = 0; k < every; ++k) {
+      if ((rc = matvec_t(op, sT, mask, p, q, W.part, W.counter, &W.S->pq, st))) return rc;
+      k_dpcg_update1<T><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, pc, W.w, W.fl, x, r, z, p, q, W.S, W.part,
+                                                              W.counter);
+      PYTO_COUNT(1);
+      if (lists) {
+        if ((rc = coarse_update_K(op, g, dp, defl, sT, (const T*)z, p, W, nchunks, W.S, 0, st))) return rc;
+      } else {
+        if ((rc = matvec_t(op, sT, mask, z, q, nullptr, nullptr, nullptr, st))) return rc;
+        if ((rc = coarse_solve(g, dp, defl, (const T*)q, W, W.S, st))) return rc;
+        k_dpcg_update2<T><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center, W.mu,
+                                                                W.fl, z, p, W.S, 0);
+        PYTO_COUNT(1);
+      }
+    }
+    PYTO_LAUNCH_CHECK();
+    PYTO_CUDA(cudaMemcpyAsync(&hs, W.S, sizeof(hs), cudaMemcpyDeviceToHost, st));
+    PYTO_CUDA(cudaStreamSynchronize(st));
+    if (!(hs.done || hs.rr <= d2 * rr_ref || hs.iters - seg0 >= kReliableSegment)) continue;
+    // fold the FP32 iterate into u; replace the recursive residual by the true one
+    if constexpr (F32) {
+      k_add_f32<<<nb, 256, 0, st>>>(nd, W.x32, W.S, u);
+      PYTO_COUNT(1);
+    }
+    const bool brk = hs.breakdown != 0;
+    if ((rc = reliable(true))) return rc;
+    ++updates;
+    PYTO_LAUNCH_CHECK();
+    PYTO_CUDA(cudaMemcpyAsync(&hs, W.S, sizeof(hs), cudaMemcpyDeviceToHost, st));
+    PYTO_CUDA(cudaStreamSynchronize(st));
+    // p.Kp <= 0, or a segment that did not halve the true residual: restart the
+    // search direction from the new residual (the recurrence has lost the
+    // conjugacy that the low-precision operator could support)
+    if (!hs.converged && (brk || hs.true_rr > 0.25 * true_prev)) {
+      if (++restarts > kMaxRestarts) break;
+      if ((rc = restart_p())) return rc;
+    }
+    rr_ref = hs.rr;
+    true_prev = hs.true_rr;
+    seg0 = hs.iters;
+  }
+  status->converged = hs.converged;
+  status->iters = hs.iters;
+  status->breakdown = restarts > kMaxRestarts ? 1 : 0;
+  status->reserved = updates;
+  status->rel_res = hs.bb > 0 ? sqrt(hs.rr * (hs.rscale2 > 0.0 ? hs.rscale2 : 1.0) / hs.bb) : 0.0;
+  status->true_rel_res = hs.bb > 0 ? sqrt(hs.true_rr / hs.bb) : 0.0;
+  if (status->breakdown && !hs.converged) return PYTO_ERR_BREAKDOWN;
+  return hs.converged ? PYTO_OK : PYTO_NOT_CONVERGED;
+}
+
+extern "C" int pyto_dpcg_mixed_solve(const pyto_operator_t* op, const double* s, const uint8_t* mask,
+                                     const pyto_deflation_t* defl, const double* b, double* u,
+                                     const pyto_solve_cfg_t* cfg, double delta, pyto_solve_status_t* status,
+                                     void* ws, size_t ws_bytes, void* stream) {
+  if (!op || !s || !b || !u || !cfg || !status || !defl_ok(defl)) return PYTO_ERR_ARG;
+  if (!(cfg->rtol > 0.0) || !(delta > 0.0) || !(delta < 1.0) || cfg->max_iters < 0) return PYTO_ERR_ARG;
+  if (((uintptr_t)b | (uintptr_t)u | (uintptr_t)defl->node_group) & 15) return PYTO_ERR_ARG;
+  const DeflP dp = make_deflp(op, defl);
+  int rc = gemv_smem_ok(dp.nc);
+  if (rc) return rc;
+  size_t need = 0;
+  DpcgWs W = carve_dpcg(op, dp.nc, ws, ws_bytes, &need, true);
+  if (!ws || ws_bytes < need) return PYTO_ERR_WORKSPACE;
+  return dpcg_reliable<float>(op, s, mask, defl, b, u, cfg, delta, status, W, (cudaStream_t)stream);
+}
+
 extern "C" int pyto_dpcg_solve(const pyto_operator_t* op, const double* s, const uint8_t* mask,
                                const pyto_deflation_t* defl, const double* b, double* u, const pyto_solve_cfg_t* cfg,
                                pyto_solve_status_t* status, void* ws, size_t ws_bytes, void* stream) {
   if (!op || !s || !b || !u || !cfg || !status || !defl_ok(defl)) return PYTO_ERR_ARG;
-  if (!(cfg->rtol >= 0.0) || cfg->max_iters < 0 || cfg->stop_rule < 0 || cfg->stop_rule > 1) return PYTO_ERR_ARG;
+  if (!(cfg->rtol >= 0.0) || cfg->max_iters < 0 || cfg->stop_rule < 0 || cfg->stop_rule > 2) return PYTO_ERR_ARG;
   if (((uintptr_t)b | (uintptr_t)u | (uintptr_t)defl->node_group) & 15) return PYTO_ERR_ARG;
   const DeflP dp = make_deflp(op, defl);
   int rc = gemv_smem_ok(dp.nc);
@@ -1442,6 +1670,10 @@ extern "C" int pyto_dpcg_solve(const pyto_operator_t* op, const double* s, const
   DpcgWs W = carve_dpcg(op, dp.nc, ws, ws_bytes, &need);
   if (!ws || ws_bytes < need) return PYTO_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
+  if (cfg->stop_rule == 2) {
+    if (!(cfg->rtol > 0.0)) return PYTO_ERR_ARG;
+    return dpcg_reliable<double>(op, s, mask, defl, b, u, cfg, kReliableDelta, status, W, st);
+  }
   const GridDims g = make_dims(op);
   PYTO_CUDA(cudaMemsetAsync(W.counter, 0, 64 * sizeof(unsigned), st));
   if ((rc = pyto_jacobi(op, s, mask, W.w, W.fl, nullptr, stream))) return rc;
@@ -1464,128 +1696,5 @@ extern "C" int pyto_dpcg_solve(const pyto_operator_t* op, const double* s, const
                                       : (before.rz0 > 0 ? sqrt(before.rz / before.rz0) : 0.0);
   status->true_rel_res = hs.bb > 0 ? sqrt(hs.true_rr / hs.bb) : 0.0;
   if (hs.breakdown) return PYTO_ERR_BREAKDOWN;
-  return hs.converged ? PYTO_OK : PYTO_NOT_CONVERGED;
-}
-
-extern "C" int pyto_dpcg_mixed_solve(const pyto_operator_t* op, const double* s, const uint8_t* mask,
-                                     const pyto_deflation_t* defl, const double* b, double* u,
-                                     const pyto_solve_cfg_t* cfg, double delta, pyto_solve_status_t* status,
-                                     void* ws, size_t ws_bytes, void* stream) {
-  if (!op || !s || !b || !u || !cfg || !status || !defl_ok(defl)) return PYTO_ERR_ARG;
-  if (!(cfg->rtol > 0.0) || !(delta > 0.0) || !(delta < 1.0) || cfg->max_iters < 0) return PYTO_ERR_ARG;
-  if (((uintptr_t)b | (uintptr_t)u | (uintptr_t)defl->node_group) & 15) return PYTO_ERR_ARG;
-  const DeflP dp = make_deflp(op, defl);
-  int rc = gemv_smem_ok(dp.nc);
-  if (rc) return rc;
-  size_t need = 0;
-  DpcgWs W = carve_dpcg(op, dp.nc, ws, ws_bytes, &need, true);
-  if (!ws || ws_bytes < need) return PYTO_ERR_WORKSPACE;
-  cudaStream_t st = (cudaStream_t)stream;
-  const GridDims g = make_dims(op);
-  const Prec pc = make_prec(op);
-  const long long nd = 3 * g.nnodes;
-  const int nb = (int)std::min<long long>((nd + 255) / 256, 8 * kNumSMs);
-  const int every = std::max(1, cfg->check_every);
-  PYTO_CUDA(cudaMemsetAsync(W.counter, 0, 64 * sizeof(unsigned), st));
-  if ((rc = pyto_jacobi(op, s, mask, W.w, W.fl, nullptr, stream))) return rc;
-  k_cast<double, float><<<nb, 256, 0, st>>>(g.nelem, s, W.s32);
-  PYTO_COUNT(1);
-  const int nchunks = chunk_setup(defl, W, st);
-  if (nchunks < 0) return nchunks;
-  const bool lists = nchunks > 0;
-  k_state_init2<<<1, 1, 0, st>>>(W.S, cfg->rtol, cfg->max_iters, 0);
-  PYTO_COUNT(1);
-  // coarse start in FP64: u = W Einv W_f^T b   (src/deflation.py:532-537)
-  if ((rc = coarse_solve(g, dp, defl, b, W, nullptr, st))) return rc;
-  k_prolong<double><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center, W.mu, W.fl, u);
-  PYTO_COUNT(1);
-
-  // r = b - K u in FP64, handed to the FP32 recurrence; the FP32 iterate x32 restarts at 0.
-  // The DEF2 recurrence never changes W_f^T r (W_f^T K p = 0 for every direction),
-  // so a residual update first removes its coarse part: u += W Einv W_f^T (b - K u).
-  auto reliable = [&](bool coarse) -> int {
-    int e;
-    if (coarse) {
-      if ((e = launch_matvec64(op, s, mask, u, W.q, PYTO_MASK_IN | PYTO_MASK_OUT, nullptr, nullptr, nullptr, st)))
-        return e;
-      k_residual64<<<nb, 256, 0, st>>>(nd, b, W.q, W.fl, W.r);
-      PYTO_COUNT(1);
-      if ((e = coarse_solve(g, dp, defl, (const double*)W.r, W, nullptr, st))) return e;
-      k_prolong<double, true><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center,
-                                                                    W.mu, W.fl, u);
-      PYTO_COUNT(1);
-    }
-    if ((e = launch_matvec64(op, s, mask, u, W.q, PYTO_MASK_IN | PYTO_MASK_OUT, nullptr, nullptr, nullptr, st)))
-      return e;
-    k_reliable<<<kNodeBlocks, kNodeThreads, 0, st>>>(g, pc, b, W.q, W.w, W.fl, W.r32, W.z32, W.S, W.part,
-                                                     W.counter);
-    PYTO_COUNT(1);
-    PYTO_CUDA(cudaMemsetAsync(W.x32, 0, nd * sizeof(float), st));
-    return PYTO_OK;
-  };
-  auto restart_p = [&]() -> int {  // p = z - W Einv W^T K z
-    int e;
-    if (lists) {
-      if ((e = coarse_update_K(op, g, dp, defl, W.s32, W.z32, W.p32, W, nchunks, W.S, 1, st))) return e;
-    } else {
-      if ((e = matvec_t(op, W.s32, mask, W.z32, W.q32, nullptr, nullptr, nullptr, st))) return e;
-      if ((e = coarse_solve(g, dp, defl, W.q32, W, nullptr, st))) return e;
-      k_dpcg_update2<float><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center,
-                                                                  W.mu, W.fl, W.z32, W.p32, W.S, 1);
-      PYTO_COUNT(1);
-    }
-    return PYTO_OK;
-  };
-  if ((rc = reliable(false))) return rc;
-  if ((rc = restart_p())) return rc;
-  PYTO_LAUNCH_CHECK();
-  KrylovState hs{};
-  PYTO_CUDA(cudaMemcpyAsync(&hs, W.S, sizeof(hs), cudaMemcpyDeviceToHost, st));
-  PYTO_CUDA(cudaStreamSynchronize(st));
-  double rr_ref = hs.rr;
-  int updates = 1, restarts = 0;
-  const double d2 = delta * delta;
-  while (!hs.converged && hs.iters < cfg->max_iters) {
-    for (int k = 0; k < every; ++k) {
-      if ((rc = matvec_t(op, W.s32, mask, W.p32, W.q32, W.part, W.counter, &W.S->pq, st))) return rc;
-      k_dpcg_update1<float><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, pc, W.w, W.fl, W.x32, W.r32, W.z32, W.p32,
-                                                                  W.q32, W.S, W.part, W.counter);
-      PYTO_COUNT(1);
-      if (lists) {
-        if ((rc = coarse_update_K(op, g, dp, defl, W.s32, W.z32, W.p32, W, nchunks, W.S, 0, st))) return rc;
-      } else {
-        if ((rc = matvec_t(op, W.s32, mask, W.z32, W.q32, nullptr, nullptr, nullptr, st))) return rc;
-        if ((rc = coarse_solve(g, dp, defl, W.q32, W, W.S, st))) return rc;
-        k_dpcg_update2<float><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center,
-                                                                    W.mu, W.fl, W.z32, W.p32, W.S, 0);
-        PYTO_COUNT(1);
-      }
-    }
-    PYTO_LAUNCH_CHECK();
-    PYTO_CUDA(cudaMemcpyAsync(&hs, W.S, sizeof(hs), cudaMemcpyDeviceToHost, st));
-    PYTO_CUDA(cudaStreamSynchronize(st));
-    if (!(hs.done || hs.rr <= d2 * rr_ref)) continue;
-    // fold the FP32 iterate into u and replace the recursive residual by the true one
-    k_add_f32<<<nb, 256, 0, st>>>(nd, W.x32, u);
-    PYTO_COUNT(1);
-    const bool brk = hs.breakdown != 0;
-    if ((rc = reliable(true))) return rc;
-    ++updates;
-    if (brk) {  // p.Kp <= 0 in FP32: restart the search direction from the new residual
-      if (++restarts > 8) break;
-      if ((rc = restart_p())) return rc;
-    }
-    PYTO_LAUNCH_CHECK();
-    PYTO_CUDA(cudaMemcpyAsync(&hs, W.S, sizeof(hs), cudaMemcpyDeviceToHost, st));
-    PYTO_CUDA(cudaStreamSynchronize(st));
-    rr_ref = hs.rr;
-  }
-  status->converged = hs.converged;
-  status->iters = hs.iters;
-  status->breakdown = restarts > 8 ? 1 : 0;
-  status->reserved = updates;
-  status->rel_res = hs.bb > 0 ? sqrt(hs.rr / hs.bb) : 0.0;
-  status->true_rel_res = hs.bb > 0 ? sqrt(hs.true_rr / hs.bb) : 0.0;
-  if (status->breakdown && !hs.converged) return PYTO_ERR_BREAKDOWN;
   return hs.converged ? PYTO_OK : PYTO_NOT_CONVERGED;
 }

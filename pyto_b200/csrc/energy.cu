@@ -201,13 +201,16 @@ __global__ void __launch_bounds__(kElemThreads) k_pnorm_elem(GridDims g, StressP
       sig[i] = t * rq;
     }
     const double vmv = von_mises(sig);
+    // d vm / d sigma; at vm = 0 (an unstressed or void element) vm^(P-1) d vm/d sigma
+    // = vm^(P-2) V sigma has the limit 0, so the element contributes nothing
+    const double iv = vmv > 0.0 ? 1.0 / vmv : 0.0;
     double dv[6];
-    dv[0] = 1.0 / (2.0 * vmv) * (2.0 * sig[0] - sig[1] - sig[2]);
-    dv[1] = 1.0 / (2.0 * vmv) * (2.0 * sig[1] - sig[0] - sig[2]);
-    dv[2] = 1.0 / (2.0 * vmv) * (2.0 * sig[2] - sig[0] - sig[1]);
-    dv[3] = 3.0 / vmv * sig[3];
-    dv[4] = 3.0 / vmv * sig[4];
-    dv[5] = 3.0 / vmv * sig[5];
+    dv[0] = 0.5 * iv * (2.0 * sig[0] - sig[1] - sig[2]);
+    dv[1] = 0.5 * iv * (2.0 * sig[1] - sig[0] - sig[2]);
+    dv[2] = 0.5 * iv * (2.0 * sig[2] - sig[0] - sig[1]);
+    dv[3] = 3.0 * iv * sig[3];
+    dv[4] = 3.0 * iv * sig[4];
+    dv[5] = 3.0 * iv * sig[5];
     const double xc = fmax(xe, 1e-12);
     const double vp = pow(vmv, P - 1.0);
     double dot = 0.0;

@@ -12,6 +12,8 @@ constexpr int kNodeThreads = 256;
 struct KrylovState {
   double rz, rz0, pq, rr, bb, alpha, beta, rtol;
   double true_rr;
+  double rscale2;  // squared scale of the recurrence vectors (residual r_true = sqrt(rscale2) r); 0 means 1
+  double rscale2_prev;  // rscale2 before the last residual replacement
   int iters, done, breakdown, converged;
   int max_iters, stop_rule, pad0, pad1;
 };
@@ -36,6 +38,7 @@ __device__ __forceinline__ double jacobi_apply(double r, int fl, int c, double w
 // stopping test after an update: rule 0 = scipy cg (||r|| < rtol ||b||, strict),
 // rule 1 = PyTO DPCG (sqrt(r.z / r0.z0) <= rtol, src/deflation.py:567)
 __device__ __forceinline__ bool krylov_converged(const KrylovState& S, double rr, double rz_new) {
+  if (S.rscale2 > 0.0) rr *= S.rscale2;
   if (S.stop_rule == 0) return sqrt(rr) < S.rtol * sqrt(S.bb);
   return sqrt(rz_new / S.rz0) <= S.rtol;
 }

@@ -163,7 +163,7 @@ class HexGrid:
         return u, SolveInfo(bool(stt.converged), int(stt.iters), bool(stt.breakdown), float(stt.rel_res),
                             float(stt.true_rel_res), rc)
 
-    def dpcg_mixed(self, s, b, defl, rtol=1e-8, delta=1e-2, max_iters=4000, check_every=10, out=None,
+    def dpcg_mixed(self, s, b, defl, rtol=1e-8, delta=1e-1, max_iters=4000, check_every=10, out=None,
                    setup=True):
         """Deflated PCG in mixed precision: an FP32 recurrence whose residual is replaced
         by the FP64 true residual b - K u (u held in FP64) each time it has dropped by

@@ -43,7 +43,7 @@ def main(argv=None):
     ap.add_argument("--warm", type=int, default=3)
     ap.add_argument("--variant", type=int, default=2, help="matvec tile variant (pyto_tune)")
     ap.add_argument("--variant32", type=int, default=None, help="FP32 matvec tile variant (pyto_tune)")
-    ap.add_argument("--delta", type=float, default=1e-2, help="reliable-update threshold for --kernel mixed")
+    ap.add_argument("--delta", type=float, default=1e-1, help="reliable-update threshold for --kernel mixed")
     a = ap.parse_args(argv)
     nel = tuple(int(v) for v in a.nel.split(","))
     A.call("pyto_tune", 0, a.variant)

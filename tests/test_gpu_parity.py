@@ -293,6 +293,31 @@ def test_dpcg_mixed_reaches_fp64_accuracy(nel, rtol):
     assert abs(C.item() - C2.item()) <= 10 * rtol * abs(C2.item())
 
 
+@pytest.mark.parametrize("rtol", [1e-10, 1e-12])
+def test_dpcg_fp64_residual_replacement(rtol):
+    """stop_rule 2: the true FP64 residual meets tolerances at which the plain
+    recurrence drifts; compliance agrees with a tight Jacobi PCG."""
+    from pyto_b200.engine import DeviceDeflation
+    nel = (12, 6, 6)
+    m = O.grid_mesh(*nel)
+    f, fixed = O.cantilever_bc(m)
+    g = _grid(nel, fixed=fixed)
+    rng = np.random.default_rng(1)
+    s, _ = g.simp(_dev(rng.uniform(0.01, 1.0, m["num_elems"])), 3.0, 1e-9)
+    grp, cnt, cen = O.deflation_groups(m["node_xyz"], 8)
+    defl = DeviceDeflation(g, grp, cen, modes=6, shift=1e-14, shift_relative=True)
+    b = _dev(f)
+    u, info = g.dpcg(s, b, defl, rtol=rtol, stop_rule=2)
+    assert info.converged and info.true_rel_res <= rtol, info
+    r = b - g.matvec(s, u)
+    r[torch.as_tensor(fixed, device="cuda")] = 0
+    assert r.norm().item() <= rtol * b.norm().item() * 1.0000001
+    u2, _ = g.pcg(s, b, rtol=1e-13)
+    _, C = g.energy(u, s=s)
+    _, C2 = g.energy(u2, s=s)
+    assert abs(C.item() - C2.item()) <= 10 * rtol * abs(C2.item())
+
+
 def test_dpcg_mixed_golden_compliance():
     from pyto_b200.engine import DeviceDeflation
     d, m, g, s, ds = _cantilever_case("cantilever_12x6x6_direct.npz", (12, 6, 6), (1.0, 1.0, 1.0))
