@@ -59,7 +59,8 @@ extern "C" {
  * where a box hex8 Ke splits into eight 3x3 blocks, and the corner diagonal). */
 typedef struct pyto_operator {
   int32_t nelx, nely, nelz;
-  int32_t reserved;
+  int32_t tune;          /* per-grid matvec tile variants (the autotuner's choice): bits 0-7 =
+                            FP64 variant + 1, bits 8-15 = FP32 variant + 1; 0 = library default */
   double hx, hy, hz;
   double E, nu;          /* material of Ke (stress recovery uses them) */
   double ke[576];        /* 24x24 Ke, row-major, reference DOF order */
@@ -104,7 +105,7 @@ typedef struct pyto_deflation {
   const int32_t* nbr_ptr;      /* [ngroups+1] CSR offsets of nbr_list */
   const int32_t* nbr_list;     /* groups sharing an element with each group (incl. itself), ascending */
   int32_t max_nbr;             /* largest neighbour list (<= 128) */
-  int32_t reserved;
+  int32_t bel_count;           /* entries of bel_list (0: read from bel_ptr[ngroups] when needed) */
   /* Optional boundary element lists (NULL: the solver applies K to z with a full
    * matvec before restricting, as src/deflation.py:560-566 does).  A rigid mode of
    * a group is in the null space of every element whose 8 corners lie in that
@@ -117,6 +118,9 @@ typedef struct pyto_deflation {
 
 /* ---- version / workspace ------------------------------------------------- */
 int pyto_version(void);
+/* Description of the last CUDA call of this thread that failed inside the library
+ * (file:line, the call, the CUDA error); "" if none.  No reference counterpart. */
+const char* pyto_last_error(void);
 /* Number of kernel launches this library has issued in the process so far (no
  * reference counterpart: instrumentation of the launch count). */
 long long pyto_launch_count(void);
@@ -227,6 +231,39 @@ int pyto_dpcg_mixed_solve(const pyto_operator_t* op, const double* s, const uint
                           const pyto_deflation_t* defl, const double* b, double* u,
                           const pyto_solve_cfg_t* cfg, double delta, pyto_solve_status_t* status,
                           void* ws, size_t ws_bytes, void* stream);
+
+/* ---- batched solves in one CUDA graph ---------------------------------------------- */
+/* One independent deflated PCG problem of a batch (no reference counterpart: PyTO
+ * solves one problem per call).  op and defl are read when the batch is created; the
+ * device buffers (s, mask, b, u, the deflation arrays, ws) are read at every launch,
+ * so rewriting s and b and launching again solves new designs and load cases.  defl
+ * needs its boundary lists with bel_count set; each item needs its own PYTO_WS_DPCG
+ * workspace; b and u 16-byte aligned.  Items may share one deflation space (several load
+ * cases of one design: same op, s and mask, different b and u): the first of them builds
+ * the coarse inverse and the others wait for it. */
+typedef struct pyto_batch_item {
+  const pyto_operator_t* op;
+  const double* s;
+  const uint8_t* mask;
+  pyto_deflation_t* defl;
+  const double* b;
+  double* u;
+  void* ws;
+  size_t ws_bytes;
+} pyto_batch_item_t;
+typedef struct pyto_batch* pyto_batch_t;
+/* Capture every item's coarse set-up and deflated PCG (cfg: stop rule 0 or 1) into one
+ * CUDA graph: one concurrent branch per item, the iterations of each in a conditional
+ * WHILE node driven by the device-side stopping flag (ends on convergence, breakdown
+ * or cfg->max_iters).  Nothing runs at creation (the capture uses a private stream;
+ * `stream` is not used). */
+int pyto_batch_create(const pyto_batch_item_t* items, int n, const pyto_solve_cfg_t* cfg,
+                      pyto_batch_t* out, void* stream);
+/* One graph launch: coarse set-up and solve of every item, no host round trips. */
+int pyto_batch_launch(pyto_batch_t b, void* stream);
+/* status[n] of the last launch (synchronises the stream); returns the worst status. */
+int pyto_batch_status(pyto_batch_t b, pyto_solve_status_t* status, void* stream);
+int pyto_batch_destroy(pyto_batch_t b);
 
 /* ---- objectives and sensitivities ------------------------------------------------ */
 /* ce[e] = u_e^T Ke v_e (u == v gives the element energy of compliance).  If s != NULL and

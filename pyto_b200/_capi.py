@@ -29,15 +29,15 @@ class PytoLibraryError(RuntimeError):
 class PytoError(RuntimeError):
     """A C-ABI call returned an error status."""
 
-    def __init__(self, fn: str, rc: int):
+    def __init__(self, fn: str, rc: int, detail: str = ""):
         names = {ERR_ARG: "invalid argument", ERR_CUDA: "CUDA error", ERR_WORKSPACE: "workspace too small",
                  ERR_BREAKDOWN: "Krylov breakdown", ERR_TOO_LARGE: "size beyond limit"}
-        super().__init__(f"{fn} failed: {names.get(rc, rc)} ({rc})")
+        super().__init__(f"{fn} failed: {names.get(rc, rc)} ({rc})" + (f": {detail}" if detail else ""))
         self.rc = rc
 
 
 class Operator(C.Structure):
-    _fields_ = [("nelx", C.c_int32), ("nely", C.c_int32), ("nelz", C.c_int32), ("reserved", C.c_int32),
+    _fields_ = [("nelx", C.c_int32), ("nely", C.c_int32), ("nelz", C.c_int32), ("tune", C.c_int32),
                 ("hx", C.c_double), ("hy", C.c_double), ("hz", C.c_double), ("E", C.c_double), ("nu", C.c_double),
                 ("ke", C.c_double * 576), ("khat", C.c_double * 72), ("kdiag", C.c_double * 3)]
 
@@ -57,13 +57,20 @@ class Deflation(C.Structure):
                 ("group_nodes", C.c_void_p), ("group_center", C.c_void_p), ("coarse_inv", C.c_void_p),
                 ("shift", C.c_double), ("shift_relative", C.c_int32), ("max_group_nodes", C.c_int32),
                 ("group_box", C.c_void_p), ("nbr_ptr", C.c_void_p), ("nbr_list", C.c_void_p), ("max_nbr", C.c_int32),
-                ("reserved", C.c_int32), ("bel_ptr", C.c_void_p), ("bel_list", C.c_void_p)]
+                ("bel_count", C.c_int32), ("bel_ptr", C.c_void_p), ("bel_list", C.c_void_p)]
+
+
+class BatchItem(C.Structure):
+    _fields_ = [("op", C.POINTER(Operator)), ("s", C.c_void_p), ("mask", C.c_void_p),
+                ("defl", C.POINTER(Deflation)), ("b", C.c_void_p), ("u", C.c_void_p), ("ws", C.c_void_p),
+                ("ws_bytes", C.c_size_t)]
 
 
 _P = C.c_void_p
 _OP = C.POINTER(Operator)
 SIGNATURES = {
     "pyto_version": (C.c_int, []),
+    "pyto_last_error": (C.c_char_p, []),
     "pyto_launch_count": (C.c_longlong, []),
     "pyto_tune": (C.c_int, [C.c_int, C.c_int]),
     "pyto_workspace_bytes": (C.c_size_t, [_OP, C.c_int]),
@@ -83,6 +90,10 @@ SIGNATURES = {
                                   C.POINTER(SolveStatus), _P, C.c_size_t, _P]),
     "pyto_dpcg_mixed_solve": (C.c_int, [_OP, _P, _P, C.POINTER(Deflation), _P, _P, C.POINTER(SolveCfg), C.c_double,
                                         C.POINTER(SolveStatus), _P, C.c_size_t, _P]),
+    "pyto_batch_create": (C.c_int, [C.POINTER(BatchItem), C.c_int, C.POINTER(SolveCfg), C.POINTER(C.c_void_p), _P]),
+    "pyto_batch_launch": (C.c_int, [_P, _P]),
+    "pyto_batch_status": (C.c_int, [_P, C.POINTER(SolveStatus), _P]),
+    "pyto_batch_destroy": (C.c_int, [_P]),
     "pyto_elem_energy": (C.c_int, [_OP, _P, _P, _P, _P, _P, _P, C.c_size_t, _P]),
     "pyto_stress": (C.c_int, [_OP, _P, _P, C.c_double, _P, _P, _P, _P, _P]),
     "pyto_pnorm_sum": (C.c_int, [_OP, _P, C.c_double, _P, _P, C.c_size_t, _P]),
@@ -116,7 +127,12 @@ def lib():
 def call(fn: str, *args, allow=(OK,)) -> int:
     rc = getattr(lib(), fn)(*args)
     if rc not in allow:
-        raise PytoError(fn, rc)
+        err = PytoError(fn, rc)
+        if rc == ERR_CUDA:
+            detail = lib().pyto_last_error()
+            if detail:
+                err = PytoError(fn, rc, detail.decode(errors="replace"))
+        raise err
     return rc
 
 

@@ -1,6 +1,8 @@
 // Workspace sizing of the C ABI.
 #include <algorithm>
 #include <atomic>
+#include <cstdio>
+#include <cstring>
 
 #include "krylov.cuh"
 
@@ -15,6 +17,13 @@ int set_matvec32_variant(int v);
 namespace pyto {
 static std::atomic<long long> g_launches{0};
 void count_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+static thread_local char g_last_error[512] = "";
+void record_error(cudaError_t e, const char* what, const char* file, int line) {
+  const char* base = strrchr(file, '/');
+  snprintf(g_last_error, sizeof(g_last_error), "%s:%d: %s -> %s (%s)", base ? base + 1 : file, line, what,
+           cudaGetErrorName(e), cudaGetErrorString(e));
+}
 }  // namespace pyto
 
 using namespace pyto;
@@ -26,6 +35,8 @@ extern "C" int pyto_tune(int kernel, int variant) {
     default: return PYTO_ERR_ARG;
   }
 }
+
+extern "C" const char* pyto_last_error(void) { return g_last_error; }
 
 extern "C" long long pyto_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
 

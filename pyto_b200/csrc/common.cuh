@@ -5,10 +5,18 @@
 
 #include "../../include/pyto_b200.h"
 
-#define PYTO_CUDA(call)                              \
-  do {                                               \
-    cudaError_t _e = (call);                         \
-    if (_e != cudaSuccess) return PYTO_ERR_CUDA;     \
+namespace pyto {
+// records the failing CUDA call of this thread (read by pyto_last_error)
+void record_error(cudaError_t e, const char* what, const char* file, int line);
+}  // namespace pyto
+
+#define PYTO_CUDA(call)                                                 \
+  do {                                                                  \
+    cudaError_t _e = (call);                                            \
+    if (_e != cudaSuccess) {                                            \
+      ::pyto::record_error(_e, #call, __FILE__, __LINE__);              \
+      return PYTO_ERR_CUDA;                                             \
+    }                                                                   \
   } while (0)
 
 #define PYTO_LAUNCH_CHECK() PYTO_CUDA(cudaGetLastError())

@@ -19,6 +19,7 @@
 // then applies it with one dense GEMV, which is a single fully parallel pass
 // instead of two latency-bound triangular solves.
 #include <algorithm>
+#include <vector>
 
 #include "krylov.cuh"
 
@@ -1204,21 +1205,38 @@ static int coarse_update_K(const pyto_operator_t* op, const GridDims& g, const D
   return PYTO_OK;
 }
 
-// Chunk table of the boundary lists; returns the chunk count (0: no lists) or a
-// negative status.  The group counters are zeroed here and left at zero by
-// every k_restrict_K launch.
-static int chunk_setup(const pyto_deflation_t* d, const DpcgWs& W, cudaStream_t st) {
+// Upper bound of the chunk count of the boundary lists (0: no lists) or a
+// negative status.  Uses defl->bel_count when set; otherwise reads the list
+// size from the device (a synchronising copy).
+static int chunk_bound(const pyto_deflation_t* d, cudaStream_t st) {
   if (!d->bel_ptr || !d->bel_list) return 0;
-  int total = 0;
-  PYTO_CUDA(cudaMemcpyAsync(&total, d->bel_ptr + d->ngroups, sizeof(int), cudaMemcpyDeviceToHost, st));
-  PYTO_CUDA(cudaStreamSynchronize(st));
+  int total = d->bel_count;
+  if (total <= 0) {
+    PYTO_CUDA(cudaMemcpyAsync(&total, d->bel_ptr + d->ngroups, sizeof(int), cudaMemcpyDeviceToHost, st));
+    PYTO_CUDA(cudaStreamSynchronize(st));
+  }
   const long long bound = (long long)total / kRkChunk + d->ngroups;  // >= number of chunks
   if (total < 0 || bound > kRkMaxChunks) return PYTO_ERR_TOO_LARGE;
+  return (int)std::max<long long>(bound, 1);
+}
+
+// Chunk tables of the boundary lists (no host synchronisation: safe under
+// stream capture).  The group counters are zeroed here and left at zero by
+// every k_restrict_K launch.
+static int chunk_tables(const pyto_deflation_t* d, const DpcgWs& W, cudaStream_t st) {
   k_chunk_ptr<<<1, 1024, 0, st>>>(d->ngroups, d->bel_ptr, W.cptr, W.cgrp);
   PYTO_COUNT(1);
   PYTO_CUDA(cudaMemsetAsync(W.gcount, 0, (size_t)d->ngroups * sizeof(unsigned), st));
   PYTO_LAUNCH_CHECK();
-  return (int)std::max<long long>(bound, 1);
+  return PYTO_OK;
+}
+
+// chunk_bound + chunk_tables; returns the chunk count (0: no lists) or a negative status
+static int chunk_setup(const pyto_deflation_t* d, const DpcgWs& W, cudaStream_t st) {
+  const int nch = chunk_bound(d, st);
+  if (nch <= 0) return nch;
+  const int rc = chunk_tables(d, W, st);
+  return rc ? rc : nch;
 }
 
 static int gemv_smem_ok(long long nc) {
@@ -1238,22 +1256,15 @@ static int gemv_smem_ok(long long nc) {
 
 using namespace pyto;
 
-extern "C" int pyto_dpcg_setup(const pyto_operator_t* op, const double* s, const uint8_t* mask,
-                               pyto_deflation_t* defl, void* ws, size_t ws_bytes, void* stream) {
-  if (!op || !s || !defl_ok(defl)) return PYTO_ERR_ARG;
+// Coarse operator set-up launches (no host synchronisation: safe under stream
+// capture).  With nchunks > 0 the boundary-list chunk tables must be built.
+static int dpcg_setup_launch(const pyto_operator_t* op, const double* s, const uint8_t* mask,
+                             const pyto_deflation_t* defl, const DpcgWs& W, int nchunks, cudaStream_t st) {
   const DeflP dp = make_deflp(op, defl);
-  int rc0 = gemv_smem_ok(dp.nc);
-  if (rc0) return rc0;
-  size_t need = 0;
-  DpcgWs W = carve_dpcg(op, dp.nc, ws, ws_bytes, &need);
-  if (!ws || ws_bytes < need) return PYTO_ERR_WORKSPACE;
-  cudaStream_t st = (cudaStream_t)stream;
   const GridDims g = make_dims(op);
   double* E = defl->coarse_inv;
   const long long n = dp.nc;
   PYTO_CUDA(cudaMemsetAsync(E, 0, (size_t)n * n * sizeof(double), st));
-  const int nchunks = chunk_setup(defl, W, st);
-  if (nchunks < 0) return nchunks;
   const size_t shm = (size_t)defl->max_nbr * 36 * sizeof(double);
   if (nchunks > 0) {
     k_coarse_rows2<<<nchunks, kCrThreads, shm, st>>>(g, make_khat(op), dp, s, mask, defl->node_group,
@@ -1288,6 +1299,21 @@ extern "C" int pyto_dpcg_setup(const pyto_operator_t* op, const double* s, const
   PYTO_COUNT(1);
   PYTO_LAUNCH_CHECK();
   return PYTO_OK;
+}
+
+extern "C" int pyto_dpcg_setup(const pyto_operator_t* op, const double* s, const uint8_t* mask,
+                               pyto_deflation_t* defl, void* ws, size_t ws_bytes, void* stream) {
+  if (!op || !s || !defl_ok(defl)) return PYTO_ERR_ARG;
+  const DeflP dp = make_deflp(op, defl);
+  int rc0 = gemv_smem_ok(dp.nc);
+  if (rc0) return rc0;
+  size_t need = 0;
+  DpcgWs W = carve_dpcg(op, dp.nc, ws, ws_bytes, &need);
+  if (!ws || ws_bytes < need) return PYTO_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int nchunks = chunk_setup(defl, W, st);
+  if (nchunks < 0) return nchunks;
+  return dpcg_setup_launch(op, s, mask, defl, W, nchunks, st);
 }
 
 namespace pyto {
@@ -1697,4 +1723,249 @@ extern "C" int pyto_dpcg_solve(const pyto_operator_t* op, const double* s, const
   status->true_rel_res = hs.bb > 0 ? sqrt(hs.true_rr / hs.bb) : 0.0;
   if (hs.breakdown) return PYTO_ERR_BREAKDOWN;
   return hs.converged ? PYTO_OK : PYTO_NOT_CONVERGED;
+}
+
+// ---------------------------------------------------------------------------
+// Batched solves in one CUDA graph
+// ---------------------------------------------------------------------------
+// Every item becomes one branch of the graph (branches are independent and run
+// concurrently): the coarse set-up of pyto_dpcg_setup, the start of the
+// deflated PCG, and a conditional WHILE node whose body is one iteration
+// (matvec + dot, update, W^T K z from the boundary lists, coarse correction
+// and direction update) followed by a one-thread kernel that sets the loop
+// condition from the device-side stopping flag.  The flag is raised on
+// convergence, breakdown or max_iters, so every loop ends; kernels of a
+// converged item return at once.  A launch of the graph solves every item;
+// the item buffers are read at each launch, so new densities and loads only
+// need the buffers rewritten.
+
+__global__ void k_while_cond(cudaGraphConditionalHandle h, const KrylovState* S) {
+  cudaGraphSetConditional(h, S->done ? 0u : 1u);
+}
+
+struct pyto_batch {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::vector<const KrylovState*> S;
+};
+
+// setup: nullptr = this branch builds the coarse inverse and records *setup_done;
+// otherwise the branch waits for that event (items sharing one deflation space)
+static int batch_branch(const pyto_batch_item_t& it, const pyto_solve_cfg_t* cfg, cudaStream_t si,
+                        cudaStream_t sb, const KrylovState** S_out, cudaEvent_t setup_done, bool do_setup) {
+  const pyto_operator_t* op = it.op;
+  const pyto_deflation_t* defl = it.defl;
+  if (!op || !it.s || !it.b || !it.u || !defl_ok(defl) || !defl->bel_ptr || !defl->bel_list || defl->bel_count <= 0)
+    return PYTO_ERR_ARG;
+  if (((uintptr_t)it.b | (uintptr_t)it.u | (uintptr_t)defl->node_group) & 15) return PYTO_ERR_ARG;
+  const DeflP dp = make_deflp(op, defl);
+  int rc = gemv_smem_ok(dp.nc);
+  if (rc) return rc;
+  size_t need = 0;
+  const DpcgWs W = carve_dpcg(op, dp.nc, it.ws, it.ws_bytes, &need);
+  if (!it.ws || it.ws_bytes < need) return PYTO_ERR_WORKSPACE;
+  const int nchunks = chunk_bound(defl, si);
+  if (nchunks <= 0) return nchunks < 0 ? nchunks : PYTO_ERR_ARG;
+  if ((rc = chunk_tables(defl, W, si))) return rc;
+  if (do_setup) {
+    if ((rc = dpcg_setup_launch(op, it.s, it.mask, defl, W, nchunks, si))) return rc;
+    PYTO_CUDA(cudaEventRecord(setup_done, si));
+  } else {
+    PYTO_CUDA(cudaStreamWaitEvent(si, setup_done, 0));
+  }
+  // start of the deflated PCG (as dpcg_run)
+  const GridDims g = make_dims(op);
+  const Prec pc = make_prec(op);
+  PYTO_CUDA(cudaMemsetAsync(W.counter, 0, 64 * sizeof(unsigned), si));
+  if ((rc = pyto_jacobi(op, it.s, it.mask, W.w, W.fl, nullptr, si))) return rc;
+  k_state_init2<<<1, 1, 0, si>>>(W.S, cfg->rtol, cfg->max_iters, cfg->stop_rule);
+  PYTO_COUNT(1);
+  if ((rc = coarse_solve(g, dp, defl, it.b, W, nullptr, si))) return rc;
+  k_prolong<double><<<kNodeBlocks, kNodeThreads, 0, si>>>(g, dp, defl->node_group, defl->group_center, W.mu, W.fl,
+                                                         it.u);
+  PYTO_COUNT(1);
+  if ((rc = launch_matvec64(op, it.s, it.mask, it.u, W.q, PYTO_MASK_IN | PYTO_MASK_OUT, nullptr, nullptr, nullptr,
+                            si)))
+    return rc;
+  k_dpcg_init<double><<<kNodeBlocks, kNodeThreads, 0, si>>>(g, pc, it.b, W.q, W.w, W.fl, W.r, W.z, W.S, W.part,
+                                                           W.counter);
+  PYTO_COUNT(1);
+  if ((rc = coarse_update_K(op, g, dp, defl, it.s, (const double*)W.z, W.p, W, nchunks, W.S, 1, si))) return rc;
+  // the iteration loop: a conditional WHILE node made the capture's next dependency
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t cg = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  PYTO_CUDA(cudaStreamGetCaptureInfo(si, &cs, nullptr, &cg, &deps, &ndeps));
+  if (cs != cudaStreamCaptureStatusActive) return PYTO_ERR_CUDA;
+  cudaGraphConditionalHandle h;
+  PYTO_CUDA(cudaGraphConditionalHandleCreate(&h, cg, 1u, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams np = {};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = h;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t cnode;
+  PYTO_CUDA(cudaGraphAddNode(&cnode, cg, deps, ndeps, &np));
+  cudaGraph_t body = np.conditional.phGraph_out[0];
+  PYTO_CUDA(cudaStreamUpdateCaptureDependencies(si, &cnode, 1, cudaStreamSetCaptureDependencies));
+  PYTO_CUDA(cudaStreamBeginCaptureToGraph(sb, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+  int brc = launch_matvec64(op, it.s, it.mask, W.p, W.q, PYTO_MASK_IN | PYTO_MASK_OUT, W.part, W.counter, &W.S->pq,
+                            sb);
+  if (!brc) {
+    k_dpcg_update1<double><<<kNodeBlocks, kNodeThreads, 0, sb>>>(g, pc, W.w, W.fl, it.u, W.r, W.z, W.p, W.q, W.S,
+                                                                W.part, W.counter);
+    PYTO_COUNT(1);
+    brc = coarse_update_K(op, g, dp, defl, it.s, (const double*)W.z, W.p, W, nchunks, W.S, 0, sb);
+  }
+  if (!brc) {
+    k_while_cond<<<1, 1, 0, sb>>>(h, W.S);
+    PYTO_COUNT(1);
+    const cudaError_t el = cudaGetLastError();
+    if (el != cudaSuccess) {
+      record_error(el, "k_while_cond launch", __FILE__, __LINE__);
+      brc = PYTO_ERR_CUDA;
+    }
+  }
+  cudaGraph_t captured = nullptr;
+  const cudaError_t ec = cudaStreamEndCapture(sb, &captured);
+  if (brc) return brc;
+  if (ec != cudaSuccess) {
+    record_error(ec, "cudaStreamEndCapture(body)", __FILE__, __LINE__);
+    return PYTO_ERR_CUDA;
+  }
+  // FP64 true residual of the result
+  if ((rc = launch_matvec64(op, it.s, it.mask, it.u, W.q, PYTO_MASK_IN | PYTO_MASK_OUT, nullptr, nullptr, nullptr,
+                            si)))
+    return rc;
+  k_true_residual2<<<kNodeBlocks, kNodeThreads, 0, si>>>(g, it.b, W.q, W.fl, W.S, W.part, W.counter);
+  PYTO_COUNT(1);
+  PYTO_LAUNCH_CHECK();
+  *S_out = W.S;
+  return PYTO_OK;
+}
+
+extern "C" int pyto_batch_create(const pyto_batch_item_t* items, int n, const pyto_solve_cfg_t* cfg,
+                                 pyto_batch_t* out, void* stream) {
+  if (!items || n <= 0 || !cfg || !out) return PYTO_ERR_ARG;
+  if (!(cfg->rtol >= 0.0) || cfg->max_iters <= 0 || cfg->stop_rule < 0 || cfg->stop_rule > 1) return PYTO_ERR_ARG;
+  *out = nullptr;
+  (void)stream;  // nothing runs at creation: the capture uses a private non-blocking stream
+  cudaStream_t st = nullptr;
+  std::vector<cudaStream_t> ss(n, nullptr);
+  std::vector<cudaEvent_t> ev(2 * n + 1, nullptr);  // [0, n): joins, n: fork, (n, 2n]: set-up done
+  cudaStream_t sb = nullptr;
+  auto* B = new pyto_batch();
+  B->S.assign(n, nullptr);
+  int rc = PYTO_OK;
+  bool capturing = false;
+  auto fail = [&](int code) {
+    rc = code;
+    return code;
+  };
+  // true when the call succeeded; a failure is recorded for pyto_last_error
+  auto ok_ = [](cudaError_t e, const char* what, int line) {
+    if (e != cudaSuccess) record_error(e, what, __FILE__, line);
+    return e == cudaSuccess;
+  };
+#define PYTO_OK_(call) ok_((call), #call, __LINE__)
+  do {
+    if (!PYTO_OK_(cudaStreamCreateWithFlags(&sb, cudaStreamNonBlocking)) ||
+        !PYTO_OK_(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking))) {
+      fail(PYTO_ERR_CUDA);
+      break;
+    }
+    bool ok = true;
+    for (int i = 0; i < n && ok; ++i) ok = PYTO_OK_(cudaStreamCreateWithFlags(&ss[i], cudaStreamNonBlocking));
+    for (int i = 0; i <= 2 * n && ok; ++i)
+      ok = PYTO_OK_(cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming));
+    if (!ok) { fail(PYTO_ERR_CUDA); break; }
+    if (!PYTO_OK_(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed))) { fail(PYTO_ERR_CUDA); break; }
+    capturing = true;
+    if (!PYTO_OK_(cudaEventRecord(ev[n], st))) { fail(PYTO_ERR_CUDA); break; }
+    for (int i = 0; i < n && !rc; ++i) {
+      if (!PYTO_OK_(cudaStreamWaitEvent(ss[i], ev[n], 0))) { fail(PYTO_ERR_CUDA); break; }
+      int owner = i;  // first item with the same deflation space builds its coarse inverse
+      for (int j = 0; j < i; ++j)
+        if (items[j].defl == items[i].defl) {
+          owner = j;
+          break;
+        }
+      if (owner != i && (items[owner].op != items[i].op || items[owner].s != items[i].s ||
+                         items[owner].mask != items[i].mask)) {
+        fail(PYTO_ERR_ARG);  // a shared deflation space needs the same operator, s and mask
+        break;
+      }
+      const int r = batch_branch(items[i], cfg, ss[i], sb, &B->S[i], ev[n + 1 + owner], owner == i);
+      if (r) { fail(r); break; }
+      if (!PYTO_OK_(cudaEventRecord(ev[i], ss[i])) || !PYTO_OK_(cudaStreamWaitEvent(st, ev[i], 0))) {
+        fail(PYTO_ERR_CUDA);
+        break;
+      }
+    }
+  } while (false);
+  if (capturing) {
+    cudaGraph_t gph = nullptr;
+    const bool ended = PYTO_OK_(cudaStreamEndCapture(st, &gph));
+    if (!rc && !ended) rc = PYTO_ERR_CUDA;
+    if (!rc) {
+      B->graph = gph;
+      if (!PYTO_OK_(cudaGraphInstantiate(&B->exec, B->graph, 0))) rc = PYTO_ERR_CUDA;
+    } else if (gph) {
+      cudaGraphDestroy(gph);
+    }
+  }
+  cudaGetLastError();  // errors are reported through rc
+  for (auto e : ev)
+    if (e) cudaEventDestroy(e);
+  for (auto s2 : ss)
+    if (s2) cudaStreamDestroy(s2);
+  if (sb) cudaStreamDestroy(sb);
+  if (st) cudaStreamDestroy(st);
+  if (rc) {
+    if (B->exec) cudaGraphExecDestroy(B->exec);
+    if (B->graph) cudaGraphDestroy(B->graph);
+    delete B;
+    return rc;
+  }
+  *out = B;
+  return PYTO_OK;
+#undef PYTO_OK_
+}
+
+extern "C" int pyto_batch_launch(pyto_batch_t b, void* stream) {
+  if (!b || !b->exec) return PYTO_ERR_ARG;
+  PYTO_CUDA(cudaGraphLaunch(b->exec, (cudaStream_t)stream));
+  return PYTO_OK;
+}
+
+extern "C" int pyto_batch_status(pyto_batch_t b, pyto_solve_status_t* status, void* stream) {
+  if (!b || !status) return PYTO_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  std::vector<KrylovState> hs(b->S.size());
+  for (size_t i = 0; i < b->S.size(); ++i)
+    PYTO_CUDA(cudaMemcpyAsync(&hs[i], b->S[i], sizeof(KrylovState), cudaMemcpyDeviceToHost, st));
+  PYTO_CUDA(cudaStreamSynchronize(st));
+  int worst = PYTO_OK;
+  for (size_t i = 0; i < b->S.size(); ++i) {
+    const KrylovState& k = hs[i];
+    pyto_solve_status_t& o = status[i];
+    o.converged = k.converged;
+    o.iters = k.iters;
+    o.breakdown = k.breakdown;
+    o.reserved = 0;
+    o.rel_res = k.bb > 0 ? sqrt((k.stop_rule == 0 ? k.rr : k.rz) / (k.stop_rule == 0 ? k.bb : k.rz0)) : 0.0;
+    o.true_rel_res = k.bb > 0 ? sqrt(k.true_rr / k.bb) : 0.0;
+    if (k.breakdown) worst = PYTO_ERR_BREAKDOWN;
+    else if (!k.converged && worst == PYTO_OK) worst = PYTO_NOT_CONVERGED;
+  }
+  return worst;
+}
+
+extern "C" int pyto_batch_destroy(pyto_batch_t b) {
+  if (!b) return PYTO_OK;
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  delete b;
+  return PYTO_OK;
 }

@@ -317,7 +317,8 @@ int launch_matvec64(const pyto_operator_t* op, const double* s, const uint8_t* m
                     int mode, double* part, unsigned* counter, double* dot, cudaStream_t st) {
   const GridDims g = make_dims(op);
   const KHat kh = make_khat(op);
-  switch (g_mv_variant) {
+  const int tv = (op->tune & 0xff) - 1;  // per-grid choice of the autotuner, else the library default
+  switch (tv >= 0 && tv <= 3 ? tv : g_mv_variant) {
     case 1: return launch_mv<double, 8, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
     case 2: return launch_mv<double, 4, 3>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
     case 3: return launch_mv<double, 16, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
@@ -329,7 +330,8 @@ int launch_matvec32(const pyto_operator_t* op, const float* s, const uint8_t* ma
                     int mode, double* part, unsigned* counter, double* dot, cudaStream_t st) {
   const GridDims g = make_dims(op);
   const KHat kh = make_khat(op);
-  switch (g_mv32_variant) {
+  const int tv = ((op->tune >> 8) & 0xff) - 1;
+  switch (tv >= 0 && tv <= 3 ? tv : g_mv32_variant) {
     case 1: return launch_mv<float, 8, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
     case 2: return launch_mv<float, 4, 3>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
     case 3: return launch_mv<float, 16, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st);

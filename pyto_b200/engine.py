@@ -308,9 +308,11 @@ class DeviceDeflation:
         fixed DOF (W_f^T K z is formed from these elements only)."""
         if not self.use_boundary_lists:
             self.struct.bel_ptr = self.struct.bel_list = None
+            self.struct.bel_count = 0
             return self
         if self.mask_version == grid.mask_version:
             self.struct.bel_ptr, self.struct.bel_list = A.ptr(self.bel_ptr), A.ptr(self.bel_list)
+            self.struct.bel_count = int(self.bel_list.numel())
             return self
         mask = grid.mask[:grid.nnodes].cpu().numpy()
         fixed_el = ((mask[self._corner_nodes] & 7) != 0).any(1)
@@ -322,5 +324,64 @@ class DeviceDeflation:
         self.bel_ptr = torch.as_tensor(bptr, device=grid.device)
         self.bel_list = torch.as_tensor(elem.astype(np.int32), device=grid.device)
         self.struct.bel_ptr, self.struct.bel_list = A.ptr(self.bel_ptr), A.ptr(self.bel_list)
+        self.struct.bel_count = int(self.bel_list.numel())
         self.mask_version = grid.mask_version
         return self
+
+
+class BatchSolver:
+    """Many deflated PCG problems solved by one CUDA-graph launch (pyto_batch_*).
+
+    ``problems`` is a list of (grid, defl, s, b): a HexGrid, its DeviceDeflation, the
+    element scaling and the right-hand side.  Problems that share one DeviceDeflation
+    are load cases of one design (same grid and s): its coarse inverse is built once
+    per launch.  ``launch()`` solves all of them; rewrite the s and b tensors in place
+    and launch again for new designs and loads.  Solutions are in ``self.u``."""
+
+    def __init__(self, problems, rtol=1e-8, max_iters=5000, stop_rule=0):
+        self.problems = list(problems)
+        n = len(self.problems)
+        if n == 0:
+            raise ValueError("empty batch")
+        self.items = (A.BatchItem * n)()
+        self.u, self._ws = [], []
+        dev = None
+        for k, (grid, defl, s, b) in enumerate(self.problems):
+            dev = grid.device
+            defl.sync(grid)
+            if not defl.use_boundary_lists or defl.struct.bel_count <= 0:
+                raise ValueError("batched solves need the boundary element lists of the deflation space")
+            nb = A.ws_bytes(grid.op, A.WS_DPCG)
+            ws = torch.empty(nb, dtype=torch.uint8, device=dev)  # one workspace per problem
+            u = torch.zeros(grid.ndof, dtype=F64, device=dev)
+            self._ws.append(ws)
+            self.u.append(u)
+            self.items[k] = A.BatchItem(C.pointer(grid.op), A.ptr(s), A.ptr(grid.mask), C.pointer(defl.struct),
+                                        A.ptr(b), A.ptr(u), A.ptr(ws), nb)
+        self.device = dev
+        self.cfg = A.SolveCfg(float(rtol), int(max_iters), int(stop_rule), 1, 0)
+        self.handle = C.c_void_p()
+        A.call("pyto_batch_create", self.items, n, C.byref(self.cfg), C.byref(self.handle), A.stream_ptr(dev))
+
+    def launch(self):
+        A.call("pyto_batch_launch", self.handle, A.stream_ptr(self.device))
+        return self
+
+    def status(self):
+        n = len(self.problems)
+        st = (A.SolveStatus * n)()
+        A.call("pyto_batch_status", self.handle, st, A.stream_ptr(self.device),
+               allow=(A.OK, A.NOT_CONVERGED, A.ERR_BREAKDOWN))
+        return [SolveInfo(bool(x.converged), int(x.iters), bool(x.breakdown), float(x.rel_res),
+                          float(x.true_rel_res), 0) for x in st]
+
+    def close(self):
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            A.call("pyto_batch_destroy", self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown
+            pass

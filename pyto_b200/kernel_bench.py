@@ -9,6 +9,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import time
 
 import numpy as np
 import torch
@@ -36,7 +37,9 @@ def _timeit(fn, reps, warm=3):
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--kernel", default="matvec", choices=["matvec", "matvec32", "energy", "filter", "jacobi", "stress", "dpcg",
-                                                          "mixed", "pcg"])
+                                                          "mixed", "pcg", "batch"])
+    ap.add_argument("--designs", type=int, default=64, help="--kernel batch: number of designs")
+    ap.add_argument("--no-tune", action="store_true", help="--kernel batch: skip the autotuner")
     ap.add_argument("--groups", type=int, default=432, help="deflation groups for --kernel dpcg")
     ap.add_argument("--nel", default="192,96,96")
     ap.add_argument("--reps", type=int, default=20)
@@ -45,6 +48,8 @@ def main(argv=None):
     ap.add_argument("--variant32", type=int, default=None, help="FP32 matvec tile variant (pyto_tune)")
     ap.add_argument("--delta", type=float, default=1e-1, help="reliable-update threshold for --kernel mixed")
     a = ap.parse_args(argv)
+    if a.kernel == "batch":
+        return batch_bench(a)
     nel = tuple(int(v) for v in a.nel.split(","))
     A.call("pyto_tune", 0, a.variant)
     if a.variant32 is not None:
@@ -95,6 +100,57 @@ def main(argv=None):
         return
     print(json.dumps({"kernel": a.kernel, "variant": a.variant, "nel": nel, "ms": t * 1e3, "algorithmic_bytes": int(nbytes),
                       "GB_s": nbytes / t / 1e9}))
+
+
+def batch_bench(a):
+    """Batched workload: designs of uneven size plus one multi-load-case design, solved
+    to rel-residual 1e-8 by one CUDA-graph launch, against a loop of single solves."""
+    from .autotune import autotune
+    from .batch import batch_problems
+    from .engine import BatchSolver
+    t0 = time.perf_counter()
+    probs = batch_problems(n_designs=a.designs)
+    tune = {}
+    if not a.no_tune:
+        for g, _, _, _ in probs:
+            if g.nel not in tune:
+                tune[g.nel] = autotune(g, reps=5)
+    t_build = time.perf_counter() - t0
+    bs = BatchSolver(probs, rtol=1e-8, max_iters=5000)
+    bs.launch()
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(a.reps):
+        bs.launch()
+    e1.record(st)
+    e1.synchronize()
+    t_graph = e0.elapsed_time(e1) / 1e3 / a.reps
+    infos = bs.status()
+    # the same problems one at a time through the plain (host-polled) solver
+    for g, defl, s, b in probs[:2]:
+        g.dpcg(s, b, defl, rtol=1e-8, max_iters=5000, stop_rule=0, check_every=20)
+    torch.cuda.synchronize()
+    e0.record(st)
+    loop_iters = 0
+    for g, defl, s, b in probs:
+        _, info = g.dpcg(s, b, defl, rtol=1e-8, max_iters=5000, stop_rule=0, check_every=20)
+        loop_iters += info.iters
+    e1.record(st)
+    e1.synchronize()
+    t_loop = e0.elapsed_time(e1) / 1e3
+    n = len(probs)
+    print(json.dumps({"kernel": "batch", "problems": n, "designs": a.designs,
+                      "dofs": int(sum(g.ndof for g, _, _, _ in probs)),
+                      "graph_s": t_graph, "graph_solves_per_s": n / t_graph,
+                      "loop_s": t_loop, "loop_solves_per_s": n / t_loop, "speedup": t_loop / t_graph,
+                      "all_converged": all(i.converged for i in infos),
+                      "max_true_rel_res": max(i.true_rel_res for i in infos),
+                      "graph_iters": int(sum(i.iters for i in infos)), "loop_iters": int(loop_iters),
+                      "build_s": t_build,
+                      "tuned": {f"{k[0]}x{k[1]}x{k[2]}": {p: v[0] for p, v in r.items()} for k, r in tune.items()}}))
+    bs.close()
 
 
 if __name__ == "__main__":
