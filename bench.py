@@ -32,6 +32,10 @@ sys.path.insert(0, ROOT)
 METRIC = "time to rel-residual 1e-8 per 5.4M-DOF solve, mixed vs FP64 GPU; % HBM roofline"
 NEL = (192, 96, 96)
 RTOL = 1e-8
+# DRAM bytes (read + write) of one K(s)u launch on this grid, from an ncu capture
+# of the matvec kernel (profiles/k_matvec_192x96x96.md: cold caches, so the y writes, which
+# stay in L2 during the launch, are not counted)
+TRAFFIC = {"f32": 30750464, "f64": 71395328}
 
 
 def peaks():
@@ -143,22 +147,27 @@ def time_solves(P, form, steps, device):
     return e0.elapsed_time(e1) / 1e3 / steps, u, info
 
 
-def time_matvec(P, reps=30):
-    """Average duration of the FP64 matvec kernel on the bench grid, CUDA events
-    on the launching (current torch) stream."""
+def time_matvec(P, reps=30, precision="f64"):
+    """Average duration of the matrix-free K(s)u kernel on the bench grid (FP64 or
+    FP32), CUDA events on the launching (current torch) stream."""
     import torch
     g = P["grid"]
     s, _ = g.simp(P["rho"], 3.0, 1e-9, want_ds=False)
     u = torch.randn(g.ndof, dtype=torch.float64, device=g.device)
+    if precision == "f32":
+        s, u = s.float(), u.float()
+        fn = lambda y: g.matvec_f32(s, u, out=y)
+    else:
+        fn = lambda y: g.matvec(s, u, out=y)
     y = torch.empty_like(u)
     for _ in range(3):
-        g.matvec(s, u, out=y)
+        fn(y)
     st = torch.cuda.current_stream(g.device)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize(g.device)
     e0.record(st)
     for _ in range(reps):
-        g.matvec(s, u, out=y)
+        fn(y)
     e1.record(st)
     e1.synchronize()
     return e0.elapsed_time(e1) / reps / 1e3
@@ -311,11 +320,20 @@ def main():
     t_fp64 = t_other if other == "fp64" else value
     t_mixed = t_other if other == "mixed" else value
 
-    # roofline of the dominant kernel (FP64 matvec)
-    t_mv = time_matvec(P)
-    mv_bytes = 48 * g.nnodes + 8 * g.nelem + g.nnodes
+    # roofline of the dominant kernel: the matrix-free operator of the timed form
+    # (FP32 for the mixed solver, FP64 otherwise); algorithmic bytes per launch =
+    # u read + y write (3 values per node each) + s read + mask read
     peak, peak_kind = peaks()
-    achieved = mv_bytes / t_mv / 1e9
+    rl = {}
+    for prec, vb in (("f32", 4), ("f64", 8)):
+        t_mv = time_matvec(P, precision=prec)
+        nbytes = 2 * 3 * vb * g.nnodes + vb * g.nelem + g.nnodes
+        ach = nbytes / t_mv / 1e9
+        rl[prec] = {"bound": "hbm", "kernel": f"k_matvec<{'float' if prec == 'f32' else 'double'}> "
+                                              f"(matrix-free K(s)u)",
+                    "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak, "peak_kind": peak_kind,
+                    "traffic": TRAFFIC.get(prec), "launch_ms": t_mv * 1e3, "algorithmic_bytes": int(nbytes)}
+    main_prec = "f32" if args.form == "mixed" else "f64"
 
     if rank == 0:
         cpu = None
@@ -345,9 +363,8 @@ def main():
             "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(rho_host.numel() * 8),
                     "d2h_bytes_per_step": int(u_host.numel() * 8)},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "kernel": "k_matvec64 (FP64 matrix-free K(s)u)", "achieved": achieved,
-                         "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": None, "launch_ms": t_mv * 1e3, "algorithmic_bytes": int(mv_bytes)},
+            "roofline": rl[main_prec],
+            "roofline_other_precision": rl["f64" if main_prec == "f32" else "f32"],
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
         }

@@ -23,7 +23,8 @@ def summarise(path):
         if len(r) <= mv or r[mn] != "gpu__time_duration.sum":
             continue
         v = float(r[mv].replace(",", ""))
-        scale = {"nsecond": 1e-3, "usecond": 1.0, "msecond": 1e3, "second": 1e6}.get(r[mu], 1.0)
+        scale = {"nsecond": 1e-3, "ns": 1e-3, "usecond": 1.0, "us": 1.0, "msecond": 1e3, "ms": 1e3,
+                 "second": 1e6, "s": 1e6}[r[mu]]
         name = r[kn].split("(")[0].split("<")[0].replace("void ", "").strip()
         tot[name] += v * scale
         cnt[name] += 1
