@@ -19,6 +19,34 @@ from .problems import cantilever
 F64 = torch.float64
 
 
+def partition_by_dof(ndofs, world):
+    """Contiguous ranges [start, end) of the problems for each of `world` ranks with
+    balanced DOF totals (problems are independent: no communication between ranks).
+    Rank r takes the problems whose DOF prefix midpoint falls in its share."""
+    nd = np.asarray(ndofs, dtype=np.float64)
+    if world <= 1 or nd.size == 0:
+        return [(0, int(nd.size))] + [(int(nd.size), int(nd.size))] * max(0, world - 1)
+    mid = np.cumsum(nd) - 0.5 * nd
+    owner = np.minimum((mid / nd.sum() * world).astype(np.int64), world - 1)
+    out = []
+    for r in range(world):
+        idx = np.flatnonzero(owner == r)
+        out.append((int(idx[0]), int(idx[-1]) + 1) if idx.size else (int(np.searchsorted(owner, r)),) * 2)
+    return out
+
+
+def max_over_ranks(seconds, group=None):
+    """Slowest rank's time (the job time of independent replicas or partitions)."""
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size(group) == 1:
+        return float(seconds)
+    backend = dist.get_backend(group)
+    dev = torch.device("cuda", torch.cuda.current_device()) if backend == "nccl" else torch.device("cpu")
+    t = torch.tensor([float(seconds)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
+    return float(t.item())
+
+
 def point_load(mesh: HexMesher, rng):
     """Unit force at a random node of the x = L face, random direction."""
     ni = mesh.node_indices
@@ -46,19 +74,31 @@ def make_design(nel, rng, lo=0.01, hi=1.0, penal=3.0, emin=1e-9, group_nodes=16,
     return mesh, g, defl, s
 
 
-def batch_problems(n_designs=64, min_nx=32, max_nx=96, multi_nel=(128, 64, 64), n_loads=8, seed=0, device=None):
+def batch_shapes(n_designs=64, min_nx=32, max_nx=96, seed=0):
+    """Grid shapes of the batch's designs (nx even in [min_nx, max_nx], ny = nz = nx/2)."""
+    rng = np.random.default_rng(seed)
+    return [(nx, nx // 2, nx // 2) for nx in (int(rng.integers(min_nx // 2, max_nx // 2 + 1)) * 2
+                                              for _ in range(n_designs))]
+
+
+def batch_problems(n_designs=64, min_nx=32, max_nx=96, multi_nel=(128, 64, 64), n_loads=8, seed=0, device=None,
+                   rank=0, world=1):
     """The batched workload: n_designs cantilevers with nx drawn in [min_nx, max_nx]
     (even, ny = nz = nx / 2), one point load each, plus one multi_nel design with
-    n_loads load cases.  Returns a list of (grid, defl, s, b)."""
-    rng = np.random.default_rng(seed)
-    out = []
-    for _ in range(n_designs):
-        nx = int(rng.integers(min_nx // 2, max_nx // 2 + 1)) * 2
-        nel = (nx, nx // 2, nx // 2)
-        mesh, g, defl, s = make_design(nel, rng, device=device)
-        out.append((g, defl, s, g.tensor(point_load(mesh, rng))))
+    n_loads load cases (units of partitioning: each design, and the multi-load design
+    as a whole).  With world > 1 only this rank's contiguous, DOF-balanced share is
+    built.  Returns a list of (grid, defl, s, b)."""
+    shapes = batch_shapes(n_designs, min_nx, max_nx, seed)
+    units = [(nel, 1) for nel in shapes]
     if multi_nel is not None and n_loads > 0:
-        mesh, g, defl, s = make_design(tuple(multi_nel), rng, device=device)
-        for _ in range(n_loads):
+        units.append((tuple(multi_nel), n_loads))
+    ndof = [n * 3 * (a + 1) * (b + 1) * (c + 1) for (a, b, c), n in units]
+    lo, hi = partition_by_dof(ndof, world)[rank]
+    out = []
+    for k in range(lo, hi):
+        nel, nloads = units[k]
+        rng = np.random.default_rng((seed, k))  # per-unit stream: the same data on any rank count
+        mesh, g, defl, s = make_design(nel, rng, device=device)
+        for _ in range(nloads):
             out.append((g, defl, s, g.tensor(point_load(mesh, rng))))
     return out
