@@ -176,6 +176,11 @@ int pyto_matvec(const pyto_operator_t* op, const double* s, const uint8_t* mask,
  * assembles K in FP64 only. */
 int pyto_matvec_f32(const pyto_operator_t* op, const float* s, const uint8_t* mask, const float* u,
                     float* y, int mode, double* dot, void* ws, size_t ws_bytes, void* stream);
+/* FP32 tile variants 4 and 5 run the element contraction on the tensor cores (tcgen05,
+ * BF16 split hi/lo operands, FP32 accumulation in TMEM).  Their waits are bounded; this
+ * returns 1 if a wait ever gave up (never expected), 0 otherwise (synchronous; reset != 0
+ * clears the flag).  No reference counterpart. */
+int pyto_tensor_core_status(int reset);
 /* pyto_matvec with a non-NULL dot, for callers that cannot allocate device memory
  * (plugins whose host owns every allocation, loops where allocation is forbidden after
  * start-up).  No counterpart in the reference.  The cross-block scratch is a fixed

@@ -81,6 +81,7 @@ SIGNATURES = {
     "pyto_bc_mask": (C.c_int, [_OP, _P, C.c_int64, _P, _P]),
     "pyto_matvec": (C.c_int, [_OP, _P, _P, _P, _P, C.c_int, _P, _P, C.c_size_t, _P]),
     "pyto_matvec_f32": (C.c_int, [_OP, _P, _P, _P, _P, C.c_int, _P, _P, C.c_size_t, _P]),
+    "pyto_tensor_core_status": (C.c_int, [C.c_int]),
     "pyto_jacobi": (C.c_int, [_OP, _P, _P, _P, _P, _P, _P]),
     "pyto_matvec_dot_noalloc": (C.c_int, [_OP, _P, _P, _P, _P, C.c_int, _P, _P]),
     "pyto_pcg_solve": (C.c_int, [_OP, _P, _P, _P, _P, C.POINTER(SolveCfg), C.POINTER(SolveStatus), _P, C.c_size_t,

@@ -1,7 +1,8 @@
 """Autotuner of the matrix-free operator's tile shape, per grid.
 
 The matvec kernel has four tile variants (CTA of 32 x TY threads marching up z,
-TY in {4, 8, 16}, with 1 to 3 CTAs per SM).  Which is fastest depends on the grid
+TY in {4, 8, 16}, with 1 to 3 CTAs per SM); the FP32 operator has two more that
+run the element contraction on the tensor cores.  Which is fastest depends on the grid
 (how the (nx+1) x (ny+1) node columns divide into tiles, and the z-slab count).
 ``autotune(grid)`` times every variant with CUDA events on the grid itself, FP64
 and FP32, and stores the choice in the grid's operator (``op.tune``), which every
@@ -15,6 +16,7 @@ from . import _capi as A
 
 _CACHE: dict = {}
 VARIANTS = (0, 1, 2, 3)
+VARIANTS_F32 = (0, 1, 2, 3, 4, 5)  # 4, 5: element contraction on the tensor cores (BF16 split)
 
 
 def _time(fn, reps):
@@ -45,7 +47,7 @@ def autotune(grid, reps=10, precisions=("f64", "f32"), use_cache=True):
     saved = grid.op.tune
     for prec in precisions:
         times = {}
-        for v in VARIANTS:
+        for v in (VARIANTS if prec == "f64" else VARIANTS_F32):
             if prec == "f64":
                 grid.op.tune = (saved & ~0xFF) | (v + 1)
                 times[v] = _time(lambda: grid.matvec(s, u, out=y), reps)

@@ -2,6 +2,8 @@
 // matrix-free K(s) u (algorithm notes in matvec.cuh).
 #include <algorithm>
 
+#include <cuda_bf16.h>
+
 #include "matvec.cuh"
 
 namespace pyto {
@@ -24,14 +26,67 @@ namespace pyto {
 // Four plane slots are in flight: ez-1 (output: BC mask and u for the fused
 // dot), ez and ez+1 (compute), ez+2 (being staged).
 // ---------------------------------------------------------------------------
-template <typename T, int TY>
+template <typename T, int TY, bool TC = false>
 struct MvSmem {
   static constexpr int TX = 32, NT = TX * TY, PX = TX + 1, PY = TY + 1, PLANE = PX * PY, RING = 5;
   static constexpr size_t su = RING * 3 * PLANE;  // T
   static constexpr size_t sG = 12 * NT;           // T
   static constexpr size_t sc = 2 * 3 * TY * TX;   // T
-  static constexpr size_t bytes = sizeof(T) * (su + sG + sc) + RING * PLANE + 16;
+  static constexpr size_t base = sizeof(T) * (su + sG + sc) + RING * PLANE + 16;
+  // tensor-core element core: A tile [NT rows x 80 bf16], B tile [32 x 80 bf16], both in
+  // the K-major no-swizzle core-matrix layout (8 rows x 16 bytes per core matrix),
+  // then the mbarrier and the TMEM address
+  static constexpr size_t tc_off = (base + 127) / 128 * 128;
+  static constexpr size_t tcA = (size_t)NT * 160, tcB = 32 * 160;
+  static constexpr size_t bytes = TC ? tc_off + tcA + tcB + 16 : base;
 };
+
+// ---------------------------------------------------------------------------
+// Tensor-core element core (FP32 operator, BF16 split hi/lo on tcgen05)
+//
+// Per element layer each thread's element contributes one row of
+//   D[e, (c,m)] = sum_(d,n) V_e[(d,n)] K^[(c,m),(d,n)]
+// (V_e: the Hadamard corner coefficients of the element's u, 24 values; K^: the
+// 24x24 parity-block operator).  With x = hi(x) + lo(x) in BF16,
+// A = [V_hi | V_lo | V_hi] (80 columns with zero padding) and B = [K_hi; K_hi; K_lo]
+// give D = V_hi K_hi + V_lo K_hi + V_hi K_lo, accumulated in FP32 in TMEM by
+// tcgen05.mma (M = 128 rows per MMA, N = 32, K = 5 x 16) issued by one thread; the
+// CTA waits on an mbarrier (bounded) and each thread reads its row back with
+// tcgen05.ld.  s_e scales the result in FP32.
+// ---------------------------------------------------------------------------
+__device__ unsigned g_mv_tc_error;  // set when a tensor-core wait gave up (a bug, never expected)
+
+__device__ __forceinline__ uint64_t umma_sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  // start >> 4 (14 bits), leading / stride byte offsets >> 4, descriptor version 1,
+  // no swizzle, base offset 0
+  return (uint64_t)((addr & 0x3FFFF) >> 4) | ((uint64_t)(lbo >> 4) << 16) | ((uint64_t)(sbo >> 4) << 32) |
+         ((uint64_t)1 << 46);
+}
+// kind::f16 instruction descriptor: D FP32, A and B BF16, both K-major, N = 32, M = 128
+constexpr uint32_t kUmmaIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
+constexpr uint32_t kUmmaLbo = 128, kUmmaSbo = 1280;  // bytes: next core matrix along K / along rows
+
+// byte offset of (row, 16-byte chunk j) in a core-matrix tile of 80 bf16 columns
+__device__ __forceinline__ uint32_t umma_row_off(int row, int j) {
+  return (uint32_t)((row >> 3) * kUmmaSbo + j * kUmmaLbo + (row & 7) * 16);
+}
+
+__device__ __forceinline__ uint32_t bf2_pack(float a, float b) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+// bounded wait for the mbarrier phase `ph`; false if the bound was hit
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t mb, uint32_t ph) {
+  uint32_t done = 0;
+  for (int it = 0; it < (1 << 20) && !done; ++it)
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\tselp.b32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(done)
+        : "r"(mb), "r"(ph)
+        : "memory");
+  return done != 0;
+}
 
 // asynchronous global->shared copy of one T (4 or 8 bytes); zero-fill when !valid
 template <typename T>
@@ -47,12 +102,13 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-template <typename T, int TY, bool DOT, bool MASKIN, int MINB>
+template <typename T, int TY, bool DOT, bool MASKIN, int MINB, bool TC = false>
 __global__ void __launch_bounds__(32 * TY, MINB)
     k_matvec(GridDims g, KHat kh, const T* __restrict__ s, const uint8_t* __restrict__ mask,
              const T* __restrict__ u, T* __restrict__ y, int zc, int mode, double* part, unsigned* counter,
              double* dot_out) {
-  using M = MvSmem<T, TY>;
+  static_assert(!TC || sizeof(T) == 4, "the tensor-core element core is the FP32 operator's");
+  using M = MvSmem<T, TY, TC>;
   constexpr int TX = M::TX, NT = M::NT, PX = M::PX, PLANE = M::PLANE;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* su = reinterpret_cast<T*>(smem_raw);  // [RING][3][PLANE]
@@ -72,6 +128,62 @@ __global__ void __launch_bounds__(32 * TY, MINB)
   // node ids and DOF ids fit in int32 (checked by pyto_operator_init)
   const int pn = g.sx * g.sy;  // nodes per plane
   const int pe = g.nx * g.ny;  // elements per layer
+
+  // tensor-core element core: B tile, mbarrier, TMEM (32 columns per 128 rows)
+  constexpr int NH = TC ? NT / 128 : 1;
+  constexpr uint32_t TCOLS = 32 * NH;
+  uint32_t tc_a = 0, tc_b = 0, tc_mb = 0, tc_tm = 0, tc_ph = 0;
+  bool tc_fail = false;
+  if constexpr (TC) {
+    static_assert(NT % 128 == 0, "tensor-core tiles need 128-thread multiples");
+    unsigned char* tcp = smem_raw + M::tc_off;
+    tc_a = (uint32_t)__cvta_generic_to_shared(tcp);
+    tc_b = tc_a + (uint32_t)M::tcA;
+    tc_mb = tc_b + (uint32_t)M::tcB;
+    uint32_t* tm_slot = reinterpret_cast<uint32_t*>(tcp + M::tcA + M::tcB + 8);
+    // B rows n (outputs (c,m) = 8c+m, 24..31 zero), columns k: [K_hi | K_hi | K_lo | 0]
+    for (int i = tid; i < 32 * 10; i += NT) {
+      const int n = i / 10, j = i % 10;
+      float val[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const int k = 8 * j + e;
+        const int seg = k / 24, kk = k % 24;
+        float v = 0.f;
+        if (n < 24 && seg < 3) {
+          const int c = n >> 3, m = n & 7, d = kk >> 3, nm = kk & 7;
+          const int q = m ^ (1 << c);
+          if (m != 0 && nm != 0 && (nm ^ (1 << d)) == q) {
+            const float kf = (float)kh.b[q][3 * c + d];
+            const float hi = __bfloat162float(__float2bfloat16_rn(kf));
+            v = (seg < 2) ? hi : kf - hi;
+          }
+        }
+        val[e] = v;
+      }
+      uint4 w4;
+      w4.x = bf2_pack(val[0], val[1]);
+      w4.y = bf2_pack(val[2], val[3]);
+      w4.z = bf2_pack(val[4], val[5]);
+      w4.w = bf2_pack(val[6], val[7]);
+      *reinterpret_cast<uint4*>(tcp + M::tcA + umma_row_off(n, j)) = w4;
+    }
+    if (tid == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_mb));
+      asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    if (tid < 32) {
+      asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                       (uint32_t)__cvta_generic_to_shared(tm_slot)),
+                   "r"(TCOLS));
+      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    tc_tm = *tm_slot;
+  }
 
   // staging slots: node (tx, ty) of the (TX+1) x (TY+1) tile, plus the last
   // tile row / column for the first TX+1+TY threads
@@ -210,6 +322,88 @@ __global__ void __launch_bounds__(32 * TY, MINB)
     for (int c = 0; c < 3; ++c)
 #pragma unroll
       for (int f = 0; f < 4; ++f) Gs[c][f] = sG[(c * 4 + f) * NT + tid];
+    if constexpr (TC) {
+      // A row of this thread: [V_hi | V_lo | V_hi | 0], V[(d,n)] = Ft[d][f] +- Fb[d][f], V[(d,0)] = 0
+      float V[24];
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int nm = 0; nm < 8; ++nm) {
+          const int f = nm & 3;
+          V[8 * d + nm] = (nm == 0) ? 0.f : ((nm & 4) ? (float)(Ft[d][f] - Fb[d][f]) : (float)(Ft[d][f] + Fb[d][f]));
+        }
+      unsigned char* arow = smem_raw + M::tc_off;
+#pragma unroll
+      for (int j = 0; j < 10; ++j) {
+        float val[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          const int k = 8 * j + e, seg = k / 24, kk = k % 24;
+          float v = 0.f;
+          if (seg < 3) {
+            const float hi = __bfloat162float(__float2bfloat16_rn(V[kk]));
+            v = (seg == 1) ? V[kk] - hi : hi;
+          }
+          val[e] = v;
+        }
+        uint4 w4;
+        w4.x = bf2_pack(val[0], val[1]);
+        w4.y = bf2_pack(val[2], val[3]);
+        w4.z = bf2_pack(val[4], val[5]);
+        w4.w = bf2_pack(val[6], val[7]);
+        *reinterpret_cast<uint4*>(arow + umma_row_off(tid, j)) = w4;
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;");
+      __syncthreads();
+      if (tid == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;");
+#pragma unroll
+        for (int h = 0; h < NH; ++h)
+#pragma unroll
+          for (int ks = 0; ks < 5; ++ks) {
+            const uint64_t ad = umma_sdesc(tc_a + h * 16 * kUmmaSbo + ks * 2 * kUmmaLbo, kUmmaLbo, kUmmaSbo);
+            const uint64_t bd = umma_sdesc(tc_b + ks * 2 * kUmmaLbo, kUmmaLbo, kUmmaSbo);
+            const uint32_t acc = ks > 0 ? 1u : 0u;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+                    tc_tm + 32u * h),
+                "l"(ad), "l"(bd), "r"(kUmmaIdesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+          }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(tc_mb)
+                     : "memory");
+      }
+      if (!mbar_wait_bounded(tc_mb, tc_ph)) {
+        tc_fail = true;
+        atomicOr(&g_mv_tc_error, 1u);
+      }
+      tc_ph ^= 1u;
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      uint32_t D[32];
+      const int wq = tid >> 5;
+      const uint32_t la = tc_tm + ((uint32_t)(32 * (wq & 3)) << 16) + 32u * (uint32_t)(wq >> 2);
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,"
+          "%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+          : "=r"(D[0]), "=r"(D[1]), "=r"(D[2]), "=r"(D[3]), "=r"(D[4]), "=r"(D[5]), "=r"(D[6]), "=r"(D[7]),
+            "=r"(D[8]), "=r"(D[9]), "=r"(D[10]), "=r"(D[11]), "=r"(D[12]), "=r"(D[13]), "=r"(D[14]), "=r"(D[15]),
+            "=r"(D[16]), "=r"(D[17]), "=r"(D[18]), "=r"(D[19]), "=r"(D[20]), "=r"(D[21]), "=r"(D[22]),
+            "=r"(D[23]), "=r"(D[24]), "=r"(D[25]), "=r"(D[26]), "=r"(D[27]), "=r"(D[28]), "=r"(D[29]),
+            "=r"(D[30]), "=r"(D[31])
+          : "r"(la));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;");
+      // bottom face gets o(c,f) - o(c,f|4); the top face's pending part is o(c,f) + o(c,f|4)
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+          const T o0 = sv * (T)__uint_as_float(D[8 * c + f]), o1 = sv * (T)__uint_as_float(D[8 * c + f + 4]);
+          Gs[c][f] += o0 - o1;
+          sG[(c * 4 + f) * NT + tid] = o0 + o1;
+        }
+    } else
     // classes in pairs (qp, qp^4): after a pair, its three top-face entries are final
 #pragma unroll
     for (int qp = 0; qp < 4; ++qp) {
@@ -266,6 +460,11 @@ __global__ void __launch_bounds__(32 * TY, MINB)
   }
   cp_async_wait0();
   __syncthreads();
+  if constexpr (TC) {
+    if (tc_fail && tid == 0) (void)mbar_wait_bounded(tc_mb, tc_ph ^ 1u);  // let a late MMA finish
+    __syncthreads();
+    if (tid < 32) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tc_tm), "r"(TCOLS));
+  }
   if (Z1 - 1 >= Z0) output(Z1 - 1, r0);
   if (DOT) {
     const double bsum = block_sum<NT>(dot, sred);
@@ -275,42 +474,45 @@ __global__ void __launch_bounds__(32 * TY, MINB)
   }
 }
 
-template <typename T, int TY, bool DOT, bool MI, int MINB>
+template <typename T, int TY, bool DOT, bool MI, int MINB, bool TC = false>
 static int launch_mv_t(const MvLaunch& L, size_t smem, const GridDims& g, const KHat& kh, const T* s,
                        const uint8_t* mask, const T* u, T* y, int mode, double* part, unsigned* counter, double* dot,
                        cudaStream_t st) {
   static bool attr = false;
   if (!attr) {
-    PYTO_CUDA(cudaFuncSetAttribute(k_matvec<T, TY, DOT, MI, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    PYTO_CUDA(cudaFuncSetAttribute(k_matvec<T, TY, DOT, MI, MINB, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem));
     attr = true;
   }
-  k_matvec<T, TY, DOT, MI, MINB><<<L.grid, 32 * TY, smem, st>>>(g, kh, s, mask, u, y, L.zc, mode, part, counter, dot);
+  k_matvec<T, TY, DOT, MI, MINB, TC><<<L.grid, 32 * TY, smem, st>>>(g, kh, s, mask, u, y, L.zc, mode, part, counter,
+                                                                    dot);
   PYTO_COUNT(1);
   PYTO_LAUNCH_CHECK();
   return PYTO_OK;
 }
 
-template <typename T, int TY, int MINB>
+template <typename T, int TY, int MINB, bool TC = false>
 static int launch_mv(const GridDims& g, const KHat& kh, const T* s, const uint8_t* mask, const T* u, T* y, int mode,
                      double* part, unsigned* counter, double* dot, cudaStream_t st) {
-  const size_t smem = MvSmem<T, TY>::bytes;
+  const size_t smem = MvSmem<T, TY, TC>::bytes;
   const MvLaunch L = matvec_launch<32, TY>(g);
   const bool mi = (mode & PYTO_MASK_IN) && mask != nullptr;
   if (dot)
-    return mi ? launch_mv_t<T, TY, true, true, MINB>(L, smem, g, kh, s, mask, u, y, mode, part, counter, dot, st)
-              : launch_mv_t<T, TY, true, false, MINB>(L, smem, g, kh, s, mask, u, y, mode, part, counter, dot, st);
-  return mi ? launch_mv_t<T, TY, false, true, MINB>(L, smem, g, kh, s, mask, u, y, mode, nullptr, nullptr, nullptr,
-                                                    st)
-            : launch_mv_t<T, TY, false, false, MINB>(L, smem, g, kh, s, mask, u, y, mode, nullptr, nullptr, nullptr,
-                                                     st);
+    return mi ? launch_mv_t<T, TY, true, true, MINB, TC>(L, smem, g, kh, s, mask, u, y, mode, part, counter, dot, st)
+              : launch_mv_t<T, TY, true, false, MINB, TC>(L, smem, g, kh, s, mask, u, y, mode, part, counter, dot,
+                                                           st);
+  return mi ? launch_mv_t<T, TY, false, true, MINB, TC>(L, smem, g, kh, s, mask, u, y, mode, nullptr, nullptr,
+                                                        nullptr, st)
+            : launch_mv_t<T, TY, false, false, MINB, TC>(L, smem, g, kh, s, mask, u, y, mode, nullptr, nullptr,
+                                                         nullptr, st);
 }
 
 // Tile variant of the FP64 matvec (2 = default: fastest measured at 192x96x96):
 //   0: 32x8 threads, 2 CTAs/SM (128 registers)   1: 32x8, 1 CTA/SM (no register cap)
 //   2: 32x4, 3 CTAs/SM                            3: 32x16, 1 CTA/SM
 static int g_mv_variant = 2;
-// Tile variant of the FP32 matvec (same numbering; 0 = default)
+// Tile variant of the FP32 matvec (same numbering; 0 = default; 4 and 5: the tile
+// shapes of 0 and 2 with the element core on the tensor cores, BF16 split hi/lo)
 static int g_mv32_variant = 0;
 
 int launch_matvec64(const pyto_operator_t* op, const double* s, const uint8_t* mask, const double* u, double* y,
@@ -331,10 +533,12 @@ int launch_matvec32(const pyto_operator_t* op, const float* s, const uint8_t* ma
   const GridDims g = make_dims(op);
   const KHat kh = make_khat(op);
   const int tv = ((op->tune >> 8) & 0xff) - 1;
-  switch (tv >= 0 && tv <= 3 ? tv : g_mv32_variant) {
+  switch (tv >= 0 && tv <= 5 ? tv : g_mv32_variant) {
     case 1: return launch_mv<float, 8, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
     case 2: return launch_mv<float, 4, 3>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
     case 3: return launch_mv<float, 16, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
+    case 4: return launch_mv<float, 8, 2, true>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
+    case 5: return launch_mv<float, 4, 3, true>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
     default: return launch_mv<float, 8, 2>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
   }
 }
@@ -349,7 +553,7 @@ int set_matvec_variant(int v) {
 }
 
 int set_matvec32_variant(int v) {
-  if (v < 0 || v > 3) return PYTO_ERR_ARG;
+  if (v < 0 || v > 5) return PYTO_ERR_ARG;
   g_mv32_variant = v;
   return PYTO_OK;
 }
@@ -464,6 +668,16 @@ extern "C" int pyto_matvec(const pyto_operator_t* op, const double* s, const uin
     PYTO_CUDA(cudaMemsetAsync(counter, 0, 64 * sizeof(unsigned), (cudaStream_t)stream));
   }
   return launch_matvec64(op, s, mask, u, y, mode, part, counter, dot, (cudaStream_t)stream);
+}
+
+extern "C" int pyto_tensor_core_status(int reset) {
+  unsigned v = 0;
+  PYTO_CUDA(cudaMemcpyFromSymbol(&v, g_mv_tc_error, sizeof(v)));
+  if (reset) {
+    const unsigned z = 0;
+    PYTO_CUDA(cudaMemcpyToSymbol(g_mv_tc_error, &z, sizeof(z)));
+  }
+  return (int)v;
 }
 
 extern "C" int pyto_matvec_f32(const pyto_operator_t* op, const float* s, const uint8_t* mask, const float* u,
