@@ -129,6 +129,8 @@ long long pyto_launch_count(void);
  * Process-wide; not thread-safe against concurrent launches. */
 #define PYTO_KERNEL_MATVEC 0
 #define PYTO_KERNEL_MATVEC32 1
+#define PYTO_KERNEL_GRAPHS 2   /* variant 1 (default): deflated PCG iteration chunks replayed as
+                                  CUDA graphs; 0: launched one kernel at a time */
 int pyto_tune(int kernel, int variant);
 /* Bytes of workspace for a call of the given kind on this operator (for
  * PYTO_WS_DPCG: any coarse size up to 24576). */

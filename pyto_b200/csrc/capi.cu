@@ -17,6 +17,8 @@ int set_matvec32_variant(int v);
 namespace pyto {
 static std::atomic<long long> g_launches{0};
 void count_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+long long launch_count_now() { return g_launches.load(std::memory_order_relaxed); }
+int g_use_graphs = 1;  // Krylov iteration chunks replayed as CUDA graphs
 
 static thread_local char g_last_error[512] = "";
 void record_error(cudaError_t e, const char* what, const char* file, int line) {
@@ -32,6 +34,10 @@ extern "C" int pyto_tune(int kernel, int variant) {
   switch (kernel) {
     case PYTO_KERNEL_MATVEC: return set_matvec_variant(variant);
     case PYTO_KERNEL_MATVEC32: return set_matvec32_variant(variant);
+    case PYTO_KERNEL_GRAPHS:
+      if (variant < 0 || variant > 1) return PYTO_ERR_ARG;
+      g_use_graphs = variant;
+      return PYTO_OK;
     default: return PYTO_ERR_ARG;
   }
 }

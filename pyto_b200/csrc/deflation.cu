@@ -377,19 +377,25 @@ __global__ void __launch_bounds__(256) k_sweep_pivot(long long n, int k0, int bk
     }
   for (int p = 0; p < bk; ++p) {
     const int buf = p & 1, pa = p >> 4, pr = p & 15;
-    if (ty == pr) {
+    if (ty == pr) {  // pivot row: register row pa of the threads with ty == p mod 16
 #pragma unroll
-      for (int a = 0; a < 4; ++a)
-        if (a == pa)
+      for (int b = 0; b < 4; ++b) {
+        double v = R[0][b];
 #pragma unroll
-          for (int b = 0; b < 4; ++b) s_row[buf][tx + 16 * b] = R[a][b];
+        for (int a = 1; a < 4; ++a)
+          if (a == pa) v = R[a][b];
+        s_row[buf][tx + 16 * b] = v;
+      }
     }
-    if (tx == pr) {
+    if (tx == pr) {  // pivot column
 #pragma unroll
-      for (int b = 0; b < 4; ++b)
-        if (b == pa)
+      for (int a = 0; a < 4; ++a) {
+        double v = R[a][0];
 #pragma unroll
-          for (int a = 0; a < 4; ++a) s_col[buf][ty + 16 * a] = R[a][b];
+        for (int b = 1; b < 4; ++b)
+          if (b == pa) v = R[a][b];
+        s_col[buf][ty + 16 * a] = v;
+      }
     }
     __syncthreads();
     const double ipiv = 1.0 / s_row[buf][p];
@@ -398,16 +404,35 @@ __global__ void __launch_bounds__(256) k_sweep_pivot(long long n, int k0, int bk
     for (int b = 0; b < 4; ++b) rv[b] = s_row[buf][tx + 16 * b] * ipiv;
 #pragma unroll
     for (int a = 0; a < 4; ++a) cv[a] = s_col[buf][ty + 16 * a];
+    // every entry: M_ij - M_ip M_pj / M_pp; then the owners of the pivot row and
+    // column replace theirs: M_pj / M_pp, M_ip / M_pp, and -1 / M_pp on the diagonal
 #pragma unroll
     for (int a = 0; a < 4; ++a)
 #pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        const bool ip = (ty + 16 * a == p), jp = (tx + 16 * b == p);
-        if (ip && jp) R[a][b] = -ipiv;
-        else if (ip) R[a][b] = rv[b];
-        else if (jp) R[a][b] = cv[a] * ipiv;
-        else R[a][b] = fma(-cv[a], rv[b], R[a][b]);
+      for (int b = 0; b < 4; ++b) R[a][b] = fma(-cv[a], rv[b], R[a][b]);
+    if (ty == pr) {
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+        if (a == pa)
+#pragma unroll
+          for (int b = 0; b < 4; ++b) R[a][b] = rv[b];
+    }
+    if (tx == pr) {
+#pragma unroll
+      for (int b = 0; b < 4; ++b)
+        if (b == pa)
+#pragma unroll
+          for (int a = 0; a < 4; ++a) R[a][b] = cv[a] * ipiv;
+      if (ty == pr) {
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+          if (a == pa) {
+#pragma unroll
+            for (int b = 0; b < 4; ++b)
+              if (b == pa) R[a][b] = -ipiv;
+          }
       }
+    }
   }
 #pragma unroll
   for (int a = 0; a < 4; ++a)
@@ -1318,6 +1343,66 @@ extern "C" int pyto_dpcg_setup(const pyto_operator_t* op, const double* s, const
 
 namespace pyto {
 
+// ---------------------------------------------------------------------------
+// A chunk of Krylov iterations (the kernels between two host polls) captured
+// once per solve on a private stream and replayed as one CUDA graph: removes
+// the gaps between the ~5 launches of every iteration.  The kernels of a
+// converged state return at once, so a replay past convergence is harmless.
+// Launches are counted per replay.
+// ---------------------------------------------------------------------------
+long long launch_count_now();
+extern int g_use_graphs;
+
+struct ChunkGraph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  long long per_replay = 0;
+  ChunkGraph() = default;
+  ChunkGraph(const ChunkGraph&) = delete;
+  ChunkGraph& operator=(const ChunkGraph&) = delete;
+  ~ChunkGraph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+  }
+  // body(stream) issues the chunk's launches and returns a status
+  template <typename F>
+  int build(F&& body) {
+    cudaStream_t cs = nullptr;
+    PYTO_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    const long long n0 = launch_count_now();
+    int rc = PYTO_OK;
+    const cudaError_t eb = cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed);
+    if (eb != cudaSuccess) {
+      record_error(eb, "cudaStreamBeginCapture(chunk)", __FILE__, __LINE__);
+      rc = PYTO_ERR_CUDA;
+    } else {
+      rc = body(cs);
+      const cudaError_t ee = cudaStreamEndCapture(cs, &graph);
+      if (!rc && ee != cudaSuccess) {
+        record_error(ee, "cudaStreamEndCapture(chunk)", __FILE__, __LINE__);
+        rc = PYTO_ERR_CUDA;
+      }
+      if (!rc) {
+        const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+        if (ei != cudaSuccess) {
+          record_error(ei, "cudaGraphInstantiate(chunk)", __FILE__, __LINE__);
+          rc = PYTO_ERR_CUDA;
+        }
+      }
+    }
+    per_replay = launch_count_now() - n0;
+    count_launches(-per_replay);  // counted when replayed
+    cudaGetLastError();
+    cudaStreamDestroy(cs);
+    return rc;
+  }
+  int launch(cudaStream_t st) {
+    PYTO_CUDA(cudaGraphLaunch(exec, st));
+    count_launches(per_replay);
+    return PYTO_OK;
+  }
+};
+
 template <typename T>
 struct DVec {
   T *r, *p, *q, *z;
@@ -1372,23 +1457,31 @@ static int dpcg_run(const pyto_operator_t* op, const T* s, const uint8_t* mask, 
   PYTO_LAUNCH_CHECK();
   PYTO_CUDA(cudaMemcpyAsync(hs, W.S, sizeof(*hs), cudaMemcpyDeviceToHost, st));
   PYTO_CUDA(cudaStreamSynchronize(st));
-  while (!hs->done && hs->iters < max_iters) {
+  auto chunk = [&](cudaStream_t cs) -> int {
+    int e;
     for (int k = 0; k < every; ++k) {
-      if ((rc = matvec_t(op, s, mask, V.p, V.q, W.part, W.counter, &W.S->pq, st))) return rc;
-      k_dpcg_update1<T><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, pc, W.w, W.fl, u, V.r, V.z, V.p, V.q, W.S, W.part,
+      if ((e = matvec_t(op, s, mask, V.p, V.q, W.part, W.counter, &W.S->pq, cs))) return e;
+      k_dpcg_update1<T><<<kNodeBlocks, kNodeThreads, 0, cs>>>(g, pc, W.w, W.fl, u, V.r, V.z, V.p, V.q, W.S, W.part,
                                                               W.counter);
       PYTO_COUNT(1);
       // mu = Einv W^T K z (from the boundary lists, or K z -> q then W^T q), p = z + beta p - W mu
       if (lists) {
-        if ((rc = coarse_update_K(op, g, dp, defl, s, V.z, V.p, W, nchunks, W.S, 0, st))) return rc;
+        if ((e = coarse_update_K(op, g, dp, defl, s, V.z, V.p, W, nchunks, W.S, 0, cs))) return e;
       } else {
-        if ((rc = matvec_t(op, s, mask, V.z, V.q, nullptr, nullptr, nullptr, st))) return rc;
-        if ((rc = coarse_solve(g, dp, defl, V.q, W, W.S, st))) return rc;
-        k_dpcg_update2<T><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center, W.mu,
+        if ((e = matvec_t(op, s, mask, V.z, V.q, nullptr, nullptr, nullptr, cs))) return e;
+        if ((e = coarse_solve(g, dp, defl, V.q, W, W.S, cs))) return e;
+        k_dpcg_update2<T><<<kNodeBlocks, kNodeThreads, 0, cs>>>(g, dp, defl->node_group, defl->group_center, W.mu,
                                                                 W.fl, V.z, V.p, W.S, 0);
         PYTO_COUNT(1);
       }
     }
+    PYTO_LAUNCH_CHECK();
+    return PYTO_OK;
+  };
+  ChunkGraph cg;
+  if (g_use_graphs && !hs->done && (rc = cg.build(chunk))) return rc;
+  while (!hs->done && hs->iters < max_iters) {
+    if ((rc = g_use_graphs ? cg.launch(st) : chunk(st))) return rc;
     PYTO_LAUNCH_CHECK();
     PYTO_CUDA(cudaMemcpyAsync(hs, W.S, sizeof(*hs), cudaMemcpyDeviceToHost, st));
     PYTO_CUDA(cudaStreamSynchronize(st));
@@ -1615,22 +1708,30 @@ static int dpcg_reliable(const pyto_operator_t* op, const double* s, const uint8
   double true_prev = hs.true_rr;  // true ||r||^2 at the previous update
   int updates = 1, restarts = 0, seg0 = 0;
   const double d2 = delta * delta;
-  while (!hs.converged && hs.iters < cfg->max_iters) {
+  auto chunk = [&](cudaStream_t cs) -> int {
+    int e;
     for (int k = 0; k < every; ++k) {
-      if ((rc = matvec_t(op, sT, mask, p, q, W.part, W.counter, &W.S->pq, st))) return rc;
-      k_dpcg_update1<T><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, pc, W.w, W.fl, x, r, z, p, q, W.S, W.part,
+      if ((e = matvec_t(op, sT, mask, p, q, W.part, W.counter, &W.S->pq, cs))) return e;
+      k_dpcg_update1<T><<<kNodeBlocks, kNodeThreads, 0, cs>>>(g, pc, W.w, W.fl, x, r, z, p, q, W.S, W.part,
                                                               W.counter);
       PYTO_COUNT(1);
       if (lists) {
-        if ((rc = coarse_update_K(op, g, dp, defl, sT, (const T*)z, p, W, nchunks, W.S, 0, st))) return rc;
+        if ((e = coarse_update_K(op, g, dp, defl, sT, (const T*)z, p, W, nchunks, W.S, 0, cs))) return e;
       } else {
-        if ((rc = matvec_t(op, sT, mask, z, q, nullptr, nullptr, nullptr, st))) return rc;
-        if ((rc = coarse_solve(g, dp, defl, (const T*)q, W, W.S, st))) return rc;
-        k_dpcg_update2<T><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center, W.mu,
+        if ((e = matvec_t(op, sT, mask, z, q, nullptr, nullptr, nullptr, cs))) return e;
+        if ((e = coarse_solve(g, dp, defl, (const T*)q, W, W.S, cs))) return e;
+        k_dpcg_update2<T><<<kNodeBlocks, kNodeThreads, 0, cs>>>(g, dp, defl->node_group, defl->group_center, W.mu,
                                                                 W.fl, z, p, W.S, 0);
         PYTO_COUNT(1);
       }
     }
+    PYTO_LAUNCH_CHECK();
+    return PYTO_OK;
+  };
+  ChunkGraph cg;
+  if (g_use_graphs && !hs.converged && (rc = cg.build(chunk))) return rc;
+  while (!hs.converged && hs.iters < cfg->max_iters) {
+    if ((rc = g_use_graphs ? cg.launch(st) : chunk(st))) return rc;
     PYTO_LAUNCH_CHECK();
     PYTO_CUDA(cudaMemcpyAsync(&hs, W.S, sizeof(hs), cudaMemcpyDeviceToHost, st));
     PYTO_CUDA(cudaStreamSynchronize(st));

@@ -125,6 +125,22 @@ def test_oc_history_matches_reference():
     np.testing.assert_allclose(hist["objective"][10], d["objective"][10], rtol=1e-8)
 
 
+def test_cfg1_oc_history_matches_reference():
+    """Config 1: 60x30x30 cantilever, rho = 0.3, Jacobi PCG to 1e-8, sensitivity filter
+    r = 1.5, volfrac 0.3, move 0.2: the 10-iteration OC objective history and the
+    post-loop solve against the reference's own run (PCG tolerance 1e-8 on both sides,
+    so the histories agree to the solver accuracy)."""
+    from pyto_b200 import topopt_common as tc, topopt_ocm
+    d = golden("cfg1_oc10.npz")
+    m, fe = _setup(nel=(60, 30, 30), solver_name="PCG", rtol=1e-8)
+    params = tc.TOParams(Constraints=[(tc.TO_QOI.VOLUME_FRACTION, None, 0.3)], RelativeFilterRadius=1.5)
+    sol, hist, ok, msg, n = topopt_ocm.topopt_optimality_criteria(
+        tc.FEA_MODE.STRUCTURAL, fe, params, maxIterations=10, plot_progress=False, print_progress=False,
+        binarize_topology=False)
+    np.testing.assert_allclose(hist["objective"][:11], d["objective"][:11], rtol=1e-6)
+    np.testing.assert_allclose(hist["volfrac"][:10], d["volfrac"][:10], rtol=1e-7)
+
+
 def test_nonzero_dirichlet_values():
     """Prescribed displacements are lifted into the right-hand side (src/bound_cond.py:58-60)."""
     import oracle as O
