@@ -67,38 +67,84 @@ __device__ __forceinline__ double hat_energy(const KHat& kh, const double (&U)[3
   return e;
 }
 
+// Element energies by element columns: thread (ex, ey) of a 32 x 8 CTA marches up
+// a slab of kEnSlab element layers, keeping the face transform of the top face of
+// layer z as the bottom face of layer z+1, so each layer reads one node face (its
+// corners are shared with the neighbouring columns through L1) and u, v reach
+// DRAM once.  SAME: v == u.
+constexpr int kEnSlab = 16;
+
+__device__ __forceinline__ void load_face(const GridDims& g, const double* __restrict__ u, int ex, int ey, int z,
+                                          double (&F)[3][4]) {
+  const long long n00 = ex + (long long)g.sx * (ey + (long long)g.sy * z);
+  const long long n01 = n00 + g.sx;
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+    face_fwd(__ldg(u + 3 * n00 + c), __ldg(u + 3 * (n00 + 1) + c), __ldg(u + 3 * n01 + c),
+             __ldg(u + 3 * (n01 + 1) + c), F[c]);
+}
+
+template <bool SAME>
 __global__ void __launch_bounds__(kElemThreads) k_elem_energy(GridDims g, KHat kh, const double* __restrict__ u,
                                                               const double* __restrict__ v,
                                                               const double* __restrict__ s, double* __restrict__ ce,
                                                               double* part, unsigned* counter, double* total) {
   __shared__ double sred[kElemThreads / 32];
+  const int ex = blockIdx.x * 32 + (threadIdx.x & 31), ey = blockIdx.y * 8 + (threadIdx.x >> 5);
+  const int z0 = blockIdx.z * kEnSlab, z1 = min(z0 + kEnSlab, g.nz);
   double acc = 0.0;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < g.nelem;
-       e += (long long)gridDim.x * blockDim.x) {
-    int ex, ey, ez;
-    elem_coords(g, e, ex, ey, ez);
-    double a[3][8], U[3][8], V[3][8];
-    gather_elem(g, u, ex, ey, ez, a);
+  if (ex < g.nx && ey < g.ny) {
+    double Ub[3][4], Vb[3][4];
+    load_face(g, u, ex, ey, z0, Ub);
+    if (!SAME) load_face(g, v, ex, ey, z0, Vb);
+    for (int ez = z0; ez < z1; ++ez) {
+      double Ut[3][4], Vt[3][4];
+      load_face(g, u, ex, ey, ez + 1, Ut);
+      if (!SAME) load_face(g, v, ex, ey, ez + 1, Vt);
+      // u^ . (K^ v^) over the parity classes; mode m = f (+) or f|4 (-): Ft +- Fb
+      double en = 0.0;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) elem_fwd(a[c], U[c]);
-    if (v != u) {
-      gather_elem(g, v, ex, ey, ez, a);
+      for (int q = 0; q < 8; ++q) {
 #pragma unroll
-      for (int c = 0; c < 3; ++c) elem_fwd(a[c], V[c]);
-    } else {
+        for (int c = 0; c < 3; ++c) {
+          const int m = member_mode(q, c);
+          if (m == 0) continue;
+          double kv = 0.0;
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            const int nm = member_mode(q, d);
+            if (nm == 0) continue;
+            const int f = nm & 3;
+            const double vh = SAME ? ((nm & 4) ? Ut[d][f] - Ub[d][f] : Ut[d][f] + Ub[d][f])
+                                   : ((nm & 4) ? Vt[d][f] - Vb[d][f] : Vt[d][f] + Vb[d][f]);
+            kv = fma(kh.b[q][3 * c + d], vh, kv);
+          }
+          const int f = m & 3;
+          const double uh = (m & 4) ? Ut[c][f] - Ub[c][f] : Ut[c][f] + Ub[c][f];
+          en = fma(uh, kv, en);
+        }
+      }
+      const long long e = ex + (long long)g.nx * (ey + (long long)g.ny * ez);
+      if (ce) ce[e] = en;
+      if (total) acc = fma(__ldg(s + e), en, acc);
 #pragma unroll
       for (int c = 0; c < 3; ++c)
 #pragma unroll
-        for (int m = 0; m < 8; ++m) V[c][m] = U[c][m];
+        for (int f = 0; f < 4; ++f) {
+          Ub[c][f] = Ut[c][f];
+          if (!SAME) Vb[c][f] = Vt[c][f];
+        }
     }
-    const double en = hat_energy(kh, U, V);
-    if (ce) ce[e] = en;
-    if (total) acc = fma(s[e], en, acc);
   }
   if (total) {
     double val[1] = {block_sum<kElemThreads>(acc, sred)};
-    grid_reduce<1>(val, part, counter, gridDim.x, [&](const double* t) { *total = t[0]; });
+    grid_reduce<1>(val, part, counter, (int)(gridDim.x * gridDim.y * gridDim.z),
+                   [&](const double* t) { *total = t[0]; });
   }
+}
+
+static dim3 energy_grid(const GridDims& g) {
+  return dim3((g.nx + 31) / 32, (g.ny + 7) / 8, (g.nz + kEnSlab - 1) / kEnSlab);
 }
 
 struct StressP {
@@ -289,15 +335,19 @@ extern "C" int pyto_elem_energy(const pyto_operator_t* op, const double* u, cons
   cudaStream_t st = (cudaStream_t)stream;
   double* part = nullptr;
   unsigned* counter = nullptr;
-  const int nb = elem_blocks(g.nelem);
+  const dim3 eg = energy_grid(g);
+  const long long nb = (long long)eg.x * eg.y * eg.z;
   if (total) {
     Carver cv{(char*)ws, 0, ws_bytes};
     counter = cv.take<unsigned>(64);
-    part = cv.take<double>(nb);
+    part = cv.take<double>((size_t)nb);
     if (!cv.ok()) return PYTO_ERR_WORKSPACE;
     PYTO_CUDA(cudaMemsetAsync(counter, 0, 64 * sizeof(unsigned), st));
   }
-  k_elem_energy<<<nb, kElemThreads, 0, st>>>(g, make_khat(op), u, v, s, ce, part, counter, total);
+  if (u == v)
+    k_elem_energy<true><<<eg, kElemThreads, 0, st>>>(g, make_khat(op), u, v, s, ce, part, counter, total);
+  else
+    k_elem_energy<false><<<eg, kElemThreads, 0, st>>>(g, make_khat(op), u, v, s, ce, part, counter, total);
   PYTO_COUNT(1);
   PYTO_LAUNCH_CHECK();
   return PYTO_OK;

@@ -5,6 +5,7 @@
 // at most (2R+1)^3 taps and Hs_i (row sum) is the sum of the in-bounds taps.
 // The tap list is built on the host and passed as a kernel argument.
 #include <math.h>
+#include <stdlib.h>
 
 #include <algorithm>
 
@@ -44,39 +45,113 @@ static int make_taps(const pyto_operator_t* op, double rel, Taps* t) {
   return PYTO_OK;
 }
 
+// Tiled stencil: a CTA produces a kFx x kFy x kFz block of outputs (256 threads,
+// one (x, y) column each, marching over kFz planes) from a shared-memory copy of
+// the block plus an R-element halo: v = the filtered quantity (0 outside the grid
+// or on inactive elements) and m = 1 where a tap counts (in the grid and active).
+// Tap offsets into the tile are precomputed on the host.  Blocks whose halo lies
+// inside the grid, without an active mask, take the row sum from the host (the
+// sum of all weights) and skip m.
+constexpr int kFx = 32, kFy = 8, kFz = 8;
+
+struct TileTaps {
+  int n, R;
+  double wsum;
+  int off[kMaxTaps];
+  double w[kMaxTaps];
+};
+
+static void tile_taps(const Taps& t, int R, TileTaps* tt) {
+  const int PX = kFx + 2 * R, PY = kFy + 2 * R;
+  tt->n = t.n;
+  tt->R = R;
+  tt->wsum = 0.0;
+  for (int k = 0; k < t.n; ++k) {
+    tt->off[k] = (t.dz[k] * PY + t.dy[k]) * PX + t.dx[k];
+    tt->w[k] = t.w[k];
+    tt->wsum += t.w[k];
+  }
+}
+
 template <int MODE>
-__global__ void __launch_bounds__(256) k_filter(GridDims g, Taps t, const double* __restrict__ x,
+__global__ void __launch_bounds__(256) k_filter(GridDims g, TileTaps t, const double* __restrict__ x,
                                                 const double* __restrict__ wv, const double* __restrict__ hs,
                                                 const uint8_t* __restrict__ active, double* __restrict__ y) {
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < g.nelem;
-       e += (long long)gridDim.x * blockDim.x) {
-    const int ex = (int)(e % g.nx);
-    const long long rr = e / g.nx;
-    const int ey = (int)(rr % g.ny);
-    const int ez = (int)(rr / g.ny);
+  extern __shared__ double fsm[];
+  const int R = t.R;
+  const int PX = kFx + 2 * R, PY = kFy + 2 * R, PZ = kFz + 2 * R;
+  const int tile = PX * PY * PZ;
+  double* sv = fsm;                                  // [PZ][PY][PX] values
+  float* sm = reinterpret_cast<float*>(fsm + tile);  // [PZ][PY][PX] tap masks
+  const int X0 = blockIdx.x * kFx, Y0 = blockIdx.y * kFy, Z0 = blockIdx.z * kFz;
+  const bool interior = !active && X0 - R >= 0 && Y0 - R >= 0 && Z0 - R >= 0 && X0 + kFx + R <= g.nx &&
+                        Y0 + kFy + R <= g.ny && Z0 + kFz + R <= g.nz;
+  for (int q = threadIdx.x; q < tile; q += blockDim.x) {
+    const int lx = q % PX, r2 = q / PX, ly = r2 % PY, lz = r2 / PY;
+    const int gx = X0 - R + lx, gy = Y0 - R + ly, gz = Z0 - R + lz;
+    double v = 0.0;
+    float m = 0.f;
+    if (gx >= 0 && gx < g.nx && gy >= 0 && gy < g.ny && gz >= 0 && gz < g.nz) {
+      const long long j = gx + (long long)g.nx * (gy + (long long)g.ny * gz);
+      if (!active || active[j]) {
+        m = 1.f;
+        if (MODE == PYTO_FILTER_RAW || MODE == PYTO_FILTER_DENSITY) v = __ldg(x + j);
+        if (MODE == PYTO_FILTER_CHAIN) v = __ldg(x + j) / __ldg(hs + j);
+        if (MODE == PYTO_FILTER_SENS) v = __ldg(wv + j) * __ldg(x + j);
+      }
+    }
+    sv[q] = v;
+    sm[q] = m;
+  }
+  __syncthreads();
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int ex = X0 + tx, ey = Y0 + ty;
+  if (ex >= g.nx || ey >= g.ny) return;
+  for (int z = 0; z < kFz && Z0 + z < g.nz; ++z) {
+    const long long e = ex + (long long)g.nx * (ey + (long long)g.ny * (Z0 + z));
     if (active && !active[e]) {
       y[e] = 0.0;
       continue;
     }
+    const int c = ((z + R) * PY + (ty + R)) * PX + (tx + R);
     double acc = 0.0, ws = 0.0;
-    for (int k = 0; k < t.n; ++k) {
-      const int jx = ex + t.dx[k], jy = ey + t.dy[k], jz = ez + t.dz[k];
-      if (jx < 0 || jx >= g.nx || jy < 0 || jy >= g.ny || jz < 0 || jz >= g.nz) continue;
-      const long long j = jx + (long long)g.nx * (jy + (long long)g.ny * jz);
-      if (active && !active[j]) continue;
-      const double w = t.w[k];
-      ws += w;
-      if (MODE == PYTO_FILTER_RAW || MODE == PYTO_FILTER_DENSITY) acc = fma(w, __ldg(x + j), acc);
-      if (MODE == PYTO_FILTER_CHAIN) acc = fma(w, __ldg(x + j) / __ldg(hs + j), acc);
-      if (MODE == PYTO_FILTER_SENS) acc = fma(w, __ldg(wv + j) * __ldg(x + j), acc);
+    if (interior) {
+      for (int k = 0; k < t.n; ++k) acc = fma(t.w[k], sv[c + t.off[k]], acc);
+      ws = t.wsum;
+    } else {
+      for (int k = 0; k < t.n; ++k) {
+        const double w = t.w[k];
+        acc = fma(w, sv[c + t.off[k]], acc);
+        ws = fma(w, (double)sm[c + t.off[k]], ws);
+      }
     }
     double out;
     if (MODE == PYTO_FILTER_RAW || MODE == PYTO_FILTER_CHAIN) out = acc;
     else if (MODE == PYTO_FILTER_DENSITY) out = acc / ws;
-    else if (MODE == PYTO_FILTER_SENS) out = acc / ws / wv[e];
+    else if (MODE == PYTO_FILTER_SENS) out = acc / ws / __ldg(wv + e);
     else out = ws;
     y[e] = out;
   }
+}
+
+static size_t filter_smem(int R) {
+  const size_t tile = (size_t)(kFx + 2 * R) * (kFy + 2 * R) * (kFz + 2 * R);
+  return tile * (sizeof(double) + sizeof(float));
+}
+
+template <int MODE>
+static int launch_filter(const GridDims& g, const TileTaps& tt, const double* x, const double* w, const double* hs,
+                         const uint8_t* active, double* y, cudaStream_t st) {
+  static bool attr = false;
+  if (!attr) {
+    PYTO_CUDA(cudaFuncSetAttribute(k_filter<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)filter_smem(3)));
+    attr = true;
+  }
+  const dim3 grid((g.nx + kFx - 1) / kFx, (g.ny + kFy - 1) / kFy, (g.nz + kFz - 1) / kFz);
+  k_filter<MODE><<<grid, 256, filter_smem(tt.R), st>>>(g, tt, x, w, hs, active, y);
+  PYTO_COUNT(1);
+  PYTO_LAUNCH_CHECK();
+  return PYTO_OK;
 }
 
 }  // namespace pyto
@@ -93,18 +168,18 @@ extern "C" int pyto_filter(const pyto_operator_t* op, double rel_radius, int mod
   Taps t;
   int rc = make_taps(op, rel_radius, &t);
   if (rc) return rc;
+  int R = 0;
+  for (int k = 0; k < t.n; ++k) R = std::max(R, std::max(abs(t.dx[k]), std::max(abs(t.dy[k]), abs(t.dz[k]))));
+  TileTaps tt;
+  tile_taps(t, R, &tt);
   const GridDims g = make_dims(op);
   cudaStream_t st = (cudaStream_t)stream;
-  const int nb = (int)std::min<long long>((g.nelem + 255) / 256, 8 * kNumSMs);
   switch (mode) {
-    case PYTO_FILTER_RAW: k_filter<PYTO_FILTER_RAW><<<nb, 256, 0, st>>>(g, t, x, w, hs, active, y); break;
-    case PYTO_FILTER_DENSITY: k_filter<PYTO_FILTER_DENSITY><<<nb, 256, 0, st>>>(g, t, x, w, hs, active, y); break;
-    case PYTO_FILTER_CHAIN: k_filter<PYTO_FILTER_CHAIN><<<nb, 256, 0, st>>>(g, t, x, w, hs, active, y); break;
-    case PYTO_FILTER_SENS: k_filter<PYTO_FILTER_SENS><<<nb, 256, 0, st>>>(g, t, x, w, hs, active, y); break;
-    case PYTO_FILTER_HS: k_filter<PYTO_FILTER_HS><<<nb, 256, 0, st>>>(g, t, x, w, hs, active, y); break;
+    case PYTO_FILTER_RAW: return launch_filter<PYTO_FILTER_RAW>(g, tt, x, w, hs, active, y, st);
+    case PYTO_FILTER_DENSITY: return launch_filter<PYTO_FILTER_DENSITY>(g, tt, x, w, hs, active, y, st);
+    case PYTO_FILTER_CHAIN: return launch_filter<PYTO_FILTER_CHAIN>(g, tt, x, w, hs, active, y, st);
+    case PYTO_FILTER_SENS: return launch_filter<PYTO_FILTER_SENS>(g, tt, x, w, hs, active, y, st);
+    case PYTO_FILTER_HS: return launch_filter<PYTO_FILTER_HS>(g, tt, x, w, hs, active, y, st);
     default: return PYTO_ERR_ARG;
   }
-  PYTO_COUNT(1);
-  PYTO_LAUNCH_CHECK();
-  return PYTO_OK;
 }

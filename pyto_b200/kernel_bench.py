@@ -37,7 +37,9 @@ def _timeit(fn, reps, warm=3):
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--kernel", default="matvec", choices=["matvec", "matvec32", "energy", "filter", "jacobi", "stress", "dpcg",
-                                                          "mixed", "pcg", "batch"])
+                                                          "mixed", "pcg", "batch", "oc"])
+    ap.add_argument("--iters", type=int, default=20, help="--kernel oc: OC iterations")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"], help="--kernel oc: DPCG form")
     ap.add_argument("--designs", type=int, default=64, help="--kernel batch: number of designs")
     ap.add_argument("--no-tune", action="store_true", help="--kernel batch: skip the autotuner")
     ap.add_argument("--groups", type=int, default=432, help="deflation groups for --kernel dpcg")
@@ -50,6 +52,8 @@ def main(argv=None):
     a = ap.parse_args(argv)
     if a.kernel == "batch":
         return batch_bench(a)
+    if a.kernel == "oc":
+        return oc_bench(a)
     nel = tuple(int(v) for v in a.nel.split(","))
     A.call("pyto_tune", 0, a.variant)
     if a.variant32 is not None:
@@ -100,6 +104,40 @@ def main(argv=None):
         return
     print(json.dumps({"kernel": a.kernel, "variant": a.variant, "nel": nel, "ms": t * 1e3, "algorithmic_bytes": int(nbytes),
                       "GB_s": nbytes / t / 1e9}))
+
+
+def oc_bench(a):
+    """OC topology optimisation through the reference-named driver (topopt_ocm) on the
+    cantilever: rho0 = volfrac, sensitivity filter r = 1.5, volfrac 0.3, move 0.2, each
+    FEA solve by the deflated PCG (432 node-box groups x 6 modes, rtol 1e-8)."""
+    from . import bound_cond, hex_structural_fea, linear_solvers, mat_lib, topopt_common as tc, topopt_ocm
+    from . import topopt_material_model as tmm
+    from .deflation import DeflationSolver
+    tmm._EVOID_RELATIVE = 1e-9
+    nel = tuple(int(v) for v in a.nel.split(","))
+    mesh = HexMesher()
+    mesh.grid_mesh(nel, (1.0, 1.0, 1.0))
+    f, fixed = cantilever(mesh)
+    bc = bound_cond.BC(force=f, fixed_dofs=fixed, dirichlet_values=np.zeros(len(fixed)))
+    mat = mat_lib.create_material_with_defaults("unit", youngs_modulus=1.0, poissons_ratio=0.3)
+    ds = DeflationSolver(modes=6, shift=1e-14, shift_relative=True)
+    ds.create_deflation_groups(mesh, a.groups)
+    fe = hex_structural_fea.HexStructuralFEA(mesh=mesh, mat_prop=mat, bc=bc, solver=linear_solvers.Solvers.DPCG,
+                                             dsolver=ds, rtol=1e-8, precision=a.precision)
+    params = tc.TOParams(Constraints=[(tc.TO_QOI.VOLUME_FRACTION, None, 0.3)], RelativeFilterRadius=1.5)
+    run = lambda n: topopt_ocm.topopt_optimality_criteria(tc.FEA_MODE.STRUCTURAL, fe, params, maxIterations=n,
+                                                          plot_progress=False, print_progress=False,
+                                                          binarize_topology=False)
+    run(1)  # warm-up: library load, workspaces
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sol, hist, ok, msg, nfea = run(a.iters)
+    torch.cuda.synchronize()
+    t = time.perf_counter() - t0
+    obj = [float(v) for v in hist["objective"]]
+    print(json.dumps({"kernel": "oc", "precision": a.precision, "nel": nel, "iterations": a.iters, "fea_solves": int(nfea), "s": t,
+                      "ms_per_iteration": 1e3 * t / max(1, nfea), "objective_first": obj[0],
+                      "objective_last": obj[-1], "volfrac_last": float(hist["volfrac"][-1])}))
 
 
 def batch_bench(a):

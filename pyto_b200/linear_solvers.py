@@ -94,8 +94,16 @@ def solve(A0, b0, solver: Solvers, bc, **kwargs):
     elif solver == Solvers.DPCG:
         dsolver = kwargs["dsolver"]
         dd = dsolver.device_deflation(g)
-        u, info = g.dpcg(A0.s, b, dd, rtol=rtol, max_iters=kwargs.get("maxIters", 2000),
-                         stop_rule=kwargs.get("stop_rule", 1))
+        # stop_rule 2 (default): the reference's recurrence with FP64 residual replacement
+        # and the true residual as the stopping test; the plain recurrence (stop_rule=1,
+        # PyTO's sqrt(r.z / r0.z0) test) drifts and can diverge on high-contrast designs,
+        # where the reference only warns and returns the last iterate
+        # (src/deflation.py:582-583).  precision="mixed": FP32 recurrence, FP64 residual.
+        if kwargs.get("precision", "fp64") == "mixed":
+            u, info = g.dpcg_mixed(A0.s, b, dd, rtol=rtol, max_iters=kwargs.get("maxIters", 4000))
+        else:
+            u, info = g.dpcg(A0.s, b, dd, rtol=rtol, max_iters=kwargs.get("maxIters", 4000),
+                             stop_rule=kwargs.get("stop_rule", 2))
         dsolver.last_info = info
     elif solver in (Solvers.SPSOLVE, Solvers.SPLU, Solvers.PARDISO, Solvers.PETSC, Solvers.PYAMG):
         tol = rtol if solver == Solvers.PYAMG else min(rtol, 1e-12)
