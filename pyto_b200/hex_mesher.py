@@ -167,7 +167,26 @@ class HexMesher:
         return np.where(col == (0 if minLimit else self.grid[axis]))[0]
 
     def setPseudoDensity(self, rho):
-        self.elemPseudoDensity = np.asarray(rho.detach().cpu().numpy() if hasattr(rho, "detach") else rho).copy()
+        """Keep a copy of the densities; a device tensor stays on the device and is copied
+        to the host only when ``elemPseudoDensity`` is read (the optimisation loops set it
+        every iteration)."""
+        if hasattr(rho, "detach"):
+            self._pseudo_dev = rho.detach().clone()
+            self._elemPseudoDensity = None
+        else:
+            self._pseudo_dev = None
+            self._elemPseudoDensity = np.asarray(rho).copy()
+
+    @property
+    def elemPseudoDensity(self):
+        if getattr(self, "_elemPseudoDensity", None) is None and getattr(self, "_pseudo_dev", None) is not None:
+            self._elemPseudoDensity = self._pseudo_dev.cpu().numpy()
+        return getattr(self, "_elemPseudoDensity", None)
+
+    @elemPseudoDensity.setter
+    def elemPseudoDensity(self, value):
+        self._pseudo_dev = None
+        self._elemPseudoDensity = value
 
     def set_active_elements(self, active):
         """Restrict the domain to a subset of the box (e.g. an L-shape); nodes touched by

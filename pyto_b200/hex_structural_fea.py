@@ -75,7 +75,7 @@ class HexStructuralFEA:
         self.elem_material_scaling = s
         self.stiff_mtrx = linear_solvers.StiffnessOperator(self.grid, s)
         self.external_force = self.bc.force
-        u = linear_solvers.solve(self.stiff_mtrx, self.grid.tensor(self.bc.force), self.solver, self.bc,
+        u = linear_solvers.solve(self.stiff_mtrx, self._force_device(), self.solver, self.bc,
                                  dsolver=self.dsolver, **{k: v for k, v in self.kwargs.items() if k != "device"})
         self.last_info = linear_solvers.solve.last_info
         self.sol_dev = u
@@ -86,6 +86,19 @@ class HexStructuralFEA:
         self.solElastic = None
         self.total_force = self.external_force
         return _np(u) if to_np else u
+
+    def _force_device(self):
+        """bc.force on the device, copied once per force array (a new array, or a rebound
+        bc.force, is copied again; modify the force by assigning a new array)."""
+        f = self.bc.force
+        if isinstance(f, torch.Tensor):
+            return self.grid.tensor(f)
+        key = (id(f), f.__array_interface__["data"][0] if hasattr(f, "__array_interface__") else None)
+        if getattr(self, "_force_key", None) != key:
+            self._force_dev = self.grid.tensor(f)
+            self._force_key = key
+            self._force_ref = f  # keeps the keyed array alive, so its id is not reused
+        return self._force_dev
 
     @property
     def deformation(self):
