@@ -74,7 +74,9 @@ typedef struct pyto_solve_cfg {
   int32_t stop_rule;    /* 0: ||r||_2 < rtol ||b||_2 (scipy cg); 1: sqrt(r.z / r0.z0) <= rtol (PyTO DPCG);
                            2 (pyto_dpcg_solve only): FP64 residual replacement, see there */
   int32_t check_every;  /* host polls convergence every this many iterations (>=1) */
-  int32_t x0_given;     /* 1: u holds the initial guess on entry; 0: start from zero */
+  int32_t x0_given;     /* 1: u holds the initial guess on entry; 0: start from zero (the deflated
+                           solvers: from the coarse solution); honoured by pyto_pcg_solve and by the
+                           residual-replacement deflated solvers (stop rule 2, mixed) */
 } pyto_solve_cfg_t;
 
 typedef struct pyto_solve_status {

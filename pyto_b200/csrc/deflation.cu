@@ -851,7 +851,7 @@ __device__ __forceinline__ void prolong_node(const GridDims& g, const DeflP& dp,
   }
 }
 
-// x = W mu (masked); ADD: x += W mu
+// x = W mu (masked); ADD: x += W mu on the free DOFs (fixed DOFs set to 0)
 template <typename T, bool ADD = false>
 __global__ void __launch_bounds__(256) k_prolong(GridDims g, DeflP dp, const int32_t* __restrict__ ngrp,
                                                  const double* __restrict__ gc, const double* __restrict__ mu,
@@ -863,11 +863,11 @@ __global__ void __launch_bounds__(256) k_prolong(GridDims g, DeflP dp, const int
     const int f = fl[n];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const T v = ((f >> c) & 1) ? T(0) : (T)w[c];
+      const bool fixed = (f >> c) & 1;  // fixed DOFs are 0 in both forms
       if (ADD)
-        x[3 * n + c] += v;
+        x[3 * n + c] = fixed ? T(0) : x[3 * n + c] + (T)w[c];
       else
-        x[3 * n + c] = v;
+        x[3 * n + c] = fixed ? T(0) : (T)w[c];
     }
   }
 }
@@ -1654,10 +1654,15 @@ static int dpcg_reliable(const pyto_operator_t* op, const double* s, const uint8
   const bool lists = nchunks > 0;
   k_state_init2<<<1, 1, 0, st>>>(W.S, cfg->rtol, cfg->max_iters, 0);
   PYTO_COUNT(1);
-  // coarse start in FP64: u = W Einv W_f^T b   (src/deflation.py:532-537)
-  if ((rc = coarse_solve(g, dp, defl, b, W, nullptr, st))) return rc;
-  k_prolong<double><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center, W.mu, W.fl, u);
-  PYTO_COUNT(1);
+  // start: the coarse solution u = W Einv W_f^T b (src/deflation.py:532-537), or the
+  // caller's u (cfg->x0_given), whose residual's coarse part the first replacement removes
+  const bool warm = cfg->x0_given != 0;
+  if (!warm) {
+    if ((rc = coarse_solve(g, dp, defl, b, W, nullptr, st))) return rc;
+    k_prolong<double><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, defl->node_group, defl->group_center, W.mu, W.fl,
+                                                           u);
+    PYTO_COUNT(1);
+  }
 
   auto reliable = [&](bool coarse) -> int {
     int e;
@@ -1698,7 +1703,7 @@ static int dpcg_reliable(const pyto_operator_t* op, const double* s, const uint8
     }
     return PYTO_OK;
   };
-  if ((rc = reliable(false))) return rc;
+  if ((rc = reliable(warm))) return rc;
   if ((rc = restart_p())) return rc;
   PYTO_LAUNCH_CHECK();
   KrylovState hs{};
@@ -1797,6 +1802,7 @@ extern "C" int pyto_dpcg_solve(const pyto_operator_t* op, const double* s, const
   DpcgWs W = carve_dpcg(op, dp.nc, ws, ws_bytes, &need);
   if (!ws || ws_bytes < need) return PYTO_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
+  if (cfg->x0_given && cfg->stop_rule != 2) return PYTO_ERR_ARG;  // rules 0/1 start from the coarse solution
   if (cfg->stop_rule == 2) {
     if (!(cfg->rtol > 0.0)) return PYTO_ERR_ARG;
     return dpcg_reliable<double>(op, s, mask, defl, b, u, cfg, kReliableDelta, status, W, st);

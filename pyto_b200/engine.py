@@ -148,13 +148,19 @@ class HexGrid:
         wsp, wsn = self._ws(A.WS_DPCG, "krylov")
         A.call("pyto_dpcg_setup", self.opp, A.ptr(s), A.ptr(self.mask), C.byref(defl.struct), wsp, wsn, self._st())
 
-    def dpcg(self, s, b, defl, rtol=1e-8, max_iters=2000, stop_rule=1, check_every=25, out=None, setup=True):
-        """Deflated PCG (coarse inverse rebuilt for s when setup=True)."""
+    def dpcg(self, s, b, defl, rtol=1e-8, max_iters=2000, stop_rule=1, check_every=25, out=None, setup=True,
+             x0=None):
+        """Deflated PCG (coarse inverse rebuilt for s when setup=True).  x0 (a warm start)
+        needs stop_rule=2."""
         if setup:
             self.dpcg_setup(s, defl)
         defl.sync(self)
         u = out if out is not None else torch.empty(self.ndof, dtype=F64, device=self.device)
-        cfg = self._cfg(rtol, max_iters, stop_rule, check_every, False)
+        if x0 is not None:
+            if stop_rule != 2:
+                raise ValueError("a warm start needs stop_rule=2 (the other rules start from the coarse solution)")
+            u.copy_(x0)
+        cfg = self._cfg(rtol, max_iters, stop_rule, check_every, x0 is not None)
         stt = A.SolveStatus()
         wsp, wsn = self._ws(A.WS_DPCG, "krylov")
         rc = A.call("pyto_dpcg_solve", self.opp, A.ptr(s), A.ptr(self.mask), C.byref(defl.struct), A.ptr(b),
@@ -164,7 +170,7 @@ class HexGrid:
                             float(stt.true_rel_res), rc)
 
     def dpcg_mixed(self, s, b, defl, rtol=1e-8, delta=1e-1, max_iters=4000, check_every=10, out=None,
-                   setup=True):
+                   setup=True, x0=None):
         """Deflated PCG in mixed precision: an FP32 recurrence whose residual is replaced
         by the FP64 true residual b - K u (u held in FP64) each time it has dropped by
         `delta`; converged when ||b - K u|| <= rtol ||b|| in FP64.  info.cycles is the
@@ -175,7 +181,9 @@ class HexGrid:
             A.call("pyto_dpcg_setup", self.opp, A.ptr(s), A.ptr(self.mask), C.byref(defl.struct), wsp, wsn,
                    self._st())
         u = out if out is not None else torch.empty(self.ndof, dtype=F64, device=self.device)
-        cfg = self._cfg(rtol, max_iters, 0, check_every, False)
+        if x0 is not None:
+            u.copy_(x0)
+        cfg = self._cfg(rtol, max_iters, 0, check_every, x0 is not None)
         stt = A.SolveStatus()
         rc = A.call("pyto_dpcg_mixed_solve", self.opp, A.ptr(s), A.ptr(self.mask), C.byref(defl.struct), A.ptr(b),
                     A.ptr(u), C.byref(cfg), float(delta), C.byref(stt), wsp, wsn, self._st(),

@@ -75,8 +75,11 @@ class HexStructuralFEA:
         self.elem_material_scaling = s
         self.stiff_mtrx = linear_solvers.StiffnessOperator(self.grid, s)
         self.external_force = self.bc.force
+        kw = {k: v for k, v in self.kwargs.items() if k not in ("device", "warm_start")}
+        if self.kwargs.get("warm_start") and self.solver == linear_solvers.Solvers.DPCG and self.sol_dev is not None:
+            kw["x0"] = self.sol_dev  # the previous design's solution
         u = linear_solvers.solve(self.stiff_mtrx, self._force_device(), self.solver, self.bc,
-                                 dsolver=self.dsolver, **{k: v for k, v in self.kwargs.items() if k != "device"})
+                                 dsolver=self.dsolver, **kw)
         self.last_info = linear_solvers.solve.last_info
         self.sol_dev = u
         self._sol_np = None

@@ -40,6 +40,7 @@ def main(argv=None):
                                                           "mixed", "pcg", "batch", "oc"])
     ap.add_argument("--iters", type=int, default=20, help="--kernel oc: OC iterations")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"], help="--kernel oc: DPCG form")
+    ap.add_argument("--warm-start", action="store_true", help="--kernel oc: start each solve from the previous one")
     ap.add_argument("--designs", type=int, default=64, help="--kernel batch: number of designs")
     ap.add_argument("--no-tune", action="store_true", help="--kernel batch: skip the autotuner")
     ap.add_argument("--groups", type=int, default=432, help="deflation groups for --kernel dpcg")
@@ -123,19 +124,30 @@ def oc_bench(a):
     ds = DeflationSolver(modes=6, shift=1e-14, shift_relative=True)
     ds.create_deflation_groups(mesh, a.groups)
     fe = hex_structural_fea.HexStructuralFEA(mesh=mesh, mat_prop=mat, bc=bc, solver=linear_solvers.Solvers.DPCG,
-                                             dsolver=ds, rtol=1e-8, precision=a.precision)
+                                             dsolver=ds, rtol=1e-8, precision=a.precision, warm_start=a.warm_start)
     params = tc.TOParams(Constraints=[(tc.TO_QOI.VOLUME_FRACTION, None, 0.3)], RelativeFilterRadius=1.5)
     run = lambda n: topopt_ocm.topopt_optimality_criteria(tc.FEA_MODE.STRUCTURAL, fe, params, maxIterations=n,
                                                           plot_progress=False, print_progress=False,
                                                           binarize_topology=False)
+    iters = []
+    solve = fe.solve
+
+    def counted_solve(*args, **kw):  # records the Krylov iterations of every FEA solve
+        out = solve(*args, **kw)
+        iters.append(int(fe.last_info.iters))
+        return out
+
+    fe.solve = counted_solve
     run(1)  # warm-up: library load, workspaces
+    iters.clear()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     sol, hist, ok, msg, nfea = run(a.iters)
     torch.cuda.synchronize()
     t = time.perf_counter() - t0
     obj = [float(v) for v in hist["objective"]]
-    print(json.dumps({"kernel": "oc", "precision": a.precision, "nel": nel, "iterations": a.iters, "fea_solves": int(nfea), "s": t,
+    print(json.dumps({"kernel": "oc", "precision": a.precision, "warm_start": a.warm_start, "nel": nel,
+                      "iterations": a.iters, "fea_solves": int(nfea), "krylov_iterations": sum(iters), "s": t,
                       "ms_per_iteration": 1e3 * t / max(1, nfea), "objective_first": obj[0],
                       "objective_last": obj[-1], "volfrac_last": float(hist["volfrac"][-1])}))
 

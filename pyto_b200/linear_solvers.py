@@ -99,11 +99,15 @@ def solve(A0, b0, solver: Solvers, bc, **kwargs):
         # PyTO's sqrt(r.z / r0.z0) test) drifts and can diverge on high-contrast designs,
         # where the reference only warns and returns the last iterate
         # (src/deflation.py:582-583).  precision="mixed": FP32 recurrence, FP64 residual.
+        # x0: a warm start (e.g. the previous design's solution; residual-replacement forms only)
+        x0 = kwargs.get("x0")
+        if x0 is not None:  # the free part of a full solution: prescribed values are added back below
+            x0 = g.tensor(x0) if lift is None else g.tensor(x0) - lift
         if kwargs.get("precision", "fp64") == "mixed":
-            u, info = g.dpcg_mixed(A0.s, b, dd, rtol=rtol, max_iters=kwargs.get("maxIters", 4000))
+            u, info = g.dpcg_mixed(A0.s, b, dd, rtol=rtol, max_iters=kwargs.get("maxIters", 4000), x0=x0)
         else:
             u, info = g.dpcg(A0.s, b, dd, rtol=rtol, max_iters=kwargs.get("maxIters", 4000),
-                             stop_rule=kwargs.get("stop_rule", 2))
+                             stop_rule=kwargs.get("stop_rule", 2), x0=x0)
         dsolver.last_info = info
     elif solver in (Solvers.SPSOLVE, Solvers.SPLU, Solvers.PARDISO, Solvers.PETSC, Solvers.PYAMG):
         tol = rtol if solver == Solvers.PYAMG else min(rtol, 1e-12)

@@ -347,6 +347,34 @@ def test_dpcg_fp64_residual_replacement(rtol):
     assert abs(C.item() - C2.item()) <= 10 * rtol * abs(C2.item())
 
 
+@pytest.mark.parametrize("mixed", [False, True])
+def test_dpcg_warm_start(mixed):
+    """A warm start (residual-replacement forms) reaches the same solution in fewer
+    iterations from a nearby design's solution."""
+    from pyto_b200.engine import DeviceDeflation
+    nel = (32, 16, 16)
+    m = O.grid_mesh(*nel)
+    f, fixed = O.cantilever_bc(m)
+    g = _grid(nel, fixed=fixed)
+    rng = np.random.default_rng(8)
+    x = rng.uniform(0.05, 1.0, m["num_elems"])
+    s0, _ = g.simp(_dev(x), 3.0, 1e-9)
+    s1, _ = g.simp(_dev(np.clip(x * (1 + 0.02 * rng.normal(size=x.size)), 0.05, 1.0)), 3.0, 1e-9)
+    grp, cnt, cen = O.deflation_groups(m["node_xyz"], 40)
+    defl = DeviceDeflation(g, grp, cen, modes=6, shift=1e-14, shift_relative=True)
+    b = _dev(f)
+    solve = (lambda s, x0=None: g.dpcg_mixed(s, b, defl, rtol=1e-10, x0=x0)) if mixed else \
+        (lambda s, x0=None: g.dpcg(s, b, defl, rtol=1e-10, stop_rule=2, x0=x0))
+    u0, _ = solve(s0)
+    u1, i1 = solve(s1)
+    u2, i2 = solve(s1, u0.clone())
+    assert i1.converged and i2.converged and i2.true_rel_res <= 1e-10
+    assert i2.iters < i1.iters, (i2.iters, i1.iters)
+    assert (u2 - u1).abs().max().item() <= 1e-7 * u1.abs().max().item()
+    with pytest.raises(ValueError):
+        g.dpcg(s1, b, defl, rtol=1e-10, stop_rule=0, x0=u0)
+
+
 def test_dpcg_mixed_golden_compliance():
     from pyto_b200.engine import DeviceDeflation
     d, m, g, s, ds = _cantilever_case("cantilever_12x6x6_direct.npz", (12, 6, 6), (1.0, 1.0, 1.0))
