@@ -127,8 +127,12 @@ const char* pyto_last_error(void);
  * reference counterpart: instrumentation of the launch count). */
 long long pyto_launch_count(void);
 /* Select the tile variant of a kernel (no reference counterpart: the tile
- * choice of the project's autotuner).  PYTO_KERNEL_MATVEC variants 0..3 (default 2).
- * Process-wide; not thread-safe against concurrent launches. */
+ * choice of the project's autotuner).  PYTO_KERNEL_MATVEC variants 0..3 (tile kernel,
+ * default 2) and 8..10 (chunk-staged kernel: node-plane rows copied as 16-byte chunks,
+ * faces and pending accumulators in registers; bitwise-equal results); PYTO_KERNEL_MATVEC32
+ * variants 0..5 and 8..11.  The chunk-staged variants need u and the mask 16-byte
+ * aligned and otherwise run the tile kernel.  Process-wide; not thread-safe against
+ * concurrent launches. */
 #define PYTO_KERNEL_MATVEC 0
 #define PYTO_KERNEL_MATVEC32 1
 #define PYTO_KERNEL_GRAPHS 2   /* variant 1 (default): deflated PCG iteration chunks replayed as

@@ -1,8 +1,10 @@
 """Autotuner of the matrix-free operator's tile shape, per grid.
 
 The matvec kernel has four tile variants (CTA of 32 x TY threads marching up z,
-TY in {4, 8, 16}, with 1 to 3 CTAs per SM); the FP32 operator has two more that
-run the element contraction on the tensor cores.  Which is fastest depends on the grid
+TY in {4, 8, 16}, with 1 to 3 CTAs per SM) and three or four chunk-staged ones
+(variants 8-11: node-plane rows copied as 16-byte chunks, faces and pending
+accumulators in registers); the FP32 operator has two more that run the element
+contraction on the tensor cores.  Which is fastest depends on the grid
 (how the (nx+1) x (ny+1) node columns divide into tiles, and the z-slab count).
 ``autotune(grid)`` times every variant with CUDA events on the grid itself, FP64
 and FP32, and stores the choice in the grid's operator (``op.tune``), which every
@@ -15,8 +17,8 @@ import torch
 from . import _capi as A
 
 _CACHE: dict = {}
-VARIANTS = (0, 1, 2, 3)
-VARIANTS_F32 = (0, 1, 2, 3, 4, 5)  # 4, 5: element contraction on the tensor cores (BF16 split)
+VARIANTS = (0, 1, 2, 3, 8, 9, 10)  # 8-10: chunk-staged planes, faces and accumulators in registers
+VARIANTS_F32 = (0, 1, 2, 3, 4, 5, 8, 9, 10, 11)  # 4, 5: element contraction on the tensor cores (BF16 split)
 
 
 def _time(fn, reps):

@@ -1411,13 +1411,16 @@ struct DVec {
 int launch_matvec32(const pyto_operator_t* op, const float* s, const uint8_t* mask, const float* u, float* y,
                     int mode, double* part, unsigned* counter, double* dot, cudaStream_t st);
 
+// K(s) u for the iteration vectors p and z only: both are zero on fixed DOFs (z =
+// M^-1 r is, by jacobi_apply; p = z + beta p - W mu is, by update2_node), so the
+// input mask would select the same values and is skipped.
 static int matvec_t(const pyto_operator_t* op, const double* s, const uint8_t* mask, const double* u, double* y,
                     double* part, unsigned* counter, double* dot, cudaStream_t st) {
-  return launch_matvec64(op, s, mask, u, y, PYTO_MASK_IN | PYTO_MASK_OUT, part, counter, dot, st);
+  return launch_matvec64(op, s, mask, u, y, PYTO_MASK_OUT, part, counter, dot, st);
 }
 static int matvec_t(const pyto_operator_t* op, const float* s, const uint8_t* mask, const float* u, float* y,
                     double* part, unsigned* counter, double* dot, cudaStream_t st) {
-  return launch_matvec32(op, s, mask, u, y, PYTO_MASK_IN | PYTO_MASK_OUT, part, counter, dot, st);
+  return launch_matvec32(op, s, mask, u, y, PYTO_MASK_OUT, part, counter, dot, st);
 }
 
 // One deflated PCG run (src/deflation.py:504-584) in vector precision T;
@@ -1917,7 +1920,7 @@ static int batch_branch(const pyto_batch_item_t& it, const pyto_solve_cfg_t* cfg
   cudaGraph_t body = np.conditional.phGraph_out[0];
   PYTO_CUDA(cudaStreamUpdateCaptureDependencies(si, &cnode, 1, cudaStreamSetCaptureDependencies));
   PYTO_CUDA(cudaStreamBeginCaptureToGraph(sb, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-  int brc = launch_matvec64(op, it.s, it.mask, W.p, W.q, PYTO_MASK_IN | PYTO_MASK_OUT, W.part, W.counter, &W.S->pq,
+  int brc = launch_matvec64(op, it.s, it.mask, W.p, W.q, PYTO_MASK_OUT, W.part, W.counter, &W.S->pq,  // p: masked
                             sb);
   if (!brc) {
     k_dpcg_update1<double><<<kNodeBlocks, kNodeThreads, 0, sb>>>(g, pc, W.w, W.fl, it.u, W.r, W.z, W.p, W.q, W.S,

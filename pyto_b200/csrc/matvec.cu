@@ -102,6 +102,10 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
+}  // namespace pyto
+#include "matvec_chunked.cuh"
+namespace pyto {
+
 template <typename T, int TY, bool DOT, bool MASKIN, int MINB, bool TC = false>
 __global__ void __launch_bounds__(32 * TY, MINB)
     k_matvec(GridDims g, KHat kh, const T* __restrict__ s, const uint8_t* __restrict__ mask,
@@ -507,20 +511,59 @@ static int launch_mv(const GridDims& g, const KHat& kh, const T* s, const uint8_
                                                          nullptr, st);
 }
 
+template <typename T, int TY, bool DOT, bool MI, int MINB, bool GS, bool RF>
+static int launch_mvc_t(const MvLaunch& L, const GridDims& g, const KHatT<T>& kh, const T* s, const uint8_t* mask,
+                        const T* u, T* y, int mode, double* part, unsigned* counter, double* dot, cudaStream_t st) {
+  constexpr size_t smem = ChunkTile<T, TY, GS>::bytes;
+  static bool attr = false;
+  if (!attr) {
+    PYTO_CUDA(cudaFuncSetAttribute(k_matvec_chunked<T, TY, DOT, MI, MINB, GS, RF>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr = true;
+  }
+  k_matvec_chunked<T, TY, DOT, MI, MINB, GS, RF><<<L.grid, 32 * TY, smem, st>>>(g, kh, s, mask, u, y, L.zc, mode, part,
+                                                                        counter, dot);
+  PYTO_COUNT(1);
+  PYTO_LAUNCH_CHECK();
+  return PYTO_OK;
+}
+
+// chunk-staged kernel; u and the mask must be 16-byte aligned, else k_matvec (same results)
+template <typename T, int TY, int MINB, bool GS = false, bool RF = false>
+static int launch_mvc(const GridDims& g, const KHat& kh, const T* s, const uint8_t* mask, const T* u, T* y, int mode,
+                      double* part, unsigned* counter, double* dot, cudaStream_t st) {
+  if (((uintptr_t)u & 15) || ((uintptr_t)mask & 15))
+    return launch_mv<T, TY, MINB>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
+  const MvLaunch L = matvec_launch<32, TY>(g);
+  const KHatT<T> kt = make_khat_t<T>(kh);
+  const bool mi = (mode & PYTO_MASK_IN) && mask != nullptr;
+  if (dot)
+    return mi ? launch_mvc_t<T, TY, true, true, MINB, GS, RF>(L, g, kt, s, mask, u, y, mode, part, counter, dot, st)
+              : launch_mvc_t<T, TY, true, false, MINB, GS, RF>(L, g, kt, s, mask, u, y, mode, part, counter, dot, st);
+  return mi ? launch_mvc_t<T, TY, false, true, MINB, GS, RF>(L, g, kt, s, mask, u, y, mode, nullptr, nullptr, nullptr,
+                                                         st)
+            : launch_mvc_t<T, TY, false, false, MINB, GS, RF>(L, g, kt, s, mask, u, y, mode, nullptr, nullptr, nullptr,
+                                                          st);
+}
+
 // Tile variant of the FP64 matvec (2 = default: fastest measured at 192x96x96):
 //   0: 32x8 threads, 2 CTAs/SM (128 registers)   1: 32x8, 1 CTA/SM (no register cap)
 //   2: 32x4, 3 CTAs/SM                            3: 32x16, 1 CTA/SM
 static int g_mv_variant = 2;
-// Tile variant of the FP32 matvec (same numbering; 0 = default; 4 and 5: the tile
-// shapes of 0 and 2 with the element core on the tensor cores, BF16 split hi/lo)
-static int g_mv32_variant = 0;
+// Tile variant of the FP32 matvec (same numbering; 4 and 5: the tile shapes of 0 and
+// 2 with the element core on the tensor cores, BF16 split hi/lo; 8-11: chunk-staged
+// kernel, 8 = default: fastest measured at 192x96x96)
+static int g_mv32_variant = 8;
 
 int launch_matvec64(const pyto_operator_t* op, const double* s, const uint8_t* mask, const double* u, double* y,
                     int mode, double* part, unsigned* counter, double* dot, cudaStream_t st) {
   const GridDims g = make_dims(op);
   const KHat kh = make_khat(op);
   const int tv = (op->tune & 0xff) - 1;  // per-grid choice of the autotuner, else the library default
-  switch (tv >= 0 && tv <= 3 ? tv : g_mv_variant) {
+  switch ((tv >= 0 && tv <= 3) || (tv >= 8 && tv <= 10) ? tv : g_mv_variant) {
+    case 8: return launch_mvc<double, 4, 3, true, true>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
+    case 9: return launch_mvc<double, 8, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
+    case 10: return launch_mvc<double, 4, 2>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
     case 1: return launch_mv<double, 8, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
     case 2: return launch_mv<double, 4, 3>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
     case 3: return launch_mv<double, 16, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
@@ -533,7 +576,11 @@ int launch_matvec32(const pyto_operator_t* op, const float* s, const uint8_t* ma
   const GridDims g = make_dims(op);
   const KHat kh = make_khat(op);
   const int tv = ((op->tune >> 8) & 0xff) - 1;
-  switch (tv >= 0 && tv <= 5 ? tv : g_mv32_variant) {
+  switch ((tv >= 0 && tv <= 5) || (tv >= 8 && tv <= 11) ? tv : g_mv32_variant) {
+    case 8: return launch_mvc<float, 8, 3>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
+    case 9: return launch_mvc<float, 8, 2>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
+    case 10: return launch_mvc<float, 4, 6>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
+    case 11: return launch_mvc<float, 16, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
     case 1: return launch_mv<float, 8, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
     case 2: return launch_mv<float, 4, 3>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
     case 3: return launch_mv<float, 16, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
@@ -547,13 +594,13 @@ int launch_matvec32(const pyto_operator_t* op, const float* s, const uint8_t* ma
 long long matvec_blocks(const pyto_operator_t* op) { return matvec_launch<32, 4>(make_dims(op)).nblocks; }
 
 int set_matvec_variant(int v) {
-  if (v < 0 || v > 3) return PYTO_ERR_ARG;
+  if (v < 0 || (v > 3 && v < 8) || v > 10) return PYTO_ERR_ARG;
   g_mv_variant = v;
   return PYTO_OK;
 }
 
 int set_matvec32_variant(int v) {
-  if (v < 0 || v > 5) return PYTO_ERR_ARG;
+  if (v < 0 || (v > 5 && v < 8) || v > 11) return PYTO_ERR_ARG;
   g_mv32_variant = v;
   return PYTO_OK;
 }

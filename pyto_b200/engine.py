@@ -110,12 +110,15 @@ class HexGrid:
                self._st())
         return (y, d) if dot else y
 
-    def matvec_f32(self, s32, u32, mode=A.MASK_IN | A.MASK_OUT, out=None):
-        """FP32 y = K(s) u (the operator of the mixed-precision inner cycles)."""
+    def matvec_f32(self, s32, u32, mode=A.MASK_IN | A.MASK_OUT, out=None, dot=False):
+        """FP32 y = K(s) u (the operator of the mixed-precision inner cycles); dot: also
+        u.y accumulated in FP64."""
         y = out if out is not None else torch.empty(self.ndof, dtype=torch.float32, device=self.device)
-        A.call("pyto_matvec_f32", self.opp, A.ptr(s32), A.ptr(self.mask), A.ptr(u32), A.ptr(y), int(mode), None,
-               None, 0, self._st())
-        return y
+        d = torch.empty(1, dtype=F64, device=self.device) if dot else None
+        wsp, wsn = self._ws(A.WS_REDUCE, "reduce") if dot else (None, 0)
+        A.call("pyto_matvec_f32", self.opp, A.ptr(s32), A.ptr(self.mask), A.ptr(u32), A.ptr(y), int(mode), A.ptr(d),
+               wsp, wsn, self._st())
+        return (y, d) if dot else y
 
     def jacobi(self, s):
         winv = torch.empty(self.nnodes, dtype=F64, device=self.device)
