@@ -934,8 +934,8 @@ __device__ __forceinline__ void update1_dof(const Prec& pc, int f, int c, double
 }
 
 // alpha = r.z / p.q; x += alpha p; r -= alpha q; z = M^-1 r; r.r, r.z (FP64).
-// Threads take quads of 4 nodes (12 DOFs, 16-byte loads); the < 4 nodes after
-// the last full quad are done one DOF at a time.
+// Threads take 16-byte chunks of the vectors (grid-stride); the DOFs after the
+// last full chunk are done one at a time.
 template <typename T>
 __global__ void __launch_bounds__(kNodeThreads, 4) k_dpcg_update1(GridDims g, Prec pc, const double* __restrict__ w,
                                                                const uint8_t* __restrict__ fl, T* __restrict__ x,
@@ -955,45 +955,39 @@ __global__ void __launch_bounds__(kNodeThreads, 4) k_dpcg_update1(GridDims g, Pr
   }
   const T al = (T)alpha;
   double rr = 0.0, rzn = 0.0;
-  const long long nq = g.nnodes / 4;
-  const long long gt = blockIdx.x * (long long)blockDim.x + threadIdx.x, gs = (long long)gridDim.x * blockDim.x;
+  // stream 16-byte chunks (N DOFs) of x, r, p, q; the Jacobi weight and flags of a
+  // DOF's node come through the read-only cache
   using CK = Chunk<T>;
-  constexpr int NK = 12 / CK::N;  // 16-byte chunks per quad
-  for (long long t = gt; t < nq; t += gs) {
-    double wn[4];
-    unsigned f4;
-    ld_quad_node(w, fl, t, wn, f4);
+  constexpr int N = CK::N;
+  const long long ndof = 3 * g.nnodes, nck = ndof / N;
+  const long long gt = blockIdx.x * (long long)blockDim.x + threadIdx.x, gs = (long long)gridDim.x * blockDim.x;
+  auto chunk = [&](long long ck, T (&xv)[N], T (&rv)[N], const T (&pv)[N], const T (&qv)[N], T (&zv)[N]) {
 #pragma unroll
-    for (int k = 0; k < NK; ++k) {
-      const long long ck = NK * t + k;
-      T xv[CK::N], rv[CK::N], pv[CK::N], qv[CK::N], zv[CK::N];
-      CK::ld(x, ck, xv);
-      CK::ld(r, ck, rv);
-      CK::ld(p, ck, pv);
-      CK::ld(q, ck, qv);
-#pragma unroll
-      for (int j = 0; j < CK::N; ++j) {
-        const int d = k * CK::N + j;  // DOF within the quad
-        update1_dof<T>(pc, (f4 >> (8 * (d / 3))) & 0xff, d % 3, wn[d / 3], al, xv[j], rv[j], zv[j], pv[j], qv[j],
-                       rr, rzn);
-      }
-      CK::st(x, ck, xv);
-      CK::st(r, ck, rv);
-      CK::st(z, ck, zv);
+    for (int j = 0; j < N; ++j) {
+      const unsigned d = (unsigned)(N * ck) + j;  // DOF ids fit in int32 (pyto_operator_init)
+      const unsigned n = d / 3;
+      update1_dof<T>(pc, __ldg(fl + n), (int)(d - 3 * n), __ldg(w + n), al, xv[j], rv[j], zv[j], pv[j], qv[j], rr,
+                     rzn);
     }
+  };
+  for (long long k = gt; k < nck; k += gs) {
+    T xv[N], rv[N], pv[N], qv[N], zv[N];
+    CK::ld(x, k, xv);
+    CK::ld(r, k, rv);
+    CK::ld(p, k, pv);
+    CK::ld(q, k, qv);
+    chunk(k, xv, rv, pv, qv, zv);
+    CK::st(x, k, xv);
+    CK::st(r, k, rv);
+    CK::st(z, k, zv);
   }
-  if (gt < g.nnodes - 4 * nq) {
-    const long long n = 4 * nq + gt;
-    const int f = fl[n];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const long long i = 3 * n + c;
-      T xi = x[i], ri = r[i], zi;
-      update1_dof<T>(pc, f, c, w[n], al, xi, ri, zi, p[i], q[i], rr, rzn);
-      x[i] = xi;
-      r[i] = ri;
-      z[i] = zi;
-    }
+  if (gt < ndof - N * nck) {  // DOFs after the last full chunk
+    const unsigned i = (unsigned)(N * nck + gt), n = i / 3;
+    T xi = x[i], ri = r[i], zi;
+    update1_dof<T>(pc, fl[n], (int)(i - 3 * n), w[n], al, xi, ri, zi, p[i], q[i], rr, rzn);
+    x[i] = xi;
+    r[i] = ri;
+    z[i] = zi;
   }
   double v[2];
   v[0] = block_sum<kNodeThreads>(rr, sred);
