@@ -218,13 +218,62 @@ __device__ __forceinline__ void mode_comp_hat(const int (&gr)[8], const int (&mk
   }
 }
 
+// 8-point Hadamard transform of corner values (the basis of mode_comp_hat)
+__device__ __forceinline__ void had8(const double (&v)[8], double (&H)[8]) {
+  double Fb[4], Ft[4];
+  face_fwd(v[0], v[1], v[2], v[3], Fb);
+  face_fwd(v[4], v[5], v[6], v[7], Ft);
+#pragma unroll
+  for (int f = 0; f < 4; ++f) {
+    H[f] = Ft[f] + Fb[f];
+    H[f + 4] = Ft[f] - Fb[f];
+  }
+}
+
+// For an element without fixed DOFs the masked rigid modes of group Gs are linear
+// combinations of four corner vectors: the indicator of the corners in Gs (ind) and
+// ind times the local corner coordinates lx, ly, lz (corner offsets times h).  Their
+// Hadamard transforms go to B[(i*8 + m) * stride] (shared memory, i = ind, lx, ly, lz).
+__device__ __forceinline__ void group_base_hat(const int (&gr)[8], int Gs, const double (&h)[3], double* B,
+                                               int stride) {
+  double v[8], H[8];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const double ind = (gr[k] == Gs) ? 1.0 : 0.0;
+      const double l = (i == 0) ? 1.0 : (i == 1) ? ((k & 1) ? h[0] : 0.0) : (i == 2) ? (((k >> 1) & 1) ? h[1] : 0.0)
+                                                                           : ((k >> 2) ? h[2] : 0.0);
+      v[k] = ind * l;
+    }
+    had8(v, H);
+#pragma unroll
+    for (int m = 0; m < 8; ++m) B[(i * 8 + m) * stride] = H[m];
+  }
+}
+
+// Component c, Hadamard mode m of masked rigid mode b (position d + local) from the
+// base vectors B (no fixed DOFs): [tx,ty,tz, rx:(0,-z,y), ry:(z,0,-x), rz:(-y,x,0)]
+__device__ __forceinline__ double mode_hat_from_base(const double* B, int stride, int b, int c, int m,
+                                                     const double (&d)[3]) {
+  const double b0 = B[m * stride];
+  auto pos = [&](int ax) { return d[ax] * b0 + B[((ax + 1) * 8 + m) * stride]; };  // (d + l)_ax ind
+  if (b < 3) return (b == c) ? b0 : 0.0;
+  if (b == 3) return (c == 1) ? -pos(2) : (c == 2) ? pos(1) : 0.0;
+  if (b == 4) return (c == 0) ? pos(2) : (c == 2) ? -pos(0) : 0.0;
+  return (c == 0) ? -pos(1) : (c == 1) ? pos(0) : 0.0;
+}
+
 // Row blocks E[G, :] from the boundary element lists: one CTA per list chunk
 // (chunk tables as for k_restrict_K), one entry per thread per pass.  For entry
 // (G, e) and every group H at a corner of e, s_e (Phi W_G|e)^T K^ (Phi W_H|e) is
 // added into a shared-memory accumulator of G's neighbour slots (the sums of
 // one CTA are formed with shared-memory atomics, so their order varies), which
 // is then added into E with global atomics.
+// Only the blocks E[G, H] with H <= G are formed (E is symmetric; k_mirror_upper
+// copies them into E[H, G]), and the mode loops are unrolled (M = dp.modes).
 constexpr int kCrThreads = 128;
+template <int M>
 __global__ void __launch_bounds__(kCrThreads) k_coarse_rows2(GridDims g, KHat kh, DeflP dp,
                                                              const double* __restrict__ s,
                                                              const uint8_t* __restrict__ mask,
@@ -237,7 +286,9 @@ __global__ void __launch_bounds__(kCrThreads) k_coarse_rows2(GridDims g, KHat kh
                                                              const int32_t* __restrict__ nptr,
                                                              const int32_t* __restrict__ nlist,
                                                              double* __restrict__ E) {
-  extern __shared__ double acc[];  // [nnb][36]
+  extern __shared__ double cr_smem[];
+  double* sbase = cr_smem;                  // [2][32][kCrThreads] group base vectors
+  double* acc = cr_smem + 64 * kCrThreads;  // [nnb][36]
   __shared__ int snb[128];
   const int ch = blockIdx.x;
   if (ch >= cptr[dp.ngroups]) return;
@@ -246,7 +297,6 @@ __global__ void __launch_bounds__(kCrThreads) k_coarse_rows2(GridDims g, KHat kh
   for (int t = threadIdx.x; t < nnb; t += blockDim.x) snb[t] = nlist[nb0 + t];
   for (int t = threadIdx.x; t < nnb * 36; t += blockDim.x) acc[t] = 0.0;
   __syncthreads();
-  const int M = dp.modes;
   const double h[3] = {dp.hx, dp.hy, dp.hz};
   const int end = bptr[G + 1];
   const int pn = g.sx * g.sy;
@@ -274,6 +324,7 @@ __global__ void __launch_bounds__(kCrThreads) k_coarse_rows2(GridDims g, KHat kh
       bool seen = false;
       for (int q = 0; q < nh; ++q) seen |= (Hs[q] == gr[k]);
       if (seen) continue;
+      if (gr[k] > G) continue;  // E[G, H] for H > G comes from the mirror
       int slot = 0;
       while (slot < nnb && snb[slot] != gr[k]) ++slot;
       if (slot == nnb) continue;  // not possible for a consistent neighbour list
@@ -282,6 +333,72 @@ __global__ void __launch_bounds__(kCrThreads) k_coarse_rows2(GridDims g, KHat kh
       ++nh;
     }
     const double relG[3] = {dp.hx * ex - gc[3 * G], dp.hy * ey - gc[3 * G + 1], dp.hz * ez - gc[3 * G + 2]};
+    bool anyfix = false;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) anyfix |= mk[k] != 0;
+    if (!anyfix) {
+      // B_GH[a][b] = s (Phi W_G,a)^T K^ (Phi W_H,b): for each (H, b) apply K^ once to
+      // mode b of H, then form all modes a of G from 12 dot products with G's base
+      double* BG = sbase + threadIdx.x;
+      double* BH = sbase + 32 * kCrThreads + threadIdx.x;
+      group_base_hat(gr, G, h, BG, kCrThreads);
+      for (int hi = 0; hi < nh; ++hi) {
+        const int H = Hs[hi];
+        const double relH[3] = {dp.hx * ex - gc[3 * H], dp.hy * ey - gc[3 * H + 1], dp.hz * ez - gc[3 * H + 2]};
+        group_base_hat(gr, H, h, BH, kCrThreads);
+#pragma unroll
+        for (int b = 0; b < M; ++b) {
+          double Hh[3][8];
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int m = 0; m < 8; ++m) Hh[c][m] = mode_hat_from_base(BH, kCrThreads, b, c, m, relH);
+          double Y[3][8];  // K^ Hh (rows m = 0 vanish)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            Y[c][0] = 0.0;
+#pragma unroll
+            for (int m = 1; m < 8; ++m) {
+              const int q = m ^ (1 << c);
+              double o = 0.0;
+#pragma unroll
+              for (int dd = 0; dd < 3; ++dd) {
+                const int md = member_mode(q, dd);
+                if (md == 0) continue;
+                o = fma(kh.b[q][3 * c + dd], Hh[dd][md], o);
+              }
+              Y[c][m] = o;
+            }
+          }
+          double D[4][3];  // base vector i of G . Y[c]
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              double t = 0.0;
+#pragma unroll
+              for (int m = 1; m < 8; ++m) t = fma(BG[(i * 8 + m) * kCrThreads], Y[c][m], t);
+              D[i][c] = t;
+            }
+          double vab[6];
+          vab[0] = D[0][0];
+          vab[1] = D[0][1];
+          vab[2] = D[0][2];
+          if (M == 6) {
+            vab[3] = -(relG[2] * D[0][1] + D[3][1]) + (relG[1] * D[0][2] + D[2][2]);
+            vab[4] = (relG[2] * D[0][0] + D[3][0]) - (relG[0] * D[0][2] + D[1][2]);
+            vab[5] = -(relG[1] * D[0][0] + D[2][0]) + (relG[0] * D[0][1] + D[1][1]);
+          }
+#pragma unroll
+          for (int a = 0; a < M; ++a) {
+            const double v = se * vab[a];
+            if (v != 0.0) atomicAdd(&acc[Sl[hi] * 36 + a * 6 + b], v);
+          }
+        }
+      }
+      continue;
+    }
+#pragma unroll
     for (int a = 0; a < M; ++a) {
       double Hg[3][8];
 #pragma unroll
@@ -307,6 +424,7 @@ __global__ void __launch_bounds__(kCrThreads) k_coarse_rows2(GridDims g, KHat kh
       for (int hi = 0; hi < nh; ++hi) {
         const int H = Hs[hi];
         const double relH[3] = {dp.hx * ex - gc[3 * H], dp.hy * ey - gc[3 * H + 1], dp.hz * ez - gc[3 * H + 2]};
+#pragma unroll
         for (int b = 0; b < M; ++b) {
           double v = 0.0;
 #pragma unroll
@@ -326,6 +444,16 @@ __global__ void __launch_bounds__(kCrThreads) k_coarse_rows2(GridDims g, KHat kh
     const int slot = t / (M * M), a = (t / M) % M, b = t % M;
     const double v = acc[slot * 36 + a * 6 + b];
     if (v != 0.0) atomicAdd(&E[((long long)G * M + a) * dp.nc + (long long)snb[slot] * M + b], v);
+  }
+}
+
+// E[i, j] = E[j, i] for the entries whose row group is below their column group
+// (the blocks k_coarse_rows2 leaves out)
+__global__ void k_mirror_upper(long long n, int modes, double* E) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n * n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long i = t / n, j = t - i * n;
+    if (i / modes < j / modes) E[t] = E[j * n + i];
   }
 }
 
@@ -363,18 +491,9 @@ __global__ void k_coarse_finish(long long nc, double* E, double shift, const dou
 // holding a 4 x 4 set of entries (rows ty + 16a, columns tx + 16b) in registers;
 // per pivot step only the pivot row and column pass through shared memory
 // (double-buffered, one barrier per step).
-__global__ void __launch_bounds__(256) k_sweep_pivot(long long n, int k0, int bk, const double* __restrict__ A,
-                                                     double* __restrict__ P) {
-  __shared__ double s_row[2][kSweepB], s_col[2][kSweepB];
+__device__ __forceinline__ void sweep_pivot_regs(double (&R)[4][4], int bk, double (*s_row)[kSweepB],
+                                                 double (*s_col)[kSweepB]) {
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  double R[4][4];
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const int i = ty + 16 * a, j = tx + 16 * b;
-      R[a][b] = (i < bk && j < bk) ? A[(k0 + i) * n + (k0 + j)] : (i == j ? 1.0 : 0.0);
-    }
   for (int p = 0; p < bk; ++p) {
     const int buf = p & 1, pa = p >> 4, pr = p & 15;
     if (ty == pr) {  // pivot row: register row pa of the threads with ty == p mod 16
@@ -434,6 +553,21 @@ __global__ void __launch_bounds__(256) k_sweep_pivot(long long n, int k0, int bk
       }
     }
   }
+}
+
+__global__ void __launch_bounds__(256) k_sweep_pivot(long long n, int k0, int bk, const double* __restrict__ A,
+                                                     double* __restrict__ P) {
+  __shared__ double s_row[2][kSweepB], s_col[2][kSweepB];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double R[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int i = ty + 16 * a, j = tx + 16 * b;
+      R[a][b] = (i < bk && j < bk) ? A[(k0 + i) * n + (k0 + j)] : (i == j ? 1.0 : 0.0);
+    }
+  sweep_pivot_regs(R, bk, s_row, s_col);
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
@@ -470,13 +604,21 @@ __global__ void __launch_bounds__(256) k_sweep_panel(long long n, int k0, int bk
 }
 
 // tile update of the lower 64x64 tiles (ti >= tj, one CTA each, 1-D grid),
-// 256 threads x (4x4) outputs, k in chunks of 32
+// 256 threads x (4x4) outputs, k in chunks of 32.  k1 >= 0: the CTA of the next
+// pivot tile (k1, k1) -- block 0, so it starts first -- goes on to sweep it in
+// registers and writes Pn = A_k1k1^-1 for the next step, behind the other tiles.
 __global__ void __launch_bounds__(256) k_sweep_update(long long n, int k0, int bk, double* __restrict__ A,
                                                       const double* __restrict__ P, const double* __restrict__ Rp,
-                                                      const double* __restrict__ U) {
+                                                      const double* __restrict__ U, int k1, double* __restrict__ Pn) {
   __shared__ double sL[32][65];  // A_iK for the tile rows: Rp[k][i]
   __shared__ double sU[32][65];  // U_Kj for the tile cols
-  const long long b = blockIdx.x;
+  __shared__ double s_row[2][kSweepB], s_col[2][kSweepB];
+  const long long ntiles = gridDim.x;
+  long long b = blockIdx.x;
+  if (k1 >= 0) {  // rotate the numbering so that block 0 is tile (k1/64, k1/64)
+    const long long t1 = k1 / 64;
+    b = (b + t1 * (t1 + 1) / 2 + t1) % ntiles;
+  }
   long long ti = (long long)((sqrt(8.0 * (double)b + 1.0) - 1.0) * 0.5);
   while (ti * (ti + 1) / 2 > b) --ti;
   while ((ti + 1) * (ti + 2) / 2 <= b) ++ti;
@@ -524,13 +666,33 @@ __global__ void __launch_bounds__(256) k_sweep_update(long long n, int k0, int b
         for (int b = 0; b < 4; ++b) acc[a][b] = fma(l[a], u[b], acc[a][b]);
     }
   }
+  const bool pivot_next = k1 >= 0 && i0 == k1 && j0 == k1;
+  const int bk1 = (int)std::min<long long>(kSweepB, n - k1);
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int b = 0; b < 4; ++b) {
       const long long i = i0 + ty + 16 * a, j = j0 + tx + 16 * b;
-      if (i < n && j < n) A[i * n + j] -= acc[a][b];
+      if (i < n && j < n) {
+        const double v = A[i * n + j] - acc[a][b];
+        A[i * n + j] = v;
+        acc[a][b] = v;
+      }
     }
+  if (!pivot_next) return;
+  // the next pivot block, as k_sweep_pivot would load it (identity padding)
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int i = ty + 16 * a, j = tx + 16 * b;
+      if (!(i < bk1 && j < bk1)) acc[a][b] = (i == j) ? 1.0 : 0.0;
+    }
+  sweep_pivot_regs(acc, bk1, s_row, s_col);
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) Pn[(ty + 16 * a) * kSweepB + tx + 16 * b] = -acc[a][b];
 }
 
 // E^-1 = -A: negate the lower tiles (diagonal tiles in full) and mirror them
@@ -759,6 +921,53 @@ __global__ void __launch_bounds__(kRkThreads, sizeof(T) == 4 ? 6 : 4) k_restrict
   if (threadIdx.x == 0) gcount[G] = 0;
 }
 
+// mu = Einv v for a compact coarse vector v (nc entries, nc even): one warp per row,
+// 16-byte loads in batches of 8 per lane, double-buffered so that the next batch is
+// in flight while the current one is consumed (v through the read-only cache);
+// 4 warps per CTA, all rows resident in one wave at the coarse sizes used.
+constexpr int kGemvBatch = 8;
+__global__ void __launch_bounds__(128) k_gemv_rows(long long nc, const double* __restrict__ Einv,
+                                                   const double* __restrict__ v, double* __restrict__ mu,
+                                                   const KrylovState* S) {
+  if (S && S->done) return;
+  const int lane = threadIdx.x & 31;
+  const long long row = 4 * (long long)blockIdx.x + (threadIdx.x >> 5);
+  if (row >= nc) return;
+  const int h = (int)(nc >> 1);
+  const double2* a2p = reinterpret_cast<const double2*>(Einv + row * nc);
+  const double2* v2 = reinterpret_cast<const double2*>(v);
+  double2 e[2][kGemvBatch];
+  auto load = [&](int jb, double2 (&d)[kGemvBatch]) {
+#pragma unroll
+    for (int k = 0; k < kGemvBatch; ++k)
+      if (jb + 32 * k < h) d[k] = __ldg(a2p + jb + 32 * k);
+  };
+  double a0 = 0.0, a1 = 0.0;
+  auto use = [&](int jb, const double2 (&d)[kGemvBatch]) {
+#pragma unroll
+    for (int k = 0; k < kGemvBatch; ++k)
+      if (jb + 32 * k < h) {
+        const double2 x = __ldg(v2 + jb + 32 * k);
+        a0 = fma(d[k].x, x.x, a0);
+        a1 = fma(d[k].y, x.y, a1);
+      }
+  };
+  constexpr int step = 32 * kGemvBatch;
+  int jb = lane;
+  load(jb, e[0]);
+  for (; jb < h; jb += 2 * step) {
+    if (jb + step < h) load(jb + step, e[1]);
+    use(jb, e[0]);
+    if (jb + step >= h) break;
+    if (jb + 2 * step < h) load(jb + 2 * step, e[0]);
+    use(jb + step, e[1]);
+  }
+  double acc = a0 + a1;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) mu[row] = acc;
+}
+
 // mu = Einv v for a compact coarse vector v (nc entries), one warp per row with
 // 16-byte loads (nc even) and four independent partial sums per lane.
 __global__ void __launch_bounds__(256) k_gemv(long long nc, const double* __restrict__ Einv,
@@ -773,20 +982,29 @@ __global__ void __launch_bounds__(256) k_gemv(long long nc, const double* __rest
     const double* a = Einv + row * nc;
     double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
     if ((nc & 1) == 0) {
+      // eight 16-byte loads per lane in flight (the kernel is bound by memory-level
+      // parallelism: one row per warp, a few warps per SM)
       const double2* a2p = reinterpret_cast<const double2*>(a);
-      const long long h = nc >> 1;
-      long long j = lane;
-      for (; j + 32 < h; j += 64) {
-        const double2 e0 = __ldg(a2p + j), e1 = __ldg(a2p + j + 32);
-        a0 = fma(e0.x, sv[2 * j], a0);
-        a1 = fma(e0.y, sv[2 * j + 1], a1);
-        a2 = fma(e1.x, sv[2 * j + 64], a2);
-        a3 = fma(e1.y, sv[2 * j + 65], a3);
+      const double2* v2 = reinterpret_cast<const double2*>(sv);
+      const int h = (int)(nc >> 1);
+      int j = lane;
+      for (; j + 7 * 32 < h; j += 8 * 32) {
+        double2 e[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) e[k] = __ldg(a2p + j + 32 * k);
+#pragma unroll
+        for (int k = 0; k < 8; k += 2) {
+          const double2 x0 = v2[j + 32 * k], x1 = v2[j + 32 * (k + 1)];
+          a0 = fma(e[k].x, x0.x, a0);
+          a1 = fma(e[k].y, x0.y, a1);
+          a2 = fma(e[k + 1].x, x1.x, a2);
+          a3 = fma(e[k + 1].y, x1.y, a3);
+        }
       }
-      if (j < h) {
-        const double2 e0 = __ldg(a2p + j);
-        a0 = fma(e0.x, sv[2 * j], a0);
-        a1 = fma(e0.y, sv[2 * j + 1], a1);
+      for (; j < h; j += 32) {
+        const double2 e0 = __ldg(a2p + j), x0 = v2[j];
+        a0 = fma(e0.x, x0.x, a0);
+        a1 = fma(e0.y, x0.y, a1);
       }
     } else {
       for (long long j = lane; j < nc; j += 32) a0 = fma(__ldg(a + j), sv[j], a0);
@@ -1145,7 +1363,7 @@ static DpcgWs carve_dpcg(const pyto_operator_t* op, long long nc, void* ws, size
   W.gcount = cv.take<unsigned>((size_t)kMaxCoarse);
   W.cv = cv.take<double>(2 * (nc > 0 ? nc : 1));  // k_restrict_K writes 6 slots per group
   W.mu = cv.take<double>(nc > 0 ? nc : 1);
-  W.P = cv.take<double>(kSweepB * kSweepB);
+  W.P = cv.take<double>(2 * kSweepB * kSweepB);
   W.Rp = cv.take<double>(kSweepB * (nc > 0 ? nc : 1));
   W.U = cv.take<double>(kSweepB * (nc > 0 ? nc : 1));
   if (mixed) {
@@ -1213,9 +1431,13 @@ static int coarse_update_K(const pyto_operator_t* op, const GridDims& g, const D
                                                   d->bel_ptr, d->bel_list, W.cptr, W.cgrp, z, W.rpart, W.gcount,
                                                   W.cv, S);
   PYTO_COUNT(1);
-  const size_t shm = (size_t)dp.nc * sizeof(double);
-  const int nb = (int)std::min<long long>((dp.nc + 7) / 8, 8 * kNumSMs);
-  k_gemv<<<nb, 256, shm, st>>>(dp.nc, d->coarse_inv, W.cv, W.mu, first ? nullptr : S);
+  if ((dp.nc & 1) == 0) {
+    k_gemv_rows<<<(int)((dp.nc + 3) / 4), 128, 0, st>>>(dp.nc, d->coarse_inv, W.cv, W.mu, first ? nullptr : S);
+  } else {
+    const size_t shm = (size_t)dp.nc * sizeof(double);
+    const int nb = (int)std::min<long long>((dp.nc + 7) / 8, 8 * kNumSMs);
+    k_gemv<<<nb, 256, shm, st>>>(dp.nc, d->coarse_inv, W.cv, W.mu, first ? nullptr : S);
+  }
   PYTO_COUNT(1);
   k_dpcg_update2<T><<<kNodeBlocks, kNodeThreads, 0, st>>>(g, dp, d->node_group, d->group_center, W.mu, W.fl, z, p,
                                                           S, first);
@@ -1286,9 +1508,25 @@ static int dpcg_setup_launch(const pyto_operator_t* op, const double* s, const u
   PYTO_CUDA(cudaMemsetAsync(E, 0, (size_t)n * n * sizeof(double), st));
   const size_t shm = (size_t)defl->max_nbr * 36 * sizeof(double);
   if (nchunks > 0) {
-    k_coarse_rows2<<<nchunks, kCrThreads, shm, st>>>(g, make_khat(op), dp, s, mask, defl->node_group,
-                                                     defl->group_center, defl->bel_ptr, defl->bel_list, W.cptr,
-                                                     W.cgrp, defl->nbr_ptr, defl->nbr_list, E);
+    const size_t shm2 = shm + 64 * kCrThreads * sizeof(double);
+    static bool attr = false;
+    if (!attr) {
+      PYTO_CUDA(cudaFuncSetAttribute(k_coarse_rows2<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(64 * kCrThreads * sizeof(double) + 128 * 36 * sizeof(double))));
+      PYTO_CUDA(cudaFuncSetAttribute(k_coarse_rows2<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(64 * kCrThreads * sizeof(double) + 128 * 36 * sizeof(double))));
+      attr = true;
+    }
+    if (dp.modes == 6)
+      k_coarse_rows2<6><<<nchunks, kCrThreads, shm2, st>>>(g, make_khat(op), dp, s, mask, defl->node_group,
+                                                          defl->group_center, defl->bel_ptr, defl->bel_list, W.cptr,
+                                                          W.cgrp, defl->nbr_ptr, defl->nbr_list, E);
+    else
+      k_coarse_rows2<3><<<nchunks, kCrThreads, shm2, st>>>(g, make_khat(op), dp, s, mask, defl->node_group,
+                                                          defl->group_center, defl->bel_ptr, defl->bel_list, W.cptr,
+                                                          W.cgrp, defl->nbr_ptr, defl->nbr_list, E);
+    PYTO_COUNT(1);
+    k_mirror_upper<<<(int)std::min<long long>((n * n + 255) / 256, 8 * kNumSMs), 256, 0, st>>>(n, dp.modes, E);
     PYTO_COUNT(1);
   } else {
     k_coarse_rows<<<dp.ngroups, kAsmThreads, shm, st>>>(g, make_khat(op), dp, s, mask, defl->node_group,
@@ -1305,13 +1543,20 @@ static int dpcg_setup_launch(const pyto_operator_t* op, const double* s, const u
   PYTO_COUNT(1);
   PYTO_LAUNCH_CHECK();
   const int tiles = (int)((n + 63) / 64);
-  for (long long k0 = 0; k0 < n; k0 += kSweepB) {
+  // pivot block inverses alternate between two buffers: the update of step K sweeps
+  // the pivot block of step K+1 into the other one
+  k_sweep_pivot<<<1, 256, 0, st>>>(n, 0, (int)std::min<long long>(kSweepB, n), E, W.P);
+  PYTO_COUNT(1);
+  int step = 0;
+  for (long long k0 = 0; k0 < n; k0 += kSweepB, ++step) {
     const int bk = (int)std::min<long long>(kSweepB, n - k0);
-    k_sweep_pivot<<<1, 256, 0, st>>>(n, (int)k0, bk, E, W.P);
+    double* Pc = W.P + (step & 1) * kSweepB * kSweepB;
+    double* Pn = W.P + ((step + 1) & 1) * kSweepB * kSweepB;
+    const long long k1 = k0 + kSweepB < n ? k0 + kSweepB : -1;
+    k_sweep_panel<<<(int)((n + 15) / 16), 256, 0, st>>>(n, (int)k0, bk, E, Pc, W.Rp, W.U);
     PYTO_COUNT(1);
-    k_sweep_panel<<<(int)((n + 15) / 16), 256, 0, st>>>(n, (int)k0, bk, E, W.P, W.Rp, W.U);
-    PYTO_COUNT(1);
-    k_sweep_update<<<(int)((long long)tiles * (tiles + 1) / 2), 256, 0, st>>>(n, (int)k0, bk, E, W.P, W.Rp, W.U);
+    k_sweep_update<<<(int)((long long)tiles * (tiles + 1) / 2), 256, 0, st>>>(n, (int)k0, bk, E, Pc, W.Rp, W.U,
+                                                                             (int)k1, Pn);
     PYTO_COUNT(1);
   }
   k_negate_sym<<<(int)std::min<long long>((n * n + 255) / 256, 8 * kNumSMs), 256, 0, st>>>(n, E);
@@ -1458,7 +1703,7 @@ static int dpcg_run(const pyto_operator_t* op, const T* s, const uint8_t* mask, 
     int e;
     for (int k = 0; k < every; ++k) {
       if ((e = matvec_t(op, s, mask, V.p, V.q, W.part, W.counter, &W.S->pq, cs))) return e;
-      k_dpcg_update1<T><<<kNodeBlocks, kNodeThreads, 0, cs>>>(g, pc, W.w, W.fl, u, V.r, V.z, V.p, V.q, W.S, W.part,
+      k_dpcg_update1<T><<<kUpdate1Blocks, kNodeThreads, 0, cs>>>(g, pc, W.w, W.fl, u, V.r, V.z, V.p, V.q, W.S, W.part,
                                                               W.counter);
       PYTO_COUNT(1);
       // mu = Einv W^T K z (from the boundary lists, or K z -> q then W^T q), p = z + beta p - W mu
@@ -1714,7 +1959,7 @@ static int dpcg_reliable(const pyto_operator_t* op, const double* s, const uint8
     int e;
     for (int k = 0; k < every; ++k) {
       if ((e = matvec_t(op, sT, mask, p, q, W.part, W.counter, &W.S->pq, cs))) return e;
-      k_dpcg_update1<T><<<kNodeBlocks, kNodeThreads, 0, cs>>>(g, pc, W.w, W.fl, x, r, z, p, q, W.S, W.part,
+      k_dpcg_update1<T><<<kUpdate1Blocks, kNodeThreads, 0, cs>>>(g, pc, W.w, W.fl, x, r, z, p, q, W.S, W.part,
                                                               W.counter);
       PYTO_COUNT(1);
       if (lists) {
@@ -1917,7 +2162,7 @@ static int batch_branch(const pyto_batch_item_t& it, const pyto_solve_cfg_t* cfg
   int brc = launch_matvec64(op, it.s, it.mask, W.p, W.q, PYTO_MASK_OUT, W.part, W.counter, &W.S->pq,  // p: masked
                             sb);
   if (!brc) {
-    k_dpcg_update1<double><<<kNodeBlocks, kNodeThreads, 0, sb>>>(g, pc, W.w, W.fl, it.u, W.r, W.z, W.p, W.q, W.S,
+    k_dpcg_update1<double><<<kUpdate1Blocks, kNodeThreads, 0, sb>>>(g, pc, W.w, W.fl, it.u, W.r, W.z, W.p, W.q, W.S,
                                                                 W.part, W.counter);
     PYTO_COUNT(1);
     brc = coarse_update_K(op, g, dp, defl, it.s, (const double*)W.z, W.p, W, nchunks, W.S, 0, sb);

@@ -8,6 +8,9 @@ namespace pyto {
 constexpr int kNodeBlocks = 16 * kNumSMs;  // grid of node-wise kernels (grid-stride; 3 partials each fit the
                                            // 4 * reduce_slots partial array)
 constexpr int kNodeThreads = 256;
+// grid of the deflated-PCG update1 (a streaming kernel): resident at once (4 CTAs of
+// 256 threads per SM at <= 64 registers); threads loop over the data
+constexpr int kUpdate1Blocks = 4 * kNumSMs;
 
 struct KrylovState {
   double rz, rz0, pq, rr, bb, alpha, beta, rtol;

@@ -232,6 +232,37 @@ def test_dpcg_coarse_spaces_converge(modes, agg):
     assert info.iters < info2.iters
 
 
+@pytest.mark.parametrize("modes,lists,ngroups", [(6, True, 24), (6, False, 24), (3, True, 40), (6, True, 60)])
+def test_coarse_inverse_matches_oracle(modes, lists, ngroups):
+    """The coarse inverse written by the set-up equals inv(W_f^T K_ff W_f + shift I)
+    (src/deflation.py:517-521) for both assembly paths (boundary lists: half the
+    blocks plus the mirror; full element sweep) and coarse sizes of one to several
+    64-wide pivot blocks."""
+    from pyto_b200.engine import DeviceDeflation
+    nel = (24, 12, 12)
+    m = O.grid_mesh(*nel)
+    f, fixed = O.cantilever_bc(m)
+    g = _grid(nel, fixed=fixed)
+    rng = np.random.default_rng(21)
+    s, _ = g.simp(_dev(rng.uniform(0.05, 1.0, m["num_elems"])), 3.0, 1e-9)
+    grp, cnt, cen = O.deflation_groups(m["node_xyz"], ngroups)
+    shift = 1e-6
+    defl = DeviceDeflation(g, grp, cen, modes=modes, shift=shift, shift_relative=False)
+    defl.use_boundary_lists = lists
+    g.dpcg_setup(s, defl)
+    nc = defl.nc
+    Einv = defl.coarse_inv.view(nc, nc).cpu().numpy()
+    K = O.assemble_K(m, s.cpu().numpy(), O.ke_hex8(1.0, 0.3))
+    free = np.setdiff1d(np.arange(3 * m["num_nodes"]), fixed)
+    W = O.deflation_W(m["node_xyz"], grp, cen, len(cnt), modes)[free]
+    E = (W.T @ (K[free][:, free] @ W)).toarray()
+    E = (E + E.T) / 2 + shift * np.eye(nc)
+    assert nc == E.shape[0] and nc > 64
+    np.testing.assert_allclose(Einv, Einv.T, rtol=0, atol=1e-12 * np.abs(Einv).max())
+    err = np.abs(Einv @ E - np.eye(nc)).max()
+    assert err <= 1e-9, err
+
+
 @pytest.mark.parametrize("nel,lshape", [((32, 16, 16), False), ((24, 8, 16), True)])
 def test_dpcg_boundary_restriction_matches_full(nel, lshape):
     """W_f^T K z from the group-boundary element lists equals the restriction of a
