@@ -32,10 +32,12 @@ sys.path.insert(0, ROOT)
 METRIC = "time to rel-residual 1e-8 per 5.4M-DOF solve, mixed vs FP64 GPU; % HBM roofline"
 NEL = (192, 96, 96)
 RTOL = 1e-8
-# DRAM bytes (read + write) of one K(s)u launch on this grid, from an ncu capture
-# of the matvec kernel (profiles/k_matvec_192x96x96.md: cold caches, so the y writes, which
-# stay in L2 during the launch, are not counted)
-TRAFFIC = {"f32": 30750464, "f64": 71395328}
+# DRAM bytes (read + write) of one K(s)u launch on this grid in the solver's mask mode
+# (output mask only), from ncu captures of the two operator kernels (profiles/
+# k_matvec_192x96x96.md; cold caches, so the y writes, which stay in L2 during the
+# launch, are mostly not counted)
+TRAFFIC = {"f32": 30762240, "f64": 71395328}
+KERNEL = {"f32": "k_matvec_chunked<float> (chunk-staged, variant 8)", "f64": "k_matvec<double> (tile, variant 2)"}
 
 
 def peaks():
@@ -149,16 +151,19 @@ def time_solves(P, form, steps, device):
 
 def time_matvec(P, reps=30, precision="f64"):
     """Average duration of the matrix-free K(s)u kernel on the bench grid (FP64 or
-    FP32), CUDA events on the launching (current torch) stream."""
+    FP32) in the mask mode of the solver's iterations (output mask only: the search
+    directions are zero on fixed DOFs), CUDA events on the launching (current torch)
+    stream."""
     import torch
+    from pyto_b200 import _capi as A
     g = P["grid"]
     s, _ = g.simp(P["rho"], 3.0, 1e-9, want_ds=False)
     u = torch.randn(g.ndof, dtype=torch.float64, device=g.device)
     if precision == "f32":
         s, u = s.float(), u.float()
-        fn = lambda y: g.matvec_f32(s, u, out=y)
+        fn = lambda y: g.matvec_f32(s, u, mode=A.MASK_OUT, out=y)
     else:
-        fn = lambda y: g.matvec(s, u, out=y)
+        fn = lambda y: g.matvec(s, u, mode=A.MASK_OUT, out=y)
     y = torch.empty_like(u)
     for _ in range(3):
         fn(y)
@@ -329,8 +334,7 @@ def main():
         t_mv = time_matvec(P, precision=prec)
         nbytes = 2 * 3 * vb * g.nnodes + vb * g.nelem + g.nnodes
         ach = nbytes / t_mv / 1e9
-        rl[prec] = {"bound": "hbm", "kernel": f"k_matvec<{'float' if prec == 'f32' else 'double'}> "
-                                              f"(matrix-free K(s)u)",
+        rl[prec] = {"bound": "hbm", "kernel": KERNEL[prec] + " matrix-free K(s)u",
                     "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak, "peak_kind": peak_kind,
                     "traffic": TRAFFIC.get(prec), "launch_ms": t_mv * 1e3, "algorithmic_bytes": int(nbytes)}
     main_prec = "f32" if args.form == "mixed" else "f64"

@@ -91,12 +91,13 @@ class HexStructuralFEA:
         return _np(u) if to_np else u
 
     def _force_device(self):
-        """bc.force on the device, copied once per force array (a new array, or a rebound
-        bc.force, is copied again; modify the force by assigning a new array)."""
+        """bc.force on the device.  Copied at every solve, as the reference reads it
+        (an in-place change between solves is seen); a read-only numpy array, which
+        cannot change in place, is copied once and kept on the device."""
         f = self.bc.force
-        if isinstance(f, torch.Tensor):
+        if isinstance(f, torch.Tensor) or not isinstance(f, np.ndarray) or f.flags.writeable:
             return self.grid.tensor(f)
-        key = (id(f), f.__array_interface__["data"][0] if hasattr(f, "__array_interface__") else None)
+        key = (id(f), f.__array_interface__["data"][0])
         if getattr(self, "_force_key", None) != key:
             self._force_dev = self.grid.tensor(f)
             self._force_key = key

@@ -51,6 +51,7 @@ def main(argv=None):
     ap.add_argument("--variant32", type=int, default=None, help="FP32 matvec tile variant (pyto_tune)")
     ap.add_argument("--delta", type=float, default=1e-1, help="reliable-update threshold for --kernel mixed")
     ap.add_argument("--mode", type=int, default=3, help="--kernel matvec/matvec32: BC mask mode (1 in, 2 out)")
+    ap.add_argument("--stop-rule", type=int, default=0, choices=[0, 1, 2], help="--kernel dpcg: stopping rule")
     a = ap.parse_args(argv)
     if a.kernel == "batch":
         return batch_bench(a)
@@ -89,7 +90,7 @@ def main(argv=None):
             ds.create_deflation_groups(mesh, a.groups)
             defl = ds.device_deflation(g)
             if a.kernel == "dpcg":
-                fn = lambda: g.dpcg(s, F, defl, rtol=1e-8, max_iters=5000, stop_rule=0, check_every=20)
+                fn = lambda: g.dpcg(s, F, defl, rtol=1e-8, max_iters=5000, stop_rule=a.stop_rule, check_every=20)
             else:
                 fn = lambda: g.dpcg_mixed(s, F, defl, rtol=1e-8, delta=a.delta, max_iters=8000,
                                           check_every=20)
@@ -121,6 +122,7 @@ def oc_bench(a):
     mesh = HexMesher()
     mesh.grid_mesh(nel, (1.0, 1.0, 1.0))
     f, fixed = cantilever(mesh)
+    f.flags.writeable = False  # a constant load: the FEA keeps its device copy
     bc = bound_cond.BC(force=f, fixed_dofs=fixed, dirichlet_values=np.zeros(len(fixed)))
     mat = mat_lib.create_material_with_defaults("unit", youngs_modulus=1.0, poissons_ratio=0.3)
     ds = DeflationSolver(modes=6, shift=1e-14, shift_relative=True)

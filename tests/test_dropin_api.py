@@ -45,6 +45,24 @@ def test_fea_solve_compliance_gradient(solver_name):
     np.testing.assert_allclose(dC, d["dC"], rtol=1e-8, atol=1e-11 * np.abs(d["dC"]).max())
 
 
+def test_force_changes_between_solves_are_seen():
+    """As in the reference, every solve reads bc.force: an in-place change between two
+    solves changes the displacement (linearly); a read-only load is kept on the device."""
+    from pyto_b200.topopt_material_model import MaterialModel
+    d = golden("cantilever_12x6x6_direct.npz")
+    m, fe = _setup()
+    u1 = fe.solve(d["rho"], MaterialModel.SIMP).copy()
+    fe.bc.force *= 2.0  # in place
+    u2 = fe.solve(d["rho"], MaterialModel.SIMP)
+    np.testing.assert_allclose(u2, 2.0 * u1, rtol=0, atol=1e-9 * np.abs(u1).max())
+    fe.bc.force = fe.bc.force / 2.0
+    fe.bc.force.flags.writeable = False
+    u3 = fe.solve(d["rho"], MaterialModel.SIMP)
+    u4 = fe.solve(d["rho"], MaterialModel.SIMP)
+    np.testing.assert_allclose(u3, u1, rtol=0, atol=1e-9 * np.abs(u1).max())
+    np.testing.assert_array_equal(u3, u4)
+
+
 def test_postprocess_pnorm_and_adjoint():
     from pyto_b200 import topopt_obj_cons_sensitivities as toc
     from pyto_b200 import topopt_material_model as tmm
