@@ -116,6 +116,10 @@ typedef struct pyto_deflation {
    * lists must be rebuilt when the fixed DOFs change. */
   const int32_t* bel_ptr;      /* [ngroups+1] CSR offsets of bel_list */
   const int32_t* bel_list;     /* boundary elements of each group, ascending element ids */
+  /* Optional per-entry metadata of bel_list (NULL: derived on the fly from node_group and
+   * the mask): bits 0-7 = corner k of the entry's element lies in the entry's group,
+   * bit 8 = the element has a fixed DOF.  Rebuilt with the lists. */
+  const uint16_t* bel_meta;    /* [bel_count] */
 } pyto_deflation_t;
 
 /* ---- version / workspace ------------------------------------------------- */

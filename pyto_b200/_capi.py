@@ -57,7 +57,8 @@ class Deflation(C.Structure):
                 ("group_nodes", C.c_void_p), ("group_center", C.c_void_p), ("coarse_inv", C.c_void_p),
                 ("shift", C.c_double), ("shift_relative", C.c_int32), ("max_group_nodes", C.c_int32),
                 ("group_box", C.c_void_p), ("nbr_ptr", C.c_void_p), ("nbr_list", C.c_void_p), ("max_nbr", C.c_int32),
-                ("bel_count", C.c_int32), ("bel_ptr", C.c_void_p), ("bel_list", C.c_void_p)]
+                ("bel_count", C.c_int32), ("bel_ptr", C.c_void_p), ("bel_list", C.c_void_p),
+                ("bel_meta", C.c_void_p)]
 
 
 class BatchItem(C.Structure):

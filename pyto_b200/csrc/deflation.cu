@@ -858,6 +858,66 @@ __device__ __forceinline__ void rk_element(const GridDims& g, const KHat& kh, co
   for (int a = 0; a < 6; ++a) acc[a] += (double)em[a];
 }
 
+// a / d for 0 <= a < 2^31 from a double reciprocal (exact after the correction)
+__device__ __forceinline__ int div_by(int a, int d, double inv) {
+  int q = (int)((double)a * inv);
+  q -= (q * d > a);
+  q += ((q + 1) * d <= a);
+  return q;
+}
+
+// rk_element for an element without fixed DOFs whose corners in G are the bits of
+// cmask (from the list's per-entry metadata): no group or mask loads, no selects
+template <typename T>
+__device__ __forceinline__ void rk_element_free(const GridDims& g, const KHat& kh, const DeflP& dp, int e,
+                                                unsigned cmask, T se, double inx, double iny, double c0, double c1,
+                                                double c2, const T* __restrict__ z, double (&acc)[6]) {
+  const int r = div_by(e, g.nx, inx);
+  const int ex = e - r * g.nx;
+  const int ez = div_by(r, g.ny, iny);
+  const int ey = r - ez * g.ny;
+  const int n0 = ex + g.sx * (ey + g.sy * ez);
+  const int pn = g.sx * g.sy;
+  T u[3][8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const T* zn = z + 3 * (n0 + (k & 1) + g.sx * ((k >> 1) & 1) + pn * (k >> 2));
+#pragma unroll
+    for (int c = 0; c < 3; ++c) u[c][k] = zn[c];
+  }
+  T Fb[3][4], Ft[3][4], Gb[3][4], Gt[3][4];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    face_fwd(u[c][0], u[c][1], u[c][2], u[c][3], Fb[c]);
+    face_fwd(u[c][4], u[c][5], u[c][6], u[c][7], Ft[c]);
+#pragma unroll
+    for (int f = 0; f < 4; ++f) Gb[c][f] = Gt[c][f] = T(0);
+  }
+  hex8_core<T>(kh, se, Fb, Ft, Gb, Gt);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    face_inv(Gb[c], u[c][0], u[c][1], u[c][2], u[c][3]);
+    face_inv(Gt[c], u[c][4], u[c][5], u[c][6], u[c][7]);
+  }
+  const T bx = (T)(dp.hx * ex - c0), by = (T)(dp.hy * ey - c1), bz = (T)(dp.hz * ez - c2);
+  const T hx = (T)dp.hx, hy = (T)dp.hy, hz = (T)dp.hz;
+  T em[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const T in = ((cmask >> k) & 1) ? T(1) : T(0);
+    const T yx = in * u[0][k], yy = in * u[1][k], yz = in * u[2][k];
+    const T rx = (k & 1) ? bx + hx : bx, ry = ((k >> 1) & 1) ? by + hy : by, rz = (k >> 2) ? bz + hz : bz;
+    em[0] += yx;
+    em[1] += yy;
+    em[2] += yz;
+    em[3] += -rz * yy + ry * yz;
+    em[4] += rz * yx - rx * yz;
+    em[5] += -ry * yx + rx * yy;
+  }
+#pragma unroll
+  for (int a = 0; a < 6; ++a) acc[a] += (double)em[a];
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kRkThreads, sizeof(T) == 4 ? 6 : 4) k_restrict_K(GridDims g, KHat kh, DeflP dp, const T* __restrict__ s,
                                                            const uint8_t* __restrict__ fl,
@@ -868,7 +928,8 @@ __global__ void __launch_bounds__(kRkThreads, sizeof(T) == 4 ? 6 : 4) k_restrict
                                                            const int32_t* __restrict__ cptr,
                                                            const int32_t* __restrict__ cgrp, const T* __restrict__ z,
                                                            double* __restrict__ part, unsigned* __restrict__ gcount,
-                                                           double* __restrict__ v, const KrylovState* S) {
+                                                           double* __restrict__ v, const KrylovState* S,
+                                                           const uint16_t* __restrict__ meta) {
   __shared__ double sred[kRkThreads / 32 * 6];
   __shared__ int s_last;
   if (S && S->done) return;
@@ -884,8 +945,18 @@ __global__ void __launch_bounds__(kRkThreads, sizeof(T) == 4 ? 6 : 4) k_restrict
   const int e1 = t0 + kRkThreads < end ? blist[t0 + kRkThreads] : -1;
   const T s0 = e0 >= 0 ? s[e0] : T(0);
   const T s1 = e1 >= 0 ? s[e1] : T(0);
-  if (s0 != T(0)) rk_element<T>(g, kh, dp, e0, G, s0, fl, ngrp, c0, c1, c2, z, acc);
-  if (s1 != T(0)) rk_element<T>(g, kh, dp, e1, G, s1, fl, ngrp, c0, c1, c2, z, acc);
+  // bits 0-7 of an entry's metadata: its element's corners in G; bit 8: the element
+  // has a fixed DOF (general path)
+  const unsigned m0 = (meta && e0 >= 0) ? meta[t0] : 0x100u, m1 = (meta && e1 >= 0) ? meta[t0 + kRkThreads] : 0x100u;
+  const double inx = 1.0 / g.nx, iny = 1.0 / g.ny;
+  if (s0 != T(0)) {
+    if (m0 & 0x100u) rk_element<T>(g, kh, dp, e0, G, s0, fl, ngrp, c0, c1, c2, z, acc);
+    else rk_element_free<T>(g, kh, dp, e0, m0, s0, inx, iny, c0, c1, c2, z, acc);
+  }
+  if (s1 != T(0)) {
+    if (m1 & 0x100u) rk_element<T>(g, kh, dp, e1, G, s1, fl, ngrp, c0, c1, c2, z, acc);
+    else rk_element_free<T>(g, kh, dp, e1, m1, s1, inx, iny, c0, c1, c2, z, acc);
+  }
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
   for (int a = 0; a < 6; ++a) {
@@ -1429,7 +1500,7 @@ static int coarse_update_K(const pyto_operator_t* op, const GridDims& g, const D
                            int first, cudaStream_t st) {
   k_restrict_K<T><<<nchunks, kRkThreads, 0, st>>>(g, make_khat(op), dp, s, W.fl, d->node_group, d->group_center,
                                                   d->bel_ptr, d->bel_list, W.cptr, W.cgrp, z, W.rpart, W.gcount,
-                                                  W.cv, S);
+                                                  W.cv, S, d->bel_meta);
   PYTO_COUNT(1);
   if ((dp.nc & 1) == 0) {
     k_gemv_rows<<<(int)((dp.nc + 3) / 4), 128, 0, st>>>(dp.nc, d->coarse_inv, W.cv, W.mu, first ? nullptr : S);

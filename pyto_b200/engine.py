@@ -318,11 +318,12 @@ class DeviceDeflation:
         DOFs: elements with a corner in the group and a corner in another group or on a
         fixed DOF (W_f^T K z is formed from these elements only)."""
         if not self.use_boundary_lists:
-            self.struct.bel_ptr = self.struct.bel_list = None
+            self.struct.bel_ptr = self.struct.bel_list = self.struct.bel_meta = None
             self.struct.bel_count = 0
             return self
         if self.mask_version == grid.mask_version:
             self.struct.bel_ptr, self.struct.bel_list = A.ptr(self.bel_ptr), A.ptr(self.bel_list)
+            self.struct.bel_meta = A.ptr(self.bel_meta)
             self.struct.bel_count = int(self.bel_list.numel())
             return self
         mask = grid.mask[:grid.nnodes].cpu().numpy()
@@ -332,9 +333,16 @@ class DeviceDeflation:
         key = np.unique((cg * grid.nelem + el[:, None]).ravel())
         grp, elem = key // grid.nelem, key % grid.nelem
         bptr = np.concatenate([[0], np.cumsum(np.bincount(grp, minlength=self.ngroups))]).astype(np.int32)
+        # per entry: which corners of its element lie in its group (bits 0-7), and
+        # whether the element has a fixed DOF (bit 8)
+        rows = cg[np.searchsorted(el, elem)]
+        meta = ((rows == grp[:, None]).astype(np.uint16) << np.arange(8, dtype=np.uint16)).sum(1, dtype=np.uint16)
+        meta |= fixed_el[elem].astype(np.uint16) << 8
         self.bel_ptr = torch.as_tensor(bptr, device=grid.device)
         self.bel_list = torch.as_tensor(elem.astype(np.int32), device=grid.device)
+        self.bel_meta = torch.as_tensor(meta.astype(np.int16), device=grid.device)  # uint16 bits
         self.struct.bel_ptr, self.struct.bel_list = A.ptr(self.bel_ptr), A.ptr(self.bel_list)
+        self.struct.bel_meta = A.ptr(self.bel_meta)
         self.struct.bel_count = int(self.bel_list.numel())
         self.mask_version = grid.mask_version
         return self
