@@ -1412,6 +1412,7 @@ struct DpcgWs {
 constexpr long long kMaxCoarse = 24576;  // coarse vector staged in shared memory (192 KB)
 constexpr double kReliableDelta = 1e-2;  // FP64 residual replacement each time ||r|| drops 100-fold
 constexpr int kReliableSegment = 100;    // and at least every this many iterations
+constexpr int kReliablePoll = 20;        // replacement triggers tested at least this often
 constexpr int kMaxRestarts = 64;         // direction restarts before giving up
 
 static DpcgWs carve_dpcg(const pyto_operator_t* op, long long nc, void* ws, size_t bytes, size_t* need,
@@ -1719,18 +1720,19 @@ struct DVec {
 };
 
 int launch_matvec32(const pyto_operator_t* op, const float* s, const uint8_t* mask, const float* u, float* y,
-                    int mode, double* part, unsigned* counter, double* dot, cudaStream_t st);
+                    int mode, double* part, unsigned* counter, double* dot, cudaStream_t st,
+                    const int* stop = nullptr);
 
 // K(s) u for the iteration vectors p and z only: both are zero on fixed DOFs (z =
 // M^-1 r is, by jacobi_apply; p = z + beta p - W mu is, by update2_node), so the
 // input mask would select the same values and is skipped.
 static int matvec_t(const pyto_operator_t* op, const double* s, const uint8_t* mask, const double* u, double* y,
-                    double* part, unsigned* counter, double* dot, cudaStream_t st) {
-  return launch_matvec64(op, s, mask, u, y, PYTO_MASK_OUT, part, counter, dot, st);
+                    double* part, unsigned* counter, double* dot, cudaStream_t st, const int* stop = nullptr) {
+  return launch_matvec64(op, s, mask, u, y, PYTO_MASK_OUT, part, counter, dot, st, stop);
 }
 static int matvec_t(const pyto_operator_t* op, const float* s, const uint8_t* mask, const float* u, float* y,
-                    double* part, unsigned* counter, double* dot, cudaStream_t st) {
-  return launch_matvec32(op, s, mask, u, y, PYTO_MASK_OUT, part, counter, dot, st);
+                    double* part, unsigned* counter, double* dot, cudaStream_t st, const int* stop = nullptr) {
+  return launch_matvec32(op, s, mask, u, y, PYTO_MASK_OUT, part, counter, dot, st, stop);
 }
 
 // One deflated PCG run (src/deflation.py:504-584) in vector precision T;
@@ -1773,7 +1775,7 @@ static int dpcg_run(const pyto_operator_t* op, const T* s, const uint8_t* mask, 
   auto chunk = [&](cudaStream_t cs) -> int {
     int e;
     for (int k = 0; k < every; ++k) {
-      if ((e = matvec_t(op, s, mask, V.p, V.q, W.part, W.counter, &W.S->pq, cs))) return e;
+      if ((e = matvec_t(op, s, mask, V.p, V.q, W.part, W.counter, &W.S->pq, cs, &W.S->done))) return e;
       k_dpcg_update1<T><<<kUpdate1Blocks, kNodeThreads, 0, cs>>>(g, pc, W.w, W.fl, u, V.r, V.z, V.p, V.q, W.S, W.part,
                                                               W.counter);
       PYTO_COUNT(1);
@@ -1941,7 +1943,7 @@ static int dpcg_reliable(const pyto_operator_t* op, const double* s, const uint8
   const Prec pc = make_prec(op);
   const long long nd = 3 * g.nnodes;
   const int nb = (int)std::min<long long>((nd + 255) / 256, 8 * kNumSMs);
-  const int every = std::max(1, cfg->check_every);
+  int every = std::max(1, cfg->check_every);
   T* r = RelVec<T>::r(W);
   T* p = RelVec<T>::p(W);
   T* q = RelVec<T>::q(W);
@@ -2022,6 +2024,10 @@ static int dpcg_reliable(const pyto_operator_t* op, const double* s, const uint8
   KrylovState hs{};
   PYTO_CUDA(cudaMemcpyAsync(&hs, W.S, sizeof(hs), cudaMemcpyDeviceToHost, st));
   PYTO_CUDA(cudaStreamSynchronize(st));
+  // the replacement triggers are tested between chunks: at most kReliablePoll
+  // iterations apart whatever the caller's polling interval (a longer unreplaced
+  // run of the low-precision recurrence loses the accuracy the replacement restores)
+  every = std::min(every, kReliablePoll);
   double rr_ref = hs.rr;
   double true_prev = hs.true_rr;  // true ||r||^2 at the previous update
   int updates = 1, restarts = 0, seg0 = 0;
@@ -2029,7 +2035,7 @@ static int dpcg_reliable(const pyto_operator_t* op, const double* s, const uint8
   auto chunk = [&](cudaStream_t cs) -> int {
     int e;
     for (int k = 0; k < every; ++k) {
-      if ((e = matvec_t(op, sT, mask, p, q, W.part, W.counter, &W.S->pq, cs))) return e;
+      if ((e = matvec_t(op, sT, mask, p, q, W.part, W.counter, &W.S->pq, cs, &W.S->done))) return e;
       k_dpcg_update1<T><<<kUpdate1Blocks, kNodeThreads, 0, cs>>>(g, pc, W.w, W.fl, x, r, z, p, q, W.S, W.part,
                                                               W.counter);
       PYTO_COUNT(1);

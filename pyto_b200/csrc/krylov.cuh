@@ -117,8 +117,11 @@ __device__ __forceinline__ void ld_quad_node(const double* w, const uint8_t* fl,
   f4 = __ldg(reinterpret_cast<const unsigned*>(fl + 4 * t));
 }
 
+// stop (optional): the solver's done flag; the launch does nothing once it is set
+// (the operator launch of an iteration past convergence)
 int launch_matvec64(const pyto_operator_t* op, const double* s, const uint8_t* mask, const double* u, double* y,
-                    int mode, double* part, unsigned* counter, double* dot, cudaStream_t st);
+                    int mode, double* part, unsigned* counter, double* dot, cudaStream_t st,
+                    const int* stop = nullptr);
 long long matvec_blocks(const pyto_operator_t* op);
 size_t reduce_slots(const pyto_operator_t* op);
 

@@ -110,8 +110,9 @@ template <typename T, int TY, bool DOT, bool MASKIN, int MINB, bool TC = false>
 __global__ void __launch_bounds__(32 * TY, MINB)
     k_matvec(GridDims g, KHat kh, const T* __restrict__ s, const uint8_t* __restrict__ mask,
              const T* __restrict__ u, T* __restrict__ y, int zc, int mode, double* part, unsigned* counter,
-             double* dot_out) {
+             double* dot_out, const int* stop) {
   static_assert(!TC || sizeof(T) == 4, "the tensor-core element core is the FP32 operator's");
+  if (stop && *stop) return;  // the solver's state is done: an iteration past convergence
   using M = MvSmem<T, TY, TC>;
   constexpr int TX = M::TX, NT = M::NT, PX = M::PX, PLANE = M::PLANE;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -481,7 +482,7 @@ __global__ void __launch_bounds__(32 * TY, MINB)
 template <typename T, int TY, bool DOT, bool MI, int MINB, bool TC = false>
 static int launch_mv_t(const MvLaunch& L, size_t smem, const GridDims& g, const KHat& kh, const T* s,
                        const uint8_t* mask, const T* u, T* y, int mode, double* part, unsigned* counter, double* dot,
-                       cudaStream_t st) {
+                       cudaStream_t st, const int* stop) {
   static bool attr = false;
   if (!attr) {
     PYTO_CUDA(cudaFuncSetAttribute(k_matvec<T, TY, DOT, MI, MINB, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -489,7 +490,7 @@ static int launch_mv_t(const MvLaunch& L, size_t smem, const GridDims& g, const 
     attr = true;
   }
   k_matvec<T, TY, DOT, MI, MINB, TC><<<L.grid, 32 * TY, smem, st>>>(g, kh, s, mask, u, y, L.zc, mode, part, counter,
-                                                                    dot);
+                                                                    dot, stop);
   PYTO_COUNT(1);
   PYTO_LAUNCH_CHECK();
   return PYTO_OK;
@@ -497,23 +498,25 @@ static int launch_mv_t(const MvLaunch& L, size_t smem, const GridDims& g, const 
 
 template <typename T, int TY, int MINB, bool TC = false>
 static int launch_mv(const GridDims& g, const KHat& kh, const T* s, const uint8_t* mask, const T* u, T* y, int mode,
-                     double* part, unsigned* counter, double* dot, cudaStream_t st) {
+                     double* part, unsigned* counter, double* dot, cudaStream_t st, const int* stop = nullptr) {
   const size_t smem = MvSmem<T, TY, TC>::bytes;
   const MvLaunch L = matvec_launch<32, TY>(g);
   const bool mi = (mode & PYTO_MASK_IN) && mask != nullptr;
   if (dot)
-    return mi ? launch_mv_t<T, TY, true, true, MINB, TC>(L, smem, g, kh, s, mask, u, y, mode, part, counter, dot, st)
+    return mi ? launch_mv_t<T, TY, true, true, MINB, TC>(L, smem, g, kh, s, mask, u, y, mode, part, counter, dot, st,
+                                                         stop)
               : launch_mv_t<T, TY, true, false, MINB, TC>(L, smem, g, kh, s, mask, u, y, mode, part, counter, dot,
-                                                           st);
+                                                           st, stop);
   return mi ? launch_mv_t<T, TY, false, true, MINB, TC>(L, smem, g, kh, s, mask, u, y, mode, nullptr, nullptr,
-                                                        nullptr, st)
+                                                        nullptr, st, stop)
             : launch_mv_t<T, TY, false, false, MINB, TC>(L, smem, g, kh, s, mask, u, y, mode, nullptr, nullptr,
-                                                         nullptr, st);
+                                                         nullptr, st, stop);
 }
 
 template <typename T, int TY, bool DOT, bool MI, int MINB, bool GS, bool RF>
 static int launch_mvc_t(const MvLaunch& L, const GridDims& g, const KHatT<T>& kh, const T* s, const uint8_t* mask,
-                        const T* u, T* y, int mode, double* part, unsigned* counter, double* dot, cudaStream_t st) {
+                        const T* u, T* y, int mode, double* part, unsigned* counter, double* dot, cudaStream_t st,
+                        const int* stop) {
   constexpr size_t smem = ChunkTile<T, TY, GS>::bytes;
   static bool attr = false;
   if (!attr) {
@@ -522,7 +525,7 @@ static int launch_mvc_t(const MvLaunch& L, const GridDims& g, const KHatT<T>& kh
     attr = true;
   }
   k_matvec_chunked<T, TY, DOT, MI, MINB, GS, RF><<<L.grid, 32 * TY, smem, st>>>(g, kh, s, mask, u, y, L.zc, mode, part,
-                                                                        counter, dot);
+                                                                        counter, dot, stop);
   PYTO_COUNT(1);
   PYTO_LAUNCH_CHECK();
   return PYTO_OK;
@@ -531,19 +534,19 @@ static int launch_mvc_t(const MvLaunch& L, const GridDims& g, const KHatT<T>& kh
 // chunk-staged kernel; u and the mask must be 16-byte aligned, else k_matvec (same results)
 template <typename T, int TY, int MINB, bool GS = false, bool RF = false>
 static int launch_mvc(const GridDims& g, const KHat& kh, const T* s, const uint8_t* mask, const T* u, T* y, int mode,
-                      double* part, unsigned* counter, double* dot, cudaStream_t st) {
+                      double* part, unsigned* counter, double* dot, cudaStream_t st, const int* stop) {
   if (((uintptr_t)u & 15) || ((uintptr_t)mask & 15))
-    return launch_mv<T, TY, MINB>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
+    return launch_mv<T, TY, MINB>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
   const MvLaunch L = matvec_launch<32, TY>(g);
   const KHatT<T> kt = make_khat_t<T>(kh);
   const bool mi = (mode & PYTO_MASK_IN) && mask != nullptr;
   if (dot)
-    return mi ? launch_mvc_t<T, TY, true, true, MINB, GS, RF>(L, g, kt, s, mask, u, y, mode, part, counter, dot, st)
-              : launch_mvc_t<T, TY, true, false, MINB, GS, RF>(L, g, kt, s, mask, u, y, mode, part, counter, dot, st);
+    return mi ? launch_mvc_t<T, TY, true, true, MINB, GS, RF>(L, g, kt, s, mask, u, y, mode, part, counter, dot, st, stop)
+              : launch_mvc_t<T, TY, true, false, MINB, GS, RF>(L, g, kt, s, mask, u, y, mode, part, counter, dot, st, stop);
   return mi ? launch_mvc_t<T, TY, false, true, MINB, GS, RF>(L, g, kt, s, mask, u, y, mode, nullptr, nullptr, nullptr,
-                                                         st)
+                                                         st, stop)
             : launch_mvc_t<T, TY, false, false, MINB, GS, RF>(L, g, kt, s, mask, u, y, mode, nullptr, nullptr, nullptr,
-                                                          st);
+                                                          st, stop);
 }
 
 // Tile variant of the FP64 matvec (2 = default: fastest measured at 192x96x96):
@@ -556,37 +559,39 @@ static int g_mv_variant = 2;
 static int g_mv32_variant = 8;
 
 int launch_matvec64(const pyto_operator_t* op, const double* s, const uint8_t* mask, const double* u, double* y,
-                    int mode, double* part, unsigned* counter, double* dot, cudaStream_t st) {
+                    int mode, double* part, unsigned* counter, double* dot, cudaStream_t st,
+                    const int* stop = nullptr) {
   const GridDims g = make_dims(op);
   const KHat kh = make_khat(op);
   const int tv = (op->tune & 0xff) - 1;  // per-grid choice of the autotuner, else the library default
   switch ((tv >= 0 && tv <= 3) || (tv >= 8 && tv <= 10) ? tv : g_mv_variant) {
-    case 8: return launch_mvc<double, 4, 3, true, true>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
-    case 9: return launch_mvc<double, 8, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
-    case 10: return launch_mvc<double, 4, 2>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
-    case 1: return launch_mv<double, 8, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
-    case 2: return launch_mv<double, 4, 3>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
-    case 3: return launch_mv<double, 16, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
-    default: return launch_mv<double, 8, 2>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
+    case 8: return launch_mvc<double, 4, 3, true, true>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
+    case 9: return launch_mvc<double, 8, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
+    case 10: return launch_mvc<double, 4, 2>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
+    case 1: return launch_mv<double, 8, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
+    case 2: return launch_mv<double, 4, 3>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
+    case 3: return launch_mv<double, 16, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
+    default: return launch_mv<double, 8, 2>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
   }
 }
 
 int launch_matvec32(const pyto_operator_t* op, const float* s, const uint8_t* mask, const float* u, float* y,
-                    int mode, double* part, unsigned* counter, double* dot, cudaStream_t st) {
+                    int mode, double* part, unsigned* counter, double* dot, cudaStream_t st,
+                    const int* stop = nullptr) {
   const GridDims g = make_dims(op);
   const KHat kh = make_khat(op);
   const int tv = ((op->tune >> 8) & 0xff) - 1;
   switch ((tv >= 0 && tv <= 5) || (tv >= 8 && tv <= 11) ? tv : g_mv32_variant) {
-    case 8: return launch_mvc<float, 8, 3>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
-    case 9: return launch_mvc<float, 8, 2>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
-    case 10: return launch_mvc<float, 4, 6>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
-    case 11: return launch_mvc<float, 16, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
-    case 1: return launch_mv<float, 8, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
-    case 2: return launch_mv<float, 4, 3>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
-    case 3: return launch_mv<float, 16, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
-    case 4: return launch_mv<float, 8, 2, true>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
-    case 5: return launch_mv<float, 4, 3, true>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
-    default: return launch_mv<float, 8, 2>(g, kh, s, mask, u, y, mode, part, counter, dot, st);
+    case 8: return launch_mvc<float, 8, 3>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
+    case 9: return launch_mvc<float, 8, 2>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
+    case 10: return launch_mvc<float, 4, 6>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
+    case 11: return launch_mvc<float, 16, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
+    case 1: return launch_mv<float, 8, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
+    case 2: return launch_mv<float, 4, 3>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
+    case 3: return launch_mv<float, 16, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
+    case 4: return launch_mv<float, 8, 2, true>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
+    case 5: return launch_mv<float, 4, 3, true>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
+    default: return launch_mv<float, 8, 2>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
   }
 }
 

@@ -85,7 +85,8 @@ template <typename T, int TY, bool DOT, bool MASKIN, int MINB, bool GS = false, 
 __global__ void __launch_bounds__(32 * TY, MINB)
     k_matvec_chunked(GridDims g, KHatT<T> kh, const T* __restrict__ s, const uint8_t* __restrict__ mask,
                      const T* __restrict__ u, T* __restrict__ y, int zc, int mode, double* part, unsigned* counter,
-                     double* dot_out) {
+                     double* dot_out, const int* stop) {
+  if (stop && *stop) return;  // the solver's state is done: an iteration past convergence
   using C = ChunkTile<T, TY, GS>;
   constexpr int TX = C::TX, NT = C::NT, PY = C::PY, CH = C::CH, NCH = C::NCH, PITCH = C::PITCH;
   constexpr int SLOT = C::SLOT, MPITCH = C::MPITCH, MSLOT = C::MSLOT, RING = C::RING, LOOK = C::LOOK;

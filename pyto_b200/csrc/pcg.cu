@@ -234,7 +234,7 @@ extern "C" int pyto_pcg_solve(const pyto_operator_t* op, const double* s, const 
   while (!hs.done && hs.iters < cfg->max_iters) {
     for (int k = 0; k < every; ++k) {
       // p is zero on fixed DOFs (p = M^-1 r + beta p, M^-1 masked): no input mask needed
-      rc = launch_matvec64(op, s, mask, W.p, W.q, PYTO_MASK_OUT, W.part, W.counter, &W.S->pq, st);
+      rc = launch_matvec64(op, s, mask, W.p, W.q, PYTO_MASK_OUT, W.part, W.counter, &W.S->pq, st, &W.S->done);
       if (rc) return rc;
       k_pcg_update1<<<kNodeBlocks, kNodeThreads, 0, st>>>(g, pc, W.w, W.fl, u, W.r, W.p, W.q, W.S, W.part,
                                                           W.counter);

@@ -52,6 +52,7 @@ def main(argv=None):
     ap.add_argument("--delta", type=float, default=1e-1, help="reliable-update threshold for --kernel mixed")
     ap.add_argument("--mode", type=int, default=3, help="--kernel matvec/matvec32: BC mask mode (1 in, 2 out)")
     ap.add_argument("--stop-rule", type=int, default=0, choices=[0, 1, 2], help="--kernel dpcg: stopping rule")
+    ap.add_argument("--check-every", type=int, default=20, help="--kernel dpcg/mixed/pcg: iterations between host polls")
     a = ap.parse_args(argv)
     if a.kernel == "batch":
         return batch_bench(a)
@@ -90,12 +91,13 @@ def main(argv=None):
             ds.create_deflation_groups(mesh, a.groups)
             defl = ds.device_deflation(g)
             if a.kernel == "dpcg":
-                fn = lambda: g.dpcg(s, F, defl, rtol=1e-8, max_iters=5000, stop_rule=a.stop_rule, check_every=20)
+                fn = lambda: g.dpcg(s, F, defl, rtol=1e-8, max_iters=5000, stop_rule=a.stop_rule,
+                                    check_every=a.check_every)
             else:
                 fn = lambda: g.dpcg_mixed(s, F, defl, rtol=1e-8, delta=a.delta, max_iters=8000,
-                                          check_every=20)
+                                          check_every=a.check_every)
         else:
-            fn = lambda: g.pcg(s, F, rtol=1e-8, check_every=20)
+            fn = lambda: g.pcg(s, F, rtol=1e-8, check_every=a.check_every)
         nbytes = 0
     else:
         fn, nbytes = (lambda: g.stress(u, s, 0.5, want=("vm",))), 24 * g.nnodes + 16 * g.nelem
