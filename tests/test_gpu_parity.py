@@ -417,6 +417,27 @@ def test_dpcg_fp64_residual_replacement(rtol):
     assert abs(C.item() - C2.item()) <= 10 * rtol * abs(C2.item())
 
 
+def test_dpcg_mixed_independent_of_polling_interval():
+    """The residual-replacement triggers are tested at least every 20 iterations, so a
+    long host polling interval neither delays the replacements nor breaks convergence."""
+    from pyto_b200.engine import DeviceDeflation
+    nel = (48, 24, 24)
+    m = O.grid_mesh(*nel)
+    f, fixed = O.cantilever_bc(m)
+    g = _grid(nel, fixed=fixed)
+    rng = np.random.default_rng(4)
+    s, _ = g.simp(_dev(rng.uniform(0.01, 1.0, m["num_elems"])), 3.0, 1e-9)
+    grp, cnt, cen = O.deflation_groups(m["node_xyz"], 60)
+    defl = DeviceDeflation(g, grp, cen, modes=6, shift=1e-14, shift_relative=True)
+    b = _dev(f)
+    u1, i1 = g.dpcg_mixed(s, b, defl, rtol=1e-9, check_every=10)
+    u2, i2 = g.dpcg_mixed(s, b, defl, rtol=1e-9, check_every=500)
+    assert i1.converged and i2.converged and i2.true_rel_res <= 1e-9
+    assert abs(i1.iters - i2.iters) <= 2, (i1.iters, i2.iters)
+    u3, i3 = g.dpcg(s, b, defl, rtol=1e-9, stop_rule=2, check_every=500)
+    assert i3.converged and i3.true_rel_res <= 1e-9
+
+
 @pytest.mark.parametrize("mixed", [False, True])
 def test_dpcg_warm_start(mixed):
     """A warm start (residual-replacement forms) reaches the same solution in fewer
