@@ -322,7 +322,8 @@ def main():
     u_main = u.clone()
     for _ in range(2):
         solve_step(P, form=other)
-    t_other, u_other, info_other = time_solves(P, other, args.steps, device)
+    with ClockSampler(local) as clk_other:
+        t_other, u_other, info_other = time_solves(P, other, args.steps, device)
     s_, _ = g.simp(P["rho"], 3.0, 1e-9, want_ds=False)
     _, c_main = g.energy(u_main, s=s_)
     _, c_other = g.energy(u_other, s=s_)
@@ -362,6 +363,7 @@ def main():
                                 "rel-residual <= 1e-8" if args.form == "mixed" else
                                 "fp64 deflated PCG (Jacobi), true rel-residual <= 1e-8"),
                        "fp64_solve_s": t_fp64, "mixed_solve_s": t_mixed, "mixed_speedup": t_fp64 / t_mixed,
+                       "other_form_clocks": clk_other.summary(),
                        "compliance": c_main, "compliance_rel_diff_vs_other_form": abs(c_main - c_other) / abs(c_other),
                        "other_form_iterations": info_other.iters,
                        "coarse_space": f"{P['ds'].ws_nGroups} node-box groups x {args.modes} rigid modes "
