@@ -29,6 +29,19 @@ void count_launches(long long n);
 #define PYTO_COUNT(n) ::pyto::count_launches(n)
 
 namespace pyto {
+// Function attributes (the dynamic shared-memory opt-in) belong to a device: a call
+// site sets them once per device it launches on.  needed() is true until done() was
+// called while that device was current.
+struct PerDevice {
+  unsigned long long mask = 0;  // devices 0..63
+  static unsigned long long bit() {
+    int d = 0;
+    cudaGetDevice(&d);
+    return 1ull << (d & 63);
+  }
+  bool needed() const { return (__atomic_load_n(&mask, __ATOMIC_ACQUIRE) & bit()) == 0; }
+  void done() { __atomic_fetch_or(&mask, bit(), __ATOMIC_RELEASE); }
+};
 
 constexpr int kNumSMs = 148;        // B200
 constexpr int kReduceBlocks = 1184; // max partial slots of a node-wise reduction (8 per SM)

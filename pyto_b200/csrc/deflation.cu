@@ -1553,14 +1553,14 @@ static int chunk_setup(const pyto_deflation_t* d, const DpcgWs& W, cudaStream_t 
 }
 
 static int gemv_smem_ok(long long nc) {
-  static bool done = false;
-  if (!done) {
+  static PerDevice attr;
+  if (attr.needed()) {
     if (cudaFuncSetAttribute(k_coarse_gemv, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(kMaxCoarse * sizeof(double))) != cudaSuccess ||
         cudaFuncSetAttribute(k_gemv, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(kMaxCoarse * sizeof(double))) != cudaSuccess)
       return PYTO_ERR_CUDA;
-    done = true;
+    attr.done();
   }
   return nc <= kMaxCoarse ? PYTO_OK : PYTO_ERR_TOO_LARGE;
 }
@@ -1581,13 +1581,13 @@ static int dpcg_setup_launch(const pyto_operator_t* op, const double* s, const u
   const size_t shm = (size_t)defl->max_nbr * 36 * sizeof(double);
   if (nchunks > 0) {
     const size_t shm2 = shm + 64 * kCrThreads * sizeof(double);
-    static bool attr = false;
-    if (!attr) {
+    static PerDevice attr;
+    if (attr.needed()) {
       PYTO_CUDA(cudaFuncSetAttribute(k_coarse_rows2<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)(64 * kCrThreads * sizeof(double) + 128 * 36 * sizeof(double))));
       PYTO_CUDA(cudaFuncSetAttribute(k_coarse_rows2<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)(64 * kCrThreads * sizeof(double) + 128 * 36 * sizeof(double))));
-      attr = true;
+      attr.done();
     }
     if (dp.modes == 6)
       k_coarse_rows2<6><<<nchunks, kCrThreads, shm2, st>>>(g, make_khat(op), dp, s, mask, defl->node_group,

@@ -142,10 +142,10 @@ static size_t filter_smem(int R) {
 template <int MODE>
 static int launch_filter(const GridDims& g, const TileTaps& tt, const double* x, const double* w, const double* hs,
                          const uint8_t* active, double* y, cudaStream_t st) {
-  static bool attr = false;
-  if (!attr) {
+  static PerDevice attr;
+  if (attr.needed()) {
     PYTO_CUDA(cudaFuncSetAttribute(k_filter<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)filter_smem(3)));
-    attr = true;
+    attr.done();
   }
   const dim3 grid((g.nx + kFx - 1) / kFx, (g.ny + kFy - 1) / kFy, (g.nz + kFz - 1) / kFz);
   k_filter<MODE><<<grid, 256, filter_smem(tt.R), st>>>(g, tt, x, w, hs, active, y);

@@ -11,20 +11,21 @@ namespace pyto {
 // ---------------------------------------------------------------------------
 // matrix-free y = K(s) u
 //
-// Per element layer ez (one barrier):
-//   1. barrier; write the owned nodes of plane ez-1 (their 4 column
-//      contributions were combined in the previous layer: x by shuffle, y
-//      through `sc`);
-//   2. stage plane ez+2 (prefetched in registers) into smem ring slot
-//      (ez+2)&3 and issue the global loads of plane ez+3;
-//   3. element core for layer ez from the face transforms of planes ez (kept
-//      from the previous layer) and ez+1;  the bottom-face part plus the
-//      pending top-face part of layer ez-1 completes plane ez, which is
-//      inverse-transformed and combined across columns for output in the
-//      next layer.  The pending top-face accumulators of a thread live in its
-//      own shared-memory slots (`sG`) rather than in registers.
-// Four plane slots are in flight: ez-1 (output: BC mask and u for the fused
-// dot), ez and ez+1 (compute), ez+2 (being staged).
+// Tile kernel (k_matvec).  Node planes stream through a 5-slot shared-memory
+// ring (SoA per component) by cp.async, one 4- or 8-byte copy per node value
+// (zero-fill outside the grid), with the BC mask staged beside them.  Per
+// element layer ez (one barrier):
+//   1. wait for plane ez+1, barrier; write the owned nodes of plane ez-1 (their
+//      4 column contributions were combined in the previous layer: x by
+//      shuffle, y through `sc`);
+//   2. issue the copies of plane ez+3;
+//   3. element core for layer ez from the face transforms of planes ez and
+//      ez+1 (both read from the ring); the bottom-face part plus the pending
+//      top-face part of layer ez-1 (in the thread's shared-memory slots `sG`)
+//      completes plane ez, which is inverse-transformed and combined across
+//      columns for output in the next layer.
+// The chunk-staged kernel (matvec_chunked.cuh) keeps this order but copies
+// whole rows as 16-byte chunks and holds faces and pending sums in registers.
 // ---------------------------------------------------------------------------
 template <typename T, int TY, bool TC = false>
 struct MvSmem {
@@ -483,11 +484,11 @@ template <typename T, int TY, bool DOT, bool MI, int MINB, bool TC = false>
 static int launch_mv_t(const MvLaunch& L, size_t smem, const GridDims& g, const KHat& kh, const T* s,
                        const uint8_t* mask, const T* u, T* y, int mode, double* part, unsigned* counter, double* dot,
                        cudaStream_t st, const int* stop) {
-  static bool attr = false;
-  if (!attr) {
+  static PerDevice attr;
+  if (attr.needed()) {
     PYTO_CUDA(cudaFuncSetAttribute(k_matvec<T, TY, DOT, MI, MINB, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem));
-    attr = true;
+    attr.done();
   }
   k_matvec<T, TY, DOT, MI, MINB, TC><<<L.grid, 32 * TY, smem, st>>>(g, kh, s, mask, u, y, L.zc, mode, part, counter,
                                                                     dot, stop);
@@ -518,11 +519,11 @@ static int launch_mvc_t(const MvLaunch& L, const GridDims& g, const KHatT<T>& kh
                         const T* u, T* y, int mode, double* part, unsigned* counter, double* dot, cudaStream_t st,
                         const int* stop) {
   constexpr size_t smem = ChunkTile<T, TY, GS>::bytes;
-  static bool attr = false;
-  if (!attr) {
+  static PerDevice attr;
+  if (attr.needed()) {
     PYTO_CUDA(cudaFuncSetAttribute(k_matvec_chunked<T, TY, DOT, MI, MINB, GS, RF>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr = true;
+    attr.done();
   }
   k_matvec_chunked<T, TY, DOT, MI, MINB, GS, RF><<<L.grid, 32 * TY, smem, st>>>(g, kh, s, mask, u, y, L.zc, mode, part,
                                                                         counter, dot, stop);

@@ -1,5 +1,6 @@
-// FP64 matrix-free hex8 operator: shared between the plain matvec entry point
-// and the fused Krylov kernels.
+// Matrix-free hex8 operator helpers (FP64 and FP32): the element core in the
+// Hadamard basis, face transforms and the tile decomposition shared by the
+// operator kernels and the deflation kernels.
 //
 // Work decomposition.  A CTA owns a box of (TX-1) x (TY-1) node columns and a
 // slab of node planes [Z0, Z1).  Its TX x TY threads each own one *element
@@ -8,18 +9,14 @@
 // neighbouring CTAs, so every node's sum is formed by exactly one thread and
 // no atomics are needed (results are bitwise reproducible).
 //
-// Per element, in the Hadamard corner basis (see element.cu):
-//   face transform of the new top face (8 add/comp), z-combination with the
-//   bottom face kept in registers from the previous layer, 57 FMAs of the
-//   block operator scaled by s_e, inverse z-split into bottom/top face
-//   contributions; a face is inverse-transformed once after both elements
-//   that share it were accumulated.  Node contributions of the 4 columns
-//   around a vertical node line are combined with one shuffle (x) and one
-//   shared-memory exchange (y).
-//
-// Node planes are staged in shared memory (SoA, double-buffered) with flat,
-// fully coalesced loads; the next plane and the next s_e are prefetched into
-// registers one layer ahead.
+// Per element, in the Hadamard corner basis (see element.cu): face transforms
+// of the bottom and top faces (8 add/comp each), their z-combination, 57 FMAs
+// of the block operator scaled by s_e, inverse z-split into bottom/top face
+// contributions; a face is inverse-transformed once after both elements that
+// share it were accumulated.  Node contributions of the 4 columns around a
+// vertical node line are combined with one shuffle (x) and one shared-memory
+// exchange (y).  The node-plane staging of the two kernels that use these
+// helpers is described in matvec.cu and matvec_chunked.cuh.
 #pragma once
 #include "common.cuh"
 
