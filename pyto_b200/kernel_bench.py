@@ -37,7 +37,7 @@ def _timeit(fn, reps, warm=3):
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--kernel", default="matvec", choices=["matvec", "matvec32", "energy", "filter", "jacobi", "stress", "dpcg",
-                                                          "mixed", "pcg", "batch", "oc"])
+                                                          "mixed", "pcg", "batch", "oc", "adjoint", "ocupdate"])
     ap.add_argument("--iters", type=int, default=20, help="--kernel oc: OC iterations")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"], help="--kernel oc: DPCG form")
     ap.add_argument("--warm-start", action="store_true", help="--kernel oc: start each solve from the previous one")
@@ -99,6 +99,20 @@ def main(argv=None):
         else:
             fn = lambda: g.pcg(s, F, rtol=1e-8, check_every=a.check_every)
         nbytes = 0
+    elif a.kernel == "adjoint":  # p-norm adjoint: explicit term T1 and the adjoint load g = dPN/du
+        x = s  # densities in (0.01, 1]
+        dpn = g.tensor(np.array([1.0]))
+        # k_pnorm_elem: u, x in; T1 and the 6-vector t per element out; k_pnorm_gather: t in, g out
+        fn, nbytes = (lambda: g.pnorm_adjoint(u, x, 0.5, 8.0, dpn)), 48 * g.nnodes + 112 * g.nelem
+    elif a.kernel == "ocupdate":  # OC bisection update (reference sequence), x restored each call
+        x0 = s.clone()
+        xw = torch.empty_like(x0)
+        dc = -g.tensor(rng.uniform(0.1, 1.0, g.nelem))
+
+        def fn():
+            xw.copy_(x0)
+            return g.oc_update(xw, dc, 0.3)
+        nbytes = 24 * g.nelem  # per bisection pass
     else:
         fn, nbytes = (lambda: g.stress(u, s, 0.5, want=("vm",))), 24 * g.nnodes + 16 * g.nelem
     t = _timeit(fn, a.reps, a.warm)
