@@ -105,6 +105,7 @@ __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_g
 
 }  // namespace pyto
 #include "matvec_chunked.cuh"
+#include "matvec_chunked2.cuh"
 namespace pyto {
 
 template <typename T, int TY, bool DOT, bool MASKIN, int MINB, bool TC = false>
@@ -550,6 +551,42 @@ static int launch_mvc(const GridDims& g, const KHat& kh, const T* s, const uint8
                                                           st, stop);
 }
 
+template <typename T, int TY, bool DOT, bool MI, int MINB>
+static int launch_mvc2_t(const GridDims& g, const KHatT<T>& kh, const T* s, const uint8_t* mask, const T* u, T* y,
+                         int mode, double* part, unsigned* counter, double* dot, cudaStream_t st, const int* stop) {
+  constexpr size_t smem = ChunkTile2<T, TY>::bytes;
+  static PerDevice attr;
+  if (attr.needed()) {
+    PYTO_CUDA(cudaFuncSetAttribute(k_matvec_chunked2<T, TY, DOT, MI, MINB>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr.done();
+  }
+  const int bx = (g.sx + 30) / 31, by = (g.sy + 2 * TY - 2) / (2 * TY - 1);
+  const int zc = matvec_zc(bx, by, g.sz);
+  const dim3 grid(bx, by, (g.sz + zc - 1) / zc);
+  k_matvec_chunked2<T, TY, DOT, MI, MINB><<<grid, 32 * TY, smem, st>>>(g, kh, s, mask, u, y, zc, mode, part, counter,
+                                                                       dot, stop);
+  PYTO_COUNT(1);
+  PYTO_LAUNCH_CHECK();
+  return PYTO_OK;
+}
+
+// two element rows per thread; u and the mask 16-byte aligned, else the tile kernel
+template <typename T, int TY, int MINB>
+static int launch_mvc2(const GridDims& g, const KHat& kh, const T* s, const uint8_t* mask, const T* u, T* y, int mode,
+                       double* part, unsigned* counter, double* dot, cudaStream_t st, const int* stop) {
+  if (((uintptr_t)u & 15) || ((uintptr_t)mask & 15))
+    return launch_mv<T, TY, MINB>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
+  const KHatT<T> kt = make_khat_t<T>(kh);
+  const bool mi = (mode & PYTO_MASK_IN) && mask != nullptr;
+  if (dot)
+    return mi ? launch_mvc2_t<T, TY, true, true, MINB>(g, kt, s, mask, u, y, mode, part, counter, dot, st, stop)
+              : launch_mvc2_t<T, TY, true, false, MINB>(g, kt, s, mask, u, y, mode, part, counter, dot, st, stop);
+  return mi ? launch_mvc2_t<T, TY, false, true, MINB>(g, kt, s, mask, u, y, mode, nullptr, nullptr, nullptr, st, stop)
+            : launch_mvc2_t<T, TY, false, false, MINB>(g, kt, s, mask, u, y, mode, nullptr, nullptr, nullptr, st,
+                                                       stop);
+}
+
 // Tile variant of the FP64 matvec (2 = default: fastest measured at 192x96x96):
 //   0: 32x8 threads, 2 CTAs/SM (128 registers)   1: 32x8, 1 CTA/SM (no register cap)
 //   2: 32x4, 3 CTAs/SM                            3: 32x16, 1 CTA/SM
@@ -582,7 +619,10 @@ int launch_matvec32(const pyto_operator_t* op, const float* s, const uint8_t* ma
   const GridDims g = make_dims(op);
   const KHat kh = make_khat(op);
   const int tv = ((op->tune >> 8) & 0xff) - 1;
-  switch ((tv >= 0 && tv <= 5) || (tv >= 8 && tv <= 11) ? tv : g_mv32_variant) {
+  switch ((tv >= 0 && tv <= 5) || (tv >= 8 && tv <= 14) ? tv : g_mv32_variant) {
+    case 12: return launch_mvc2<float, 8, 2>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
+    case 13: return launch_mvc2<float, 4, 3>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
+    case 14: return launch_mvc2<float, 8, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
     case 8: return launch_mvc<float, 8, 3>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
     case 9: return launch_mvc<float, 8, 2>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
     case 10: return launch_mvc<float, 4, 6>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
@@ -606,7 +646,7 @@ int set_matvec_variant(int v) {
 }
 
 int set_matvec32_variant(int v) {
-  if (v < 0 || (v > 5 && v < 8) || v > 11) return PYTO_ERR_ARG;
+  if (v < 0 || (v > 5 && v < 8) || v > 14) return PYTO_ERR_ARG;
   g_mv32_variant = v;
   return PYTO_OK;
 }
