@@ -487,77 +487,76 @@ __global__ void k_coarse_finish(long long nc, double* E, double shift, const dou
 // blocked sweep inversion: after all pivot blocks A = -E^-1
 //   P = A_KK^-1, U = P A_K:, A_ij -= A_iK U_Kj, A_Kj = U_Kj, A_iK = U_Ki^T, A_KK = -P
 // ---------------------------------------------------------------------------
-// In-place sweep of the bk x bk diagonal block (result -M^-1).  256 threads, each
-// holding a 4 x 4 set of entries (rows ty + 16a, columns tx + 16b) in registers;
-// per pivot step only the pivot row and column pass through shared memory
-// (double-buffered, one barrier per step).
-__device__ __forceinline__ void sweep_pivot_regs(double (&R)[4][4], int bk, double (*s_row)[kSweepB],
-                                                 double (*s_col)[kSweepB]) {
+// Element k of a 4-vector held in registers, by selects (a dynamic index would put
+// the array in local memory).
+__device__ __forceinline__ double pick4(double v0, double v1, double v2, double v3, int k) {
+  double r = v0;
+  r = (k == 1) ? v1 : r;
+  r = (k == 2) ? v2 : r;
+  r = (k == 3) ? v3 : r;
+  return r;
+}
+
+// In-place sweep of the symmetric 64 x 64 block held by 256 threads (thread (ty, tx)
+// owns rows ty + 16a, columns tx + 16b), pivots 0..63 in order:
+//   M_pp -> -1/M_pp,  M_pj -> M_pj/M_pp,  M_ip -> M_ip/M_pp,  M_ij -= M_ip M_pj / M_pp,
+// leaving -M^-1.  Padding pivots (identity rows/columns beyond bk) are decoupled, so they
+// are swept with the rest.  The owners of row p publish it (raw and divided by the
+// pivot) in a double-buffered shared row, so each pivot costs one barrier, and the
+// pivot loop stays rolled: the code is executed 64 times from the instruction cache
+// instead of once per pivot from L2.  The block stays bitwise symmetric (M_ip is read
+// as M_pi).  sm: >= 2 * 130 doubles.
+__device__ __forceinline__ void sweep_pivot_rolled(double (&R)[4][4], double* sm) {
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  for (int p = 0; p < bk; ++p) {
-    const int buf = p & 1, pa = p >> 4, pr = p & 15;
-    if (ty == pr) {  // pivot row: register row pa of the threads with ty == p mod 16
+#pragma unroll 1
+  for (int p = 0; p < 64; ++p) {
+    double* row = sm + (p & 1) * 130;  // [0, 64): M_p:, [64, 128): M_p: / M_pp, 128: 1 / M_pp
+    const int pr = p & 15, pa = p >> 4;
+    if (ty == pr) {  // half a warp: the owners of row p
+      double v[4];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) v[b] = pick4(R[0][b], R[1][b], R[2][b], R[3][b], pa);
+      const unsigned half = 0xFFFFu << (16 * (ty & 1));
+      const double mpp = __shfl_sync(half, pick4(v[0], v[1], v[2], v[3], pa), pr, 16);
+      const double ip = 1.0 / mpp;
 #pragma unroll
       for (int b = 0; b < 4; ++b) {
-        double v = R[0][b];
-#pragma unroll
-        for (int a = 1; a < 4; ++a)
-          if (a == pa) v = R[a][b];
-        s_row[buf][tx + 16 * b] = v;
+        row[tx + 16 * b] = v[b];
+        row[64 + tx + 16 * b] = v[b] * ip;
       }
-    }
-    if (tx == pr) {  // pivot column
-#pragma unroll
-      for (int a = 0; a < 4; ++a) {
-        double v = R[a][0];
-#pragma unroll
-        for (int b = 1; b < 4; ++b)
-          if (b == pa) v = R[a][b];
-        s_col[buf][ty + 16 * a] = v;
-      }
+      if (tx == 0) row[128] = ip;
     }
     __syncthreads();
-    const double ipiv = 1.0 / s_row[buf][p];
-    double rv[4], cv[4];
+    double mip[4], rcj[4];
 #pragma unroll
-    for (int b = 0; b < 4; ++b) rv[b] = s_row[buf][tx + 16 * b] * ipiv;
+    for (int a = 0; a < 4; ++a) mip[a] = row[ty + 16 * a];
 #pragma unroll
-    for (int a = 0; a < 4; ++a) cv[a] = s_col[buf][ty + 16 * a];
-    // every entry: M_ij - M_ip M_pj / M_pp; then the owners of the pivot row and
-    // column replace theirs: M_pj / M_pp, M_ip / M_pp, and -1 / M_pp on the diagonal
+    for (int b = 0; b < 4; ++b) rcj[b] = row[64 + tx + 16 * b];
 #pragma unroll
     for (int a = 0; a < 4; ++a)
 #pragma unroll
-      for (int b = 0; b < 4; ++b) R[a][b] = fma(-cv[a], rv[b], R[a][b]);
-    if (ty == pr) {
+      for (int b = 0; b < 4; ++b) R[a][b] = fma(-mip[a], rcj[b], R[a][b]);
+    if (ty == pr) {  // row p: M_pj / M_pp
 #pragma unroll
       for (int a = 0; a < 4; ++a)
-        if (a == pa)
 #pragma unroll
-          for (int b = 0; b < 4; ++b) R[a][b] = rv[b];
+        for (int b = 0; b < 4; ++b)
+          if (a == pa) R[a][b] = rcj[b];
     }
-    if (tx == pr) {
+    if (tx == pr) {  // column p: M_ip / M_pp (= M_pi / M_pp), and the pivot itself
+      const double ip = row[128];
 #pragma unroll
-      for (int b = 0; b < 4; ++b)
-        if (b == pa)
+      for (int a = 0; a < 4; ++a)
 #pragma unroll
-          for (int a = 0; a < 4; ++a) R[a][b] = cv[a] * ipiv;
-      if (ty == pr) {
-#pragma unroll
-        for (int a = 0; a < 4; ++a)
-          if (a == pa) {
-#pragma unroll
-            for (int b = 0; b < 4; ++b)
-              if (b == pa) R[a][b] = -ipiv;
-          }
-      }
+        for (int b = 0; b < 4; ++b)
+          if (b == pa) R[a][b] = (ty + 16 * a == p) ? -ip : mip[a] * ip;
     }
   }
+  __syncthreads();  // the caller may reuse sm
 }
 
 __global__ void __launch_bounds__(256) k_sweep_pivot(long long n, int k0, int bk, const double* __restrict__ A,
                                                      double* __restrict__ P) {
-  __shared__ double s_row[2][kSweepB], s_col[2][kSweepB];
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   double R[4][4];
 #pragma unroll
@@ -567,7 +566,8 @@ __global__ void __launch_bounds__(256) k_sweep_pivot(long long n, int k0, int bk
       const int i = ty + 16 * a, j = tx + 16 * b;
       R[a][b] = (i < bk && j < bk) ? A[(k0 + i) * n + (k0 + j)] : (i == j ? 1.0 : 0.0);
     }
-  sweep_pivot_regs(R, bk, s_row, s_col);
+  __shared__ double sm[2 * 130];
+  sweep_pivot_rolled(R, sm);
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
@@ -607,12 +607,12 @@ __global__ void __launch_bounds__(256) k_sweep_panel(long long n, int k0, int bk
 // 256 threads x (4x4) outputs, k in chunks of 32.  k1 >= 0: the CTA of the next
 // pivot tile (k1, k1) -- block 0, so it starts first -- goes on to sweep it in
 // registers and writes Pn = A_k1k1^-1 for the next step, behind the other tiles.
-__global__ void __launch_bounds__(256) k_sweep_update(long long n, int k0, int bk, double* __restrict__ A,
+__global__ void __launch_bounds__(256, 3) k_sweep_update(long long n, int k0, int bk, double* __restrict__ A,
                                                       const double* __restrict__ P, const double* __restrict__ Rp,
                                                       const double* __restrict__ U, int k1, double* __restrict__ Pn) {
-  __shared__ double sL[32][65];  // A_iK for the tile rows: Rp[k][i]
-  __shared__ double sU[32][65];  // U_Kj for the tile cols
-  __shared__ double s_row[2][kSweepB], s_col[2][kSweepB];
+  __shared__ double sLU[2][32][65];  // [0]: A_iK for the tile rows (Rp[k][i]); [1]: U_Kj for the tile cols
+  double(&sL)[32][65] = sLU[0];
+  double(&sU)[32][65] = sLU[1];
   const long long ntiles = gridDim.x;
   long long b = blockIdx.x;
   if (k1 >= 0) {  // rotate the numbering so that block 0 is tile (k1/64, k1/64)
@@ -688,7 +688,8 @@ __global__ void __launch_bounds__(256) k_sweep_update(long long n, int k0, int b
       const int i = ty + 16 * a, j = tx + 16 * b;
       if (!(i < bk1 && j < bk1)) acc[a][b] = (i == j) ? 1.0 : 0.0;
     }
-  sweep_pivot_regs(acc, bk1, s_row, s_col);
+  __syncthreads();
+  sweep_pivot_rolled(acc, &sLU[0][0][0]);  // sL, sU are free now
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
