@@ -124,6 +124,10 @@ typedef struct pyto_deflation {
 
 /* ---- version / workspace ------------------------------------------------- */
 int pyto_version(void);
+/* sizeof of this library's ABI structs, for bindings to check their layout:
+ * 0 pyto_operator_t, 1 pyto_solve_cfg_t, 2 pyto_solve_status_t, 3 pyto_deflation_t,
+ * 4 pyto_batch_item_t; 0 for other values.  No reference counterpart. */
+size_t pyto_struct_size(int which);
 /* Description of the last CUDA call of this thread that failed inside the library
  * (file:line, the call, the CUDA error); "" if none.  No reference counterpart. */
 const char* pyto_last_error(void);

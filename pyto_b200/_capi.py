@@ -71,6 +71,7 @@ _P = C.c_void_p
 _OP = C.POINTER(Operator)
 SIGNATURES = {
     "pyto_version": (C.c_int, []),
+    "pyto_struct_size": (C.c_size_t, [C.c_int]),
     "pyto_last_error": (C.c_char_p, []),
     "pyto_launch_count": (C.c_longlong, []),
     "pyto_tune": (C.c_int, [C.c_int, C.c_int]),

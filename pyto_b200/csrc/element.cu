@@ -40,6 +40,17 @@ void constitutive(double E, double nu, double D[6][6]) {
 
 extern "C" int pyto_version(void) { return 1; }
 
+extern "C" size_t pyto_struct_size(int which) {
+  switch (which) {
+    case 0: return sizeof(pyto_operator_t);
+    case 1: return sizeof(pyto_solve_cfg_t);
+    case 2: return sizeof(pyto_solve_status_t);
+    case 3: return sizeof(pyto_deflation_t);
+    case 4: return sizeof(pyto_batch_item_t);
+    default: return 0;
+  }
+}
+
 extern "C" int pyto_ke_hex8(double E, double nu, double hx, double hy, double hz, double* ke) {
   if (!ke || !(hx > 0) || !(hy > 0) || !(hz > 0) || !(nu < 0.5) || !(nu > -1.0)) return PYTO_ERR_ARG;
   double D[6][6];

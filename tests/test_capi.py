@@ -26,6 +26,14 @@ def test_library_exports_every_declared_symbol():
     assert L.pyto_version() >= 1
 
 
+def test_ctypes_structs_match_the_c_layout():
+    """The ctypes mirrors of the ABI structs have the C compiler's sizes."""
+    L = A.lib()
+    for which, cls in enumerate((A.Operator, A.SolveCfg, A.SolveStatus, A.Deflation, A.BatchItem)):
+        assert L.pyto_struct_size(which) == C.sizeof(cls), cls.__name__
+    assert L.pyto_struct_size(5) == 0
+
+
 @pytest.mark.parametrize("tag,E,nu,h", [("unit", 1.0, 0.3, (1, 1, 1)), ("box", 1.0, 0.3, (1.0, 0.5, 2.0)),
                                         ("half", 2.5, 0.25, (0.5, 0.5, 0.5))])
 def test_ke_matches_reference(tag, E, nu, h):
