@@ -36,8 +36,9 @@ RTOL = 1e-8
 # (output mask only), from ncu captures of the two operator kernels (profiles/
 # k_matvec_192x96x96.md; cold caches, so the y writes, which stay in L2 during the
 # launch, are mostly not counted)
-TRAFFIC = {"f32": 30762240, "f64": 71395328}
-KERNEL = {"f32": "k_matvec_chunked<float> (chunk-staged, variant 8)", "f64": "k_matvec<double> (tile, variant 2)"}
+TRAFFIC = {"f32": 30771456, "f64": 71395328}
+KERNEL = {"f32": "k_matvec_chunked2<float, packed FP32x2> (two element rows per thread, variant 16)",
+          "f64": "k_matvec<double> (tile, variant 2)"}
 
 
 def peaks():

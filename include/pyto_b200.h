@@ -138,9 +138,10 @@ long long pyto_launch_count(void);
  * choice of the project's autotuner).  PYTO_KERNEL_MATVEC variants 0..3 (tile kernel,
  * default 2) and 8..10 (chunk-staged kernel: node-plane rows copied as 16-byte chunks,
  * faces and pending accumulators in registers; bitwise-equal results); PYTO_KERNEL_MATVEC32
- * variants 0..5, 8..11 and 12..14 (chunk-staged, two element rows per thread).  The chunk-staged variants need u and the mask 16-byte
- * aligned and otherwise run the tile kernel.  Process-wide; not thread-safe against
- * concurrent launches. */
+ * variants 0..5, 8..11, 12..14 (chunk-staged, two element rows per thread) and 15..17
+ * (the same with the two rows as packed FP32x2 lanes; default 16).  The chunk-staged
+ * variants need u and the mask 16-byte aligned and otherwise run the tile kernel.
+ * Process-wide; not thread-safe against concurrent launches. */
 #define PYTO_KERNEL_MATVEC 0
 #define PYTO_KERNEL_MATVEC32 1
 #define PYTO_KERNEL_GRAPHS 2   /* variant 1 (default): deflated PCG iteration chunks replayed as

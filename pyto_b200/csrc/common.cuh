@@ -191,4 +191,28 @@ struct Carver {
   bool ok() const { return base != nullptr && off <= cap; }
 };
 
+// Two FP32 lanes in one 64-bit register pair for the packed FP32x2 arithmetic of
+// sm_100 (__fadd2_rn / __fmul2_rn / __ffma2_rn): two independent elements go through
+// the same arithmetic in one instruction stream.  Each lane rounds exactly as the
+// scalar operation.  In a namespace of its own so that fma() on floats keeps
+// resolving to the global one (this fma is found by argument-dependent lookup).
+namespace packed {
+struct f32x2 {
+  float2 v;
+  f32x2() = default;
+  __host__ __device__ constexpr explicit f32x2(float a) : v{a, a} {}
+  __host__ __device__ constexpr f32x2(float a, float b) : v{a, b} {}
+  __host__ __device__ constexpr explicit f32x2(float2 w) : v(w) {}
+};
+__device__ __forceinline__ f32x2 operator+(f32x2 a, f32x2 b) { return f32x2(__fadd2_rn(a.v, b.v)); }
+__device__ __forceinline__ f32x2 operator-(f32x2 a) { return f32x2(-a.v.x, -a.v.y); }
+__device__ __forceinline__ f32x2 operator-(f32x2 a, f32x2 b) {
+  return f32x2(__fadd2_rn(a.v, make_float2(-b.v.x, -b.v.y)));
+}
+__device__ __forceinline__ f32x2 operator*(f32x2 a, f32x2 b) { return f32x2(__fmul2_rn(a.v, b.v)); }
+__device__ __forceinline__ f32x2 fma(f32x2 a, f32x2 b, f32x2 c) { return f32x2(__ffma2_rn(a.v, b.v, c.v)); }
+__device__ __forceinline__ f32x2& operator+=(f32x2& a, f32x2 b) { return a = a + b; }
+__device__ __forceinline__ f32x2& operator-=(f32x2& a, f32x2 b) { return a = a - b; }
+}  // namespace packed
+
 }  // namespace pyto

@@ -1,6 +1,7 @@
 // FP64 operator kernels: BC mask, SIMP scaling, Jacobi data, and the
 // matrix-free K(s) u (algorithm notes in matvec.cuh).
 #include <algorithm>
+#include <atomic>
 
 #include <cuda_bf16.h>
 
@@ -481,16 +482,28 @@ __global__ void __launch_bounds__(32 * TY, MINB)
   }
 }
 
+// CTAs of `kernel` resident per SM at `threads` threads and `smem` bytes of dynamic
+// shared memory (the kernel's attributes already set), times the SM count.
+template <typename K>
+static int resident_slots(K kernel, int threads, size_t smem) {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, smem) != cudaSuccess || n < 1) n = 1;
+  return n * kNumSMs;
+}
+
 template <typename T, int TY, bool DOT, bool MI, int MINB, bool TC = false>
-static int launch_mv_t(const MvLaunch& L, size_t smem, const GridDims& g, const KHat& kh, const T* s,
-                       const uint8_t* mask, const T* u, T* y, int mode, double* part, unsigned* counter, double* dot,
-                       cudaStream_t st, const int* stop) {
+static int launch_mv_t(size_t smem, const GridDims& g, const KHat& kh, const T* s, const uint8_t* mask, const T* u,
+                       T* y, int mode, double* part, unsigned* counter, double* dot, cudaStream_t st,
+                       const int* stop) {
   static PerDevice attr;
+  static std::atomic<int> slots{0};
   if (attr.needed()) {
     PYTO_CUDA(cudaFuncSetAttribute(k_matvec<T, TY, DOT, MI, MINB, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem));
+    slots.store(resident_slots(k_matvec<T, TY, DOT, MI, MINB, TC>, 32 * TY, smem));
     attr.done();
   }
+  const MvLaunch L = matvec_launch<32, TY>(g, slots.load());
   k_matvec<T, TY, DOT, MI, MINB, TC><<<L.grid, 32 * TY, smem, st>>>(g, kh, s, mask, u, y, L.zc, mode, part, counter,
                                                                     dot, stop);
   PYTO_COUNT(1);
@@ -502,30 +515,31 @@ template <typename T, int TY, int MINB, bool TC = false>
 static int launch_mv(const GridDims& g, const KHat& kh, const T* s, const uint8_t* mask, const T* u, T* y, int mode,
                      double* part, unsigned* counter, double* dot, cudaStream_t st, const int* stop = nullptr) {
   const size_t smem = MvSmem<T, TY, TC>::bytes;
-  const MvLaunch L = matvec_launch<32, TY>(g);
   const bool mi = (mode & PYTO_MASK_IN) && mask != nullptr;
   if (dot)
-    return mi ? launch_mv_t<T, TY, true, true, MINB, TC>(L, smem, g, kh, s, mask, u, y, mode, part, counter, dot, st,
+    return mi ? launch_mv_t<T, TY, true, true, MINB, TC>(smem, g, kh, s, mask, u, y, mode, part, counter, dot, st,
                                                          stop)
-              : launch_mv_t<T, TY, true, false, MINB, TC>(L, smem, g, kh, s, mask, u, y, mode, part, counter, dot,
+              : launch_mv_t<T, TY, true, false, MINB, TC>(smem, g, kh, s, mask, u, y, mode, part, counter, dot,
                                                            st, stop);
-  return mi ? launch_mv_t<T, TY, false, true, MINB, TC>(L, smem, g, kh, s, mask, u, y, mode, nullptr, nullptr,
+  return mi ? launch_mv_t<T, TY, false, true, MINB, TC>(smem, g, kh, s, mask, u, y, mode, nullptr, nullptr,
                                                         nullptr, st, stop)
-            : launch_mv_t<T, TY, false, false, MINB, TC>(L, smem, g, kh, s, mask, u, y, mode, nullptr, nullptr,
+            : launch_mv_t<T, TY, false, false, MINB, TC>(smem, g, kh, s, mask, u, y, mode, nullptr, nullptr,
                                                          nullptr, st, stop);
 }
 
 template <typename T, int TY, bool DOT, bool MI, int MINB, bool GS, bool RF>
-static int launch_mvc_t(const MvLaunch& L, const GridDims& g, const KHatT<T>& kh, const T* s, const uint8_t* mask,
-                        const T* u, T* y, int mode, double* part, unsigned* counter, double* dot, cudaStream_t st,
-                        const int* stop) {
+static int launch_mvc_t(const GridDims& g, const KHatT<T>& kh, const T* s, const uint8_t* mask, const T* u, T* y,
+                        int mode, double* part, unsigned* counter, double* dot, cudaStream_t st, const int* stop) {
   constexpr size_t smem = ChunkTile<T, TY, GS>::bytes;
   static PerDevice attr;
+  static std::atomic<int> slots{0};
   if (attr.needed()) {
     PYTO_CUDA(cudaFuncSetAttribute(k_matvec_chunked<T, TY, DOT, MI, MINB, GS, RF>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    slots.store(resident_slots(k_matvec_chunked<T, TY, DOT, MI, MINB, GS, RF>, 32 * TY, smem));
     attr.done();
   }
+  const MvLaunch L = matvec_launch<32, TY>(g, slots.load());
   k_matvec_chunked<T, TY, DOT, MI, MINB, GS, RF><<<L.grid, 32 * TY, smem, st>>>(g, kh, s, mask, u, y, L.zc, mode, part,
                                                                         counter, dot, stop);
   PYTO_COUNT(1);
@@ -539,40 +553,43 @@ static int launch_mvc(const GridDims& g, const KHat& kh, const T* s, const uint8
                       double* part, unsigned* counter, double* dot, cudaStream_t st, const int* stop) {
   if (((uintptr_t)u & 15) || ((uintptr_t)mask & 15))
     return launch_mv<T, TY, MINB>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
-  const MvLaunch L = matvec_launch<32, TY>(g);
   const KHatT<T> kt = make_khat_t<T>(kh);
   const bool mi = (mode & PYTO_MASK_IN) && mask != nullptr;
   if (dot)
-    return mi ? launch_mvc_t<T, TY, true, true, MINB, GS, RF>(L, g, kt, s, mask, u, y, mode, part, counter, dot, st, stop)
-              : launch_mvc_t<T, TY, true, false, MINB, GS, RF>(L, g, kt, s, mask, u, y, mode, part, counter, dot, st, stop);
-  return mi ? launch_mvc_t<T, TY, false, true, MINB, GS, RF>(L, g, kt, s, mask, u, y, mode, nullptr, nullptr, nullptr,
+    return mi ? launch_mvc_t<T, TY, true, true, MINB, GS, RF>(g, kt, s, mask, u, y, mode, part, counter, dot, st, stop)
+              : launch_mvc_t<T, TY, true, false, MINB, GS, RF>(g, kt, s, mask, u, y, mode, part, counter, dot, st, stop);
+  return mi ? launch_mvc_t<T, TY, false, true, MINB, GS, RF>(g, kt, s, mask, u, y, mode, nullptr, nullptr, nullptr,
                                                          st, stop)
-            : launch_mvc_t<T, TY, false, false, MINB, GS, RF>(L, g, kt, s, mask, u, y, mode, nullptr, nullptr, nullptr,
+            : launch_mvc_t<T, TY, false, false, MINB, GS, RF>(g, kt, s, mask, u, y, mode, nullptr, nullptr, nullptr,
                                                           st, stop);
 }
 
-template <typename T, int TY, bool DOT, bool MI, int MINB>
-static int launch_mvc2_t(const GridDims& g, const KHatT<T>& kh, const T* s, const uint8_t* mask, const T* u, T* y,
-                         int mode, double* part, unsigned* counter, double* dot, cudaStream_t st, const int* stop) {
+template <typename T, int TY, bool DOT, bool MI, int MINB, bool PACK>
+static int launch_mvc2_t(const GridDims& g, const KHatT<T>& kh, const T* s, const uint8_t* mask,
+                         const T* u, T* y, int mode, double* part, unsigned* counter, double* dot, cudaStream_t st,
+                         const int* stop) {
   constexpr size_t smem = ChunkTile2<T, TY>::bytes;
   static PerDevice attr;
+  static std::atomic<int> slots{0};
   if (attr.needed()) {
-    PYTO_CUDA(cudaFuncSetAttribute(k_matvec_chunked2<T, TY, DOT, MI, MINB>,
+    PYTO_CUDA(cudaFuncSetAttribute(k_matvec_chunked2<T, TY, DOT, MI, MINB, PACK>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    slots.store(resident_slots(k_matvec_chunked2<T, TY, DOT, MI, MINB, PACK>, 32 * TY, smem));
     attr.done();
   }
   const int bx = (g.sx + 30) / 31, by = (g.sy + 2 * TY - 2) / (2 * TY - 1);
-  const int zc = matvec_zc(bx, by, g.sz);
+  const int zc = matvec_zc(bx, by, g.sz, slots.load());
   const dim3 grid(bx, by, (g.sz + zc - 1) / zc);
-  k_matvec_chunked2<T, TY, DOT, MI, MINB><<<grid, 32 * TY, smem, st>>>(g, kh, s, mask, u, y, zc, mode, part, counter,
-                                                                       dot, stop);
+  k_matvec_chunked2<T, TY, DOT, MI, MINB, PACK><<<grid, 32 * TY, smem, st>>>(g, kh, s, mask, u, y, zc, mode, part,
+                                                                             counter, dot, stop);
   PYTO_COUNT(1);
   PYTO_LAUNCH_CHECK();
   return PYTO_OK;
 }
 
-// two element rows per thread; u and the mask 16-byte aligned, else the tile kernel
-template <typename T, int TY, int MINB>
+// two element rows per thread (PACK: as packed FP32x2 lanes); u and the mask 16-byte
+// aligned, else the tile kernel
+template <typename T, int TY, int MINB, bool PACK = false>
 static int launch_mvc2(const GridDims& g, const KHat& kh, const T* s, const uint8_t* mask, const T* u, T* y, int mode,
                        double* part, unsigned* counter, double* dot, cudaStream_t st, const int* stop) {
   if (((uintptr_t)u & 15) || ((uintptr_t)mask & 15))
@@ -580,11 +597,13 @@ static int launch_mvc2(const GridDims& g, const KHat& kh, const T* s, const uint
   const KHatT<T> kt = make_khat_t<T>(kh);
   const bool mi = (mode & PYTO_MASK_IN) && mask != nullptr;
   if (dot)
-    return mi ? launch_mvc2_t<T, TY, true, true, MINB>(g, kt, s, mask, u, y, mode, part, counter, dot, st, stop)
-              : launch_mvc2_t<T, TY, true, false, MINB>(g, kt, s, mask, u, y, mode, part, counter, dot, st, stop);
-  return mi ? launch_mvc2_t<T, TY, false, true, MINB>(g, kt, s, mask, u, y, mode, nullptr, nullptr, nullptr, st, stop)
-            : launch_mvc2_t<T, TY, false, false, MINB>(g, kt, s, mask, u, y, mode, nullptr, nullptr, nullptr, st,
-                                                       stop);
+    return mi ? launch_mvc2_t<T, TY, true, true, MINB, PACK>(g, kt, s, mask, u, y, mode, part, counter, dot, st, stop)
+              : launch_mvc2_t<T, TY, true, false, MINB, PACK>(g, kt, s, mask, u, y, mode, part, counter, dot, st,
+                                                              stop);
+  return mi ? launch_mvc2_t<T, TY, false, true, MINB, PACK>(g, kt, s, mask, u, y, mode, nullptr, nullptr, nullptr, st,
+                                                            stop)
+            : launch_mvc2_t<T, TY, false, false, MINB, PACK>(g, kt, s, mask, u, y, mode, nullptr, nullptr, nullptr,
+                                                             st, stop);
 }
 
 // Tile variant of the FP64 matvec (2 = default: fastest measured at 192x96x96):
@@ -593,8 +612,9 @@ static int launch_mvc2(const GridDims& g, const KHat& kh, const T* s, const uint
 static int g_mv_variant = 2;
 // Tile variant of the FP32 matvec (same numbering; 4 and 5: the tile shapes of 0 and
 // 2 with the element core on the tensor cores, BF16 split hi/lo; 8-11: chunk-staged
-// kernel, 8 = default: fastest measured at 192x96x96)
-static int g_mv32_variant = 8;
+// kernel; 12-14: chunk-staged with two element rows per thread; 15-17: the same with
+// the two rows as packed FP32x2 lanes, 16 = default: fastest measured at 192x96x96)
+static int g_mv32_variant = 16;
 
 int launch_matvec64(const pyto_operator_t* op, const double* s, const uint8_t* mask, const double* u, double* y,
                     int mode, double* part, unsigned* counter, double* dot, cudaStream_t st,
@@ -619,7 +639,10 @@ int launch_matvec32(const pyto_operator_t* op, const float* s, const uint8_t* ma
   const GridDims g = make_dims(op);
   const KHat kh = make_khat(op);
   const int tv = ((op->tune >> 8) & 0xff) - 1;
-  switch ((tv >= 0 && tv <= 5) || (tv >= 8 && tv <= 14) ? tv : g_mv32_variant) {
+  switch ((tv >= 0 && tv <= 5) || (tv >= 8 && tv <= 17) ? tv : g_mv32_variant) {
+    case 15: return launch_mvc2<float, 8, 2, true>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
+    case 16: return launch_mvc2<float, 4, 3, true>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
+    case 17: return launch_mvc2<float, 8, 1, true>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
     case 12: return launch_mvc2<float, 8, 2>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
     case 13: return launch_mvc2<float, 4, 3>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
     case 14: return launch_mvc2<float, 8, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
@@ -636,8 +659,8 @@ int launch_matvec32(const pyto_operator_t* op, const float* s, const uint8_t* ma
   }
 }
 
-// upper bound of the block count over the tile variants (the smallest tile has the most)
-long long matvec_blocks(const pyto_operator_t* op) { return matvec_launch<32, 4>(make_dims(op)).nblocks; }
+// upper bound of the CTA count of any operator launch (sizes the per-CTA partial sums)
+long long matvec_blocks(const pyto_operator_t* op) { return matvec_block_bound(make_dims(op)); }
 
 int set_matvec_variant(int v) {
   if (v < 0 || (v > 3 && v < 8) || v > 10) return PYTO_ERR_ARG;
@@ -646,7 +669,7 @@ int set_matvec_variant(int v) {
 }
 
 int set_matvec32_variant(int v) {
-  if (v < 0 || (v > 5 && v < 8) || v > 14) return PYTO_ERR_ARG;
+  if (v < 0 || (v > 5 && v < 8) || v > 17) return PYTO_ERR_ARG;
   g_mv32_variant = v;
   return PYTO_OK;
 }

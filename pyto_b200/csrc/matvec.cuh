@@ -98,16 +98,35 @@ __device__ __forceinline__ void face_inv(const T (&G)[4], T& c00, T& c10, T& c01
   c11 = C + D;
 }
 
-// Number of node planes per CTA: aim at ~2 waves of 2 resident CTAs per SM
-// while keeping the one-layer halo overhead small.
-inline int matvec_zc(int bx, int by, int sz) {
+constexpr long long kMatvecMaxBlocks = 4096;  // CTA cap of the slab split
+
+// Node planes per CTA for bx x by tiles per plane with `slots` CTAs resident on the
+// device: of the splits into slabs of zc = ceil(sz / nb) planes (zc >= 4 unless
+// sz < 4, at most max(kMatvecMaxBlocks, bx by) CTAs), the one with the least
+// (waves of `slots` CTAs) x (zc + 2), the 2 standing for the recomputed halo layer and
+// the pipeline start of a slab.  A partly filled last wave leaves SMs idle for a
+// whole slab, so the split is chosen against the wave count, not a CTA target.
+inline int matvec_zc(int bx, int by, int sz, int slots) {
   const long long nxy = (long long)bx * by;
-  long long want = (2LL * kNumSMs * 2 + nxy - 1) / nxy;
-  if (want < 1) want = 1;
-  if (want > sz) want = sz;
-  int zc = (int)((sz + want - 1) / want);
-  if (zc < 4) zc = (sz < 4) ? sz : 4;
-  return zc;
+  const int zmin = sz < 4 ? sz : 4;
+  long long nbmax = kMatvecMaxBlocks / nxy;
+  const long long nbz_max = (sz + zmin - 1) / zmin;
+  if (nbmax > nbz_max) nbmax = nbz_max;
+  if (nbmax < 1) nbmax = 1;
+  if (slots < 1) slots = 1;
+  int best_zc = sz;
+  long long best = -1;
+  for (long long nb = 1; nb <= nbmax; ++nb) {
+    const int zc = (int)((sz + nb - 1) / nb);
+    if (zc < zmin) break;
+    const long long nbz = (sz + zc - 1) / zc;
+    const long long cost = ((nxy * nbz + slots - 1) / slots) * (zc + 2);
+    if (best < 0 || cost < best) {
+      best = cost;
+      best_zc = zc;
+    }
+  }
+  return best_zc;
 }
 
 struct MvLaunch {
@@ -117,14 +136,21 @@ struct MvLaunch {
 };
 
 template <int TX, int TY>
-inline MvLaunch matvec_launch(const GridDims& g) {
+inline MvLaunch matvec_launch(const GridDims& g, int slots) {
   MvLaunch L;
   const int bx = (g.sx + TX - 2) / (TX - 1), by = (g.sy + TY - 2) / (TY - 1);
-  L.zc = matvec_zc(bx, by, g.sz);
+  L.zc = matvec_zc(bx, by, g.sz, slots);
   const int bz = (g.sz + L.zc - 1) / L.zc;
   L.grid = dim3(bx, by, bz);
   L.nblocks = (long long)bx * by * bz;
   return L;
+}
+
+// Upper bound of the CTA count of every operator launch: a split never exceeds
+// max(kMatvecMaxBlocks, tiles per plane), and the 31 x 3-node tile has the most tiles.
+inline long long matvec_block_bound(const GridDims& g) {
+  const long long nxy = (long long)((g.sx + 30) / 31) * ((g.sy + 2) / 3);
+  return nxy > kMatvecMaxBlocks ? nxy : kMatvecMaxBlocks;
 }
 
 }  // namespace pyto

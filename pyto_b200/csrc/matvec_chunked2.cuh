@@ -34,8 +34,9 @@ struct ChunkTile2 {
 
 // Element core in the Hadamard basis (the arithmetic of k_matvec_chunked): adds the
 // bottom-face part of s K^ (Fb, Ft) to Gs and writes the top-face part to Gn.
-template <typename T>
-__device__ __forceinline__ void chunk_elem_core(const KHatT<T>& kh, T sv, const T (&Fb)[3][4], const T (&Ft)[3][4],
+// For packed FP32x2 values T, the FP32 coefficients are broadcast to both lanes.
+template <typename T, typename KC>
+__device__ __forceinline__ void chunk_elem_core(const KHatT<KC>& kh, T sv, const T (&Fb)[3][4], const T (&Ft)[3][4],
                                                 T (&Gs)[3][4], T (&Gn)[3][4]) {
 #pragma unroll
   for (int qp = 0; qp < 4; ++qp) {
@@ -61,7 +62,7 @@ __device__ __forceinline__ void chunk_elem_core(const KHatT<T>& kh, T sv, const 
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
           if (member_mode(q, d) == 0) continue;
-          const T kc = kh.b[q][3 * c + d];
+          const T kc = T(kh.b[q][3 * c + d]);
           o = first ? kc * v[d] : fma(kc, v[d], o);
           first = false;
         }
@@ -75,7 +76,12 @@ __device__ __forceinline__ void chunk_elem_core(const KHatT<T>& kh, T sv, const 
   }
 }
 
-template <typename T, int TY, bool DOT, bool MASKIN, int MINB>
+// PACK (FP32 only): the two elements of a thread go through the element core as the
+// two lanes of packed FP32x2 values (face transforms, z-combination, block operator,
+// accumulation and inverse transforms: one instruction for both).  Elements outside
+// the grid have s = 0 and staged values that are finite (zero-filled outside u), so
+// the core runs for both lanes and adds exact zeros for a missing element.
+template <typename T, int TY, bool DOT, bool MASKIN, int MINB, bool PACK = false>
 __global__ void __launch_bounds__(32 * TY, MINB)
     k_matvec_chunked2(GridDims g, KHatT<T> kh, const T* __restrict__ s, const uint8_t* __restrict__ mask,
                       const T* __restrict__ u, T* __restrict__ y, int zc, int mode, double* part, unsigned* counter,
@@ -232,65 +238,145 @@ __global__ void __launch_bounds__(32 * TY, MINB)
     if (Z0 - 1 + k <= Z1) issue_plane(Z0 - 1 + k);
     else cp_async_commit();
   }
-  // One element layer for both elements (see k_matvec_chunked for the roles of the
-  // register sets; here each role holds the two elements' arrays)
-  auto layer = [&](int ez, const T (&Fba)[3][4], const T (&Fbb)[3][4], T (&Fta)[3][4], T (&Ftb)[3][4],
-                   T (&Gsa)[3][4], T (&Gsb)[3][4], T (&Gna)[3][4], T (&Gnb)[3][4]) {
-    cp_async_wait_n<LOOK - 1>();
-    __syncthreads();
-    if (ez - 1 >= Z0) output(ez - 1);
-    if (ez + 1 + LOOK <= Z1) issue_plane(ez + 1 + LOOK);
-    else cp_async_commit();
-    face2(ez + 1, Fta, Ftb);
-    const T sva = sa_next, svb = sb_next;
-    eidx += pe;
-    const bool nxt = ez + 1 < Z1 && ez + 1 < g.nz;
-    sa_next = (in_a && nxt) ? __ldg(s + eidx) : T(0);
-    sb_next = (in_b && nxt) ? __ldg(s + eidx + g.nx) : T(0);
-    const bool lay = ez >= 0 && ez < g.nz;
-    if (in_a && lay) {
-      chunk_elem_core<T>(kh, sva, Fba, Fta, Gsa, Gna);
-    } else {
-#pragma unroll
-      for (int c = 0; c < 3; ++c)
-#pragma unroll
-        for (int f = 0; f < 4; ++f) Gna[c][f] = T(0);
-    }
-    if (in_b && lay) {
-      chunk_elem_core<T>(kh, svb, Fbb, Ftb, Gsb, Gnb);
-    } else {
-#pragma unroll
-      for (int c = 0; c < 3; ++c)
-#pragma unroll
-        for (int f = 0; f < 4; ++f) Gnb[c][f] = T(0);
-    }
-    if (ez >= Z0) {
-      T* scb = sc + (ez & 1) * (3 * TY * TX) + ty * TX + tx;
+  if constexpr (PACK) {
+    static_assert(sizeof(T) == 4, "packed form is FP32");
+    using P = packed::f32x2;
+    // face transforms of both elements from plane k as lane pairs (a, b)
+    auto face2p = [&](int k, P (&F)[3][4]) {
+      const int slot = slot_of(k);
+      const int pk = pn * k;
+      const int nl = n0l + pk, nm = n0m + pk, nh = n0h + pk;
+      const T* base = su + slot * SLOT + 3 * tx;
+      const T* pl = base + (2 * ty) * PITCH + ((3 * nl) & (CH - 1));
+      const T* pm = base + (2 * ty + 1) * PITCH + ((3 * nm) & (CH - 1));
+      const T* ph = base + (2 * ty + 2) * PITCH + ((3 * nh) & (CH - 1));
+      int ml0 = 0, ml1 = 0, mm0 = 0, mm1 = 0, mh0 = 0, mh1 = 0;
+      if (MASKIN) {
+        const uint8_t* mb = smk + slot * MSLOT + tx;
+        const uint8_t* ql = mb + (2 * ty) * MPITCH + (nl & 15);
+        const uint8_t* qm = mb + (2 * ty + 1) * MPITCH + (nm & 15);
+        const uint8_t* qh = mb + (2 * ty + 2) * MPITCH + (nh & 15);
+        ml0 = ql[0];
+        ml1 = ql[1];
+        mm0 = qm[0];
+        mm1 = qm[1];
+        mh0 = qh[0];
+        mh1 = qh[1];
+      }
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        T a00, a10, a01, a11, b00, b10, b01, b11;
-        face_inv(Gsa[c], a00, a10, a01, a11);
-        face_inv(Gsb[c], b00, b10, b01, b11);
-        cM[c] = (a11 + b10) + __shfl_down_sync(0xffffffffu, a01 + b00, 1);  // mid row, in the thread
-        cH[c] = b11 + __shfl_down_sync(0xffffffffu, b01, 1);                // high row, this thread's part
-        scb[c * TY * TX] = a10 + __shfl_down_sync(0xffffffffu, a00, 1);     // low row: the row below's high
+        T l0 = pl[c], l1 = pl[3 + c], m0 = pm[c], m1 = pm[3 + c], h0 = ph[c], h1 = ph[3 + c];
+        if (MASKIN) {
+          if ((ml0 >> c) & 1) l0 = T(0);
+          if ((ml1 >> c) & 1) l1 = T(0);
+          if ((mm0 >> c) & 1) m0 = T(0);
+          if ((mm1 >> c) & 1) m1 = T(0);
+          if ((mh0 >> c) & 1) h0 = T(0);
+          if ((mh1 >> c) & 1) h1 = T(0);
+        }
+        face_fwd(P(l0, m0), P(l1, m1), P(m0, h0), P(m1, h1), F[c]);
       }
+    };
+    auto layerp = [&](int ez, const P (&Fb)[3][4], P (&Ft)[3][4], P (&Gs)[3][4], P (&Gn)[3][4]) {
+      cp_async_wait_n<LOOK - 1>();
+      __syncthreads();
+      if (ez - 1 >= Z0) output(ez - 1);
+      if (ez + 1 + LOOK <= Z1) issue_plane(ez + 1 + LOOK);
+      else cp_async_commit();
+      face2p(ez + 1, Ft);
+      const P sv(sa_next, sb_next);  // 0 for an element outside the grid or the slab
+      eidx += pe;
+      const bool nxt = ez + 1 < Z1 && ez + 1 < g.nz;
+      sa_next = (in_a && nxt) ? __ldg(s + eidx) : T(0);
+      sb_next = (in_b && nxt) ? __ldg(s + eidx + g.nx) : T(0);
+      chunk_elem_core<P>(kh, sv, Fb, Ft, Gs, Gn);
+      if (ez >= Z0) {
+        T* scb = sc + (ez & 1) * (3 * TY * TX) + ty * TX + tx;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          P c00, c10, c01, c11;
+          face_inv(Gs[c], c00, c10, c01, c11);  // lane x: element a, lane y: element b
+          cM[c] = (c11.v.x + c10.v.y) + __shfl_down_sync(0xffffffffu, c01.v.x + c00.v.y, 1);
+          cH[c] = c11.v.y + __shfl_down_sync(0xffffffffu, c01.v.y, 1);
+          scb[c * TY * TX] = c10.v.x + __shfl_down_sync(0xffffffffu, c00.v.x, 1);
+        }
+      }
+    };
+    P FA[3][4], FB[3][4], GA[3][4], GB[3][4];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int f = 0; f < 4; ++f) GA[c][f] = P(0.0f);
+    cp_async_wait_n<LOOK - 1>();
+    __syncthreads();
+    if (Z0 - 1 + LOOK <= Z1) issue_plane(Z0 - 1 + LOOK);
+    else cp_async_commit();
+    face2p(Z0 - 1, FA);
+    for (int ez = Z0 - 1; ez < Z1; ez += 2) {
+      layerp(ez, FA, FB, GA, GB);
+      if (ez + 1 < Z1) layerp(ez + 1, FB, FA, GB, GA);
     }
-  };
+  } else {
+    // One element layer for both elements (see k_matvec_chunked for the roles of the
+    // register sets; here each role holds the two elements' arrays)
+    auto layer = [&](int ez, const T (&Fba)[3][4], const T (&Fbb)[3][4], T (&Fta)[3][4], T (&Ftb)[3][4],
+                     T (&Gsa)[3][4], T (&Gsb)[3][4], T (&Gna)[3][4], T (&Gnb)[3][4]) {
+      cp_async_wait_n<LOOK - 1>();
+      __syncthreads();
+      if (ez - 1 >= Z0) output(ez - 1);
+      if (ez + 1 + LOOK <= Z1) issue_plane(ez + 1 + LOOK);
+      else cp_async_commit();
+      face2(ez + 1, Fta, Ftb);
+      const T sva = sa_next, svb = sb_next;
+      eidx += pe;
+      const bool nxt = ez + 1 < Z1 && ez + 1 < g.nz;
+      sa_next = (in_a && nxt) ? __ldg(s + eidx) : T(0);
+      sb_next = (in_b && nxt) ? __ldg(s + eidx + g.nx) : T(0);
+      const bool lay = ez >= 0 && ez < g.nz;
+      if (in_a && lay) {
+        chunk_elem_core<T>(kh, sva, Fba, Fta, Gsa, Gna);
+      } else {
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+          for (int f = 0; f < 4; ++f) Gna[c][f] = T(0);
+      }
+      if (in_b && lay) {
+        chunk_elem_core<T>(kh, svb, Fbb, Ftb, Gsb, Gnb);
+      } else {
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+          for (int f = 0; f < 4; ++f) Gnb[c][f] = T(0);
+      }
+      if (ez >= Z0) {
+        T* scb = sc + (ez & 1) * (3 * TY * TX) + ty * TX + tx;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          T a00, a10, a01, a11, b00, b10, b01, b11;
+          face_inv(Gsa[c], a00, a10, a01, a11);
+          face_inv(Gsb[c], b00, b10, b01, b11);
+          cM[c] = (a11 + b10) + __shfl_down_sync(0xffffffffu, a01 + b00, 1);  // mid row, in the thread
+          cH[c] = b11 + __shfl_down_sync(0xffffffffu, b01, 1);                // high row, this thread's part
+          scb[c * TY * TX] = a10 + __shfl_down_sync(0xffffffffu, a00, 1);     // low row: the row below's high
+        }
+      }
+    };
 
-  T FAa[3][4], FAb[3][4], FBa[3][4], FBb[3][4], GAa[3][4], GAb[3][4], GBa[3][4], GBb[3][4];
+    T FAa[3][4], FAb[3][4], FBa[3][4], FBb[3][4], GAa[3][4], GAb[3][4], GBa[3][4], GBb[3][4];
 #pragma unroll
-  for (int c = 0; c < 3; ++c)
+    for (int c = 0; c < 3; ++c)
 #pragma unroll
-    for (int f = 0; f < 4; ++f) GAa[c][f] = GAb[c][f] = T(0);
-  cp_async_wait_n<LOOK - 1>();
-  __syncthreads();
-  if (Z0 - 1 + LOOK <= Z1) issue_plane(Z0 - 1 + LOOK);
-  else cp_async_commit();
-  face2(Z0 - 1, FAa, FAb);
-  for (int ez = Z0 - 1; ez < Z1; ez += 2) {
-    layer(ez, FAa, FAb, FBa, FBb, GAa, GAb, GBa, GBb);
-    if (ez + 1 < Z1) layer(ez + 1, FBa, FBb, FAa, FAb, GBa, GBb, GAa, GAb);
+      for (int f = 0; f < 4; ++f) GAa[c][f] = GAb[c][f] = T(0);
+    cp_async_wait_n<LOOK - 1>();
+    __syncthreads();
+    if (Z0 - 1 + LOOK <= Z1) issue_plane(Z0 - 1 + LOOK);
+    else cp_async_commit();
+    face2(Z0 - 1, FAa, FAb);
+    for (int ez = Z0 - 1; ez < Z1; ez += 2) {
+      layer(ez, FAa, FAb, FBa, FBb, GAa, GAb, GBa, GBb);
+      if (ez + 1 < Z1) layer(ez + 1, FBa, FBb, FAa, FAb, GBa, GBb, GAa, GAb);
+    }
   }
   cp_async_wait_n<0>();
   __syncthreads();

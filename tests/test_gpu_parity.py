@@ -79,7 +79,7 @@ def test_matvec_tile_variants(variant, nel):
 @pytest.mark.parametrize("nel", [(1, 1, 1), (33, 9, 17), (7, 20, 5), (70, 11, 30), (62, 14, 3), (96, 48, 40)])
 @pytest.mark.parametrize("f32", [False, True])
 def test_matvec_chunked_equals_tile_kernel(nel, f32):
-    """The chunk-staged kernels (variants 8-14; 12-14 with two element rows per thread)
+    """The chunk-staged kernels (variants 8-17; 12-17 with two element rows per thread, 15-17 packed FP32x2)
     perform the tile kernel's arithmetic in the
     same order (up to the compiler's FMA contraction): equal results to a few ulps in every
     mask mode, with and without the fused dot product, and run to run bitwise; a u that
@@ -93,7 +93,7 @@ def test_matvec_chunked_equals_tile_kernel(nel, f32):
     s = _dev(rng.uniform(0.01, 1.0, m["num_elems"])).to(dt)
     ubuf = _dev(rng.normal(size=3 * m["num_nodes"] + 1)).to(dt)
     which, mv = (1, g.matvec_f32) if f32 else (0, g.matvec)
-    variants = (8, 9, 10, 11, 12, 13, 14) if f32 else (8, 9, 10)
+    variants = (8, 9, 10, 11, 12, 13, 14, 15, 16, 17) if f32 else (8, 9, 10)
     try:
         for u in (ubuf[:-1], ubuf[1:]):
             for mode in (0, 1, 2, 3):
@@ -317,7 +317,7 @@ def test_boundary_lists_follow_fixed_dofs():
     assert defl.bel_list.numel() == want
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 8, 9, 10, 11, 12, 13, 14])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17])
 def test_matvec_f32_matches_fp64(variant):
     """FP32 operator: relative error of K(s)u against the FP64 operator at FP32 rounding
     (variants 4, 5: tensor-core contraction with BF16 split operands, ~2^-16)."""
