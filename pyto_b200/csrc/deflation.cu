@@ -804,7 +804,7 @@ __global__ void __launch_bounds__(1024) k_chunk_ptr(int ngroups, const int32_t* 
 
 // adds the contribution of boundary element e to the 6 mode sums of group G
 template <typename T>
-__device__ __forceinline__ void rk_element(const GridDims& g, const KHat& kh, const DeflP& dp, int e, int G, T se,
+__device__ __forceinline__ void rk_element(const GridDims& g, const KHatT<T>& kh, const DeflP& dp, int e, int G, T se,
                                            const uint8_t* __restrict__ fl, const int32_t* __restrict__ ngrp,
                                            double c0, double c1, double c2, const T* __restrict__ z,
                                            double (&acc)[6]) {
@@ -832,7 +832,7 @@ __device__ __forceinline__ void rk_element(const GridDims& g, const KHat& kh, co
 #pragma unroll
     for (int f = 0; f < 4; ++f) Gb[c][f] = Gt[c][f] = T(0);
   }
-  hex8_core<T>(kh, se, Fb, Ft, Gb, Gt);
+  hex8_core<T, KHatT<T>>(kh, se, Fb, Ft, Gb, Gt);
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     face_inv(Gb[c], u[c][0], u[c][1], u[c][2], u[c][3]);
@@ -870,7 +870,7 @@ __device__ __forceinline__ int div_by(int a, int d, double inv) {
 // rk_element for an element without fixed DOFs whose corners in G are the bits of
 // cmask (from the list's per-entry metadata): no group or mask loads, no selects
 template <typename T>
-__device__ __forceinline__ void rk_element_free(const GridDims& g, const KHat& kh, const DeflP& dp, int e,
+__device__ __forceinline__ void rk_element_free(const GridDims& g, const KHatT<T>& kh, const DeflP& dp, int e,
                                                 unsigned cmask, T se, double inx, double iny, double c0, double c1,
                                                 double c2, const T* __restrict__ z, double (&acc)[6]) {
   const int r = div_by(e, g.nx, inx);
@@ -894,7 +894,7 @@ __device__ __forceinline__ void rk_element_free(const GridDims& g, const KHat& k
 #pragma unroll
     for (int f = 0; f < 4; ++f) Gb[c][f] = Gt[c][f] = T(0);
   }
-  hex8_core<T>(kh, se, Fb, Ft, Gb, Gt);
+  hex8_core<T, KHatT<T>>(kh, se, Fb, Ft, Gb, Gt);
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
     face_inv(Gb[c], u[c][0], u[c][1], u[c][2], u[c][3]);
@@ -920,7 +920,7 @@ __device__ __forceinline__ void rk_element_free(const GridDims& g, const KHat& k
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kRkThreads, sizeof(T) == 4 ? 6 : 4) k_restrict_K(GridDims g, KHat kh, DeflP dp, const T* __restrict__ s,
+__global__ void __launch_bounds__(kRkThreads, sizeof(T) == 4 ? 6 : 4) k_restrict_K(GridDims g, KHatT<T> kh, DeflP dp, const T* __restrict__ s,
                                                            const uint8_t* __restrict__ fl,
                                                            const int32_t* __restrict__ ngrp,
                                                            const double* __restrict__ gc,
@@ -1500,9 +1500,9 @@ template <typename T>
 static int coarse_update_K(const pyto_operator_t* op, const GridDims& g, const DeflP& dp, const pyto_deflation_t* d,
                            const T* s, const T* z, T* p, const DpcgWs& W, int nchunks, const KrylovState* S,
                            int first, cudaStream_t st) {
-  k_restrict_K<T><<<nchunks, kRkThreads, 0, st>>>(g, make_khat(op), dp, s, W.fl, d->node_group, d->group_center,
-                                                  d->bel_ptr, d->bel_list, W.cptr, W.cgrp, z, W.rpart, W.gcount,
-                                                  W.cv, S, d->bel_meta);
+  k_restrict_K<T><<<nchunks, kRkThreads, 0, st>>>(g, make_khat_t<T>(make_khat(op)), dp, s, W.fl, d->node_group,
+                                                  d->group_center, d->bel_ptr, d->bel_list, W.cptr, W.cgrp, z,
+                                                  W.rpart, W.gcount, W.cv, S, d->bel_meta);
   PYTO_COUNT(1);
   if ((dp.nc & 1) == 0) {
     k_gemv_rows<<<(int)((dp.nc + 3) / 4), 128, 0, st>>>(dp.nc, d->coarse_inv, W.cv, W.mu, first ? nullptr : S);

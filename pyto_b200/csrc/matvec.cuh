@@ -32,14 +32,29 @@ struct MvTile {
   static constexpr int LOADS = (PLANE_D + NT - 1) / NT;
 };
 
+// The block operator's coefficients in the kernel's precision (no per-use conversion
+// from the FP64 KHat in FP32 kernels).
+template <typename T>
+struct KHatT {
+  T b[8][9];
+};
+
+template <typename T>
+inline KHatT<T> make_khat_t(const KHat& kh) {
+  KHatT<T> k;
+  for (int q = 0; q < 8; ++q)
+    for (int i = 0; i < 9; ++i) k.b[q][i] = (T)kh.b[q][i];
+  return k;
+}
+
 // Mode of component c in parity class q (the pair (c, q ^ (1<<c))).
 __host__ __device__ constexpr int member_mode(int q, int c) { return q ^ (1 << c); }
 
 // Element core in the Hadamard basis.  Fb/Ft: face transforms of bottom/top
 // faces, [comp][face mode].  Adds the bottom-face part of s*K^u to Gb and the
-// top-face part to Gt.
-template <typename T>
-__device__ __forceinline__ void hex8_core(const KHat& kh, T s, const T (&Fb)[3][4], const T (&Ft)[3][4],
+// top-face part to Gt.  KH: KHat or KHatT<T> (coefficients b[8][9]).
+template <typename T, typename KH = KHat>
+__device__ __forceinline__ void hex8_core(const KH& kh, T s, const T (&Fb)[3][4], const T (&Ft)[3][4],
                                           T (&Gb)[3][4], T (&Gt)[3][4]) {
 #pragma unroll
   for (int q = 0; q < 8; ++q) {

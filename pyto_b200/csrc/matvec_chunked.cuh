@@ -26,19 +26,6 @@
 
 namespace pyto {
 
-template <typename T>
-struct KHatT {
-  T b[8][9];
-};
-
-template <typename T>
-inline KHatT<T> make_khat_t(const KHat& kh) {
-  KHatT<T> k;
-  for (int q = 0; q < 8; ++q)
-    for (int i = 0; i < 9; ++i) k.b[q][i] = (T)kh.b[q][i];
-  return k;
-}
-
 template <typename T, int TY, bool GS = false>
 struct ChunkTile {
   static constexpr int TX = 32, NT = TX * TY, PX = TX + 1, PY = TY + 1;
