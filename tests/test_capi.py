@@ -77,3 +77,19 @@ def test_workspace_sizes_are_reported():
     for k in (A.WS_REDUCE, A.WS_PCG, A.WS_DPCG):
         assert A.ws_bytes(op, k) > 0
     assert A.ws_bytes(op, A.WS_PCG) >= 3 * 8 * 3 * 13 * 7 * 7
+
+
+def test_autotuner_variants_are_the_ones_the_library_accepts():
+    """Every operator variant the autotuner times is accepted by pyto_tune, and the
+    numbers around them are rejected (host-side check only: no kernel runs)."""
+    from pyto_b200.autotune import VARIANTS, VARIANTS_F32
+    L = A.lib()
+    try:
+        for which, listed in ((0, VARIANTS), (1, VARIANTS_F32)):
+            for v in range(-1, max(listed) + 3):
+                rc = L.pyto_tune(which, v)
+                assert (rc == 0) == (v in listed), (which, v, rc)
+                if rc:
+                    assert rc == A.ERR_ARG, (which, v, rc)
+    finally:
+        assert L.pyto_tune(0, 2) == 0 and L.pyto_tune(1, 16) == 0  # library defaults
