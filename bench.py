@@ -33,10 +33,12 @@ METRIC = "time to rel-residual 1e-8 per 5.4M-DOF solve, mixed vs FP64 GPU; % HBM
 NEL = (192, 96, 96)
 RTOL = 1e-8
 # DRAM bytes (read + write) of one K(s)u launch on this grid in the solver's mask mode
-# (output mask only), from ncu captures of the two operator kernels (profiles/
-# k_matvec_192x96x96.md; cold caches, so the y writes, which stay in L2 during the
-# launch, are mostly not counted)
+# (output mask only), from one ncu capture of each operator kernel of this build (cold
+# caches, so the y writes, which stay in L2 during the launch, are mostly not counted).
+# They are constants of the kernels, not measured by this script.
 TRAFFIC = {"f32": 30771456, "f64": 71395328}
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on this grid "
+                  "(kernel_bench --kernel matvec32 --variant32 16 / --kernel matvec --variant 2, --mode 2)")
 KERNEL = {"f32": "k_matvec_chunked2<float, packed FP32x2> (two element rows per thread, variant 16)",
           "f64": "k_matvec<double> (tile, variant 2)"}
 
@@ -184,37 +186,98 @@ def time_matvec(P, reps=30, precision="f64"):
     return e0.elapsed_time(e1) / reps / 1e3
 
 
-def cpu_reference(sample_nel=(60, 30, 30)):
-    """PyTO's own path for this solve, restated by the oracle: COO assembly +
-    Dirichlet elimination + scipy cg with the Jacobi preconditioner
-    (src/hex_structural_fea.py:87-129, src/linear_solvers.py:164-168), timed on
-    a bounded sample (the 60x30x30 grid with the same density recipe) and scaled
-    to 192x96x96: assembly by element count, CG by DOF x iterations, with the
-    iteration count scaled by grid refinement (Jacobi-PCG iterations grow
-    linearly with 1/h)."""
+def cpu_inputs(nel=NEL, groups=432):
+    """The bench input on the host, for the CPU restatement of the reference's path:
+    cantilever load and clamp, rho = H(U[0.01,1], seed 0)/Hs (r = 2), SIMP p = 3,
+    Emin = 1e-9, and the reference's node-box deflation groups."""
     import oracle as O
-    from pyto_b200.problems import uniform_density
-    m = O.grid_mesh(*sample_nel)
-    f, fixed = O.cantilever_bc(m)
-    H, Hs = O.smoothing_filter(m, 2.0)
-    rho = (H @ uniform_density(sample_nel, 0.01, 1.0, seed=0)) / Hs
-    Ke = O.ke_hex8(1.0, 0.3)
+    from oracle import cpu
+    from pyto_b200.deflation import DeflationSolver
+    from pyto_b200.hex_mesher import HexMesher
+    from pyto_b200.problems import cantilever, uniform_density
+    mesh = HexMesher()
+    mesh.grid_mesh(nel, (1.0, 1.0, 1.0))
+    f, fixed = cantilever(mesh)
+    rho = cpu.density_filter(nel, uniform_density(nel, 0.01, 1.0, seed=0), 2.0)
+    ds = DeflationSolver(modes=6, shift=1e-14, shift_relative=True)
+    ds.create_deflation_groups(mesh, groups)
+    return dict(nel=nel, f=f, fixed=fixed, s=O.simp_scaling(rho, 3.0, 1e-9), ke=O.ke_hex8(1.0, 0.3),
+                group=ds.ws_nodeGroupNumber, center=ds.ws_groupCenter)
+
+
+def cpu_solve(I, max_iters=5000):
+    """One solve of the reference's CPU path, restated in C with OpenMP (oracle/
+    hex8_cpu.c): CSR assembly of K_ff (src/hex_structural_fea.py:87-102,
+    src/bound_cond.py:40-70), W^T K W + shift and its dense Cholesky, and the
+    reference's deflated PCG recurrence with two products with K per iteration
+    (src/deflation.py:504-584), stopped on ||r|| < 1e-8 ||b||.  Returns the times of
+    the three phases, the iterations and the solution."""
+    from oracle import cpu
+    fea = cpu.CpuFEA(I["nel"], I["ke"], I["fixed"])
+    t_asm = fea.assemble(I["s"])
+    u, info = fea.dpcg(I["f"], I["group"], I["center"], modes=6, shift=1e-14, shift_relative=True, rtol=RTOL,
+                       max_iters=max_iters)
+    fea.close()
+    info["assemble_s"] = t_asm
+    return u, info
+
+
+def cpu_sample(iters_full, n_sample=30):
+    """Bounded sample of the CPU path on the full bench grid: assembly, coarse set-up
+    and n_sample deflated-PCG iterations, scaled to a whole solve by the iteration
+    count of the same recurrence (the GPU FP64 solve of this run uses it, with the
+    same coarse space and stopping rule)."""
+    from oracle import cpu
+    I = cpu_inputs()
+    _, info = cpu_solve(I, max_iters=n_sample)
+    per_it = info["solve_s"] / max(1, info["iters"])
+    value = info["assemble_s"] + info["setup_s"] + per_it * iters_full
+    return dict(value=value, unit="s", cores=cpu.threads(), kind="port",
+                sample=(f"C/OpenMP restatement of the reference's CPU path (CSR assembly of K_ff, W^T K W + dense "
+                        f"Cholesky, deflated PCG with 2 SpMV per iteration; oracle/hex8_cpu.c) on the full "
+                        f"{NEL[0]}x{NEL[1]}x{NEL[2]} grid: assembly {info['assemble_s']:.2f} s, coarse set-up "
+                        f"{info['setup_s']:.2f} s, {info['iters']} iterations {info['solve_s']:.2f} s "
+                        f"({per_it * 1e3:.1f} ms each), scaled to the {iters_full} iterations of the same recurrence"),
+                threads=cpu.threads(), os_cpu_count=os.cpu_count())
+
+
+def reference_arm(args):
+    """The reference arm: the reference's CPU path (restated in C, all host threads)
+    solving the bench's full problem to rel-residual 1e-8, measured end to end
+    (assembly + coarse set-up + iterations), one step per timed solve."""
+    from oracle import cpu
+    cpu.build()
     t0 = time.perf_counter()
-    K = O.assemble_K(m, O.simp_scaling(rho, 3.0, 1e-9), Ke)
-    A_, b_, free = O.impose_dirichlet_bc(K, f, fixed, np.zeros(len(fixed)))
-    t1 = time.perf_counter()
-    x, iters = O.pcg_scipy(A_, b_, O.jacobi_inverse(A_), RTOL)
-    t2 = time.perf_counter()
-    ne1, nd1 = m["num_elems"], len(free)
-    ne2 = int(np.prod(NEL))
-    nd2 = 3 * (NEL[0] + 1) * (NEL[1] + 1) * (NEL[2] + 1) - 3 * (NEL[1] + 1) * (NEL[2] + 1)
-    ratio_it = NEL[0] / sample_nel[0]
-    est = (t1 - t0) * ne2 / ne1 + (t2 - t1) * (nd2 / nd1) * ratio_it
-    return dict(value=est, unit="s", cores=1, kind="port",
-                sample=(f"oracle restatement of the reference's per-solve path (COO assembly + elimination + scipy "
-                        f"Jacobi-PCG, single-threaded SpMV) on {sample_nel[0]}x{sample_nel[1]}x{sample_nel[2]}: "
-                        f"assembly {t1 - t0:.2f}s, {iters} CG iters {t2 - t1:.2f}s; scaled x{ne2 / ne1:.1f} "
-                        f"(elements) and x{nd2 / nd1:.1f} DOF x {ratio_it:.1f} iterations"))
+    I = cpu_inputs()
+    t_prep = time.perf_counter() - t0
+    steps = max(1, min(args.steps, args.ref_steps))
+    times, infos = [], []
+    for _ in range(steps):
+        t1 = time.perf_counter()
+        u, info = cpu_solve(I)
+        times.append(time.perf_counter() - t1)
+        infos.append(info)
+    value = sum(times) / steps
+    info = infos[-1]
+    C = float(I["f"] @ u)
+    sample = (f"full {NEL[0]}x{NEL[1]}x{NEL[2]} solve to ||r|| < 1e-8 ||b|| ({info['iters']} iterations, true "
+              f"rel-residual {info['true_rel_res']:.2e}): C/OpenMP restatement of the reference's CPU path (CSR "
+              f"assembly of K_ff {info['assemble_s']:.2f} s, W^T K W + dense Cholesky {info['setup_s']:.2f} s, deflated "
+              f"PCG with 2 SpMV per iteration {info['solve_s']:.2f} s; oracle/hex8_cpu.c), "
+              f"{cpu.threads()} OpenMP threads of {os.cpu_count()} host CPUs")
+    line = {"metric": METRIC, "value": value, "unit": "s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": steps, "warmup": 0, "ms_per_step": value * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{NEL[0]}x{NEL[1]}x{NEL[2]} hex8 cantilever, 5447811 DOF, rho = H(U[0.01,1], "
+                                   "seed 0)/Hs r=2, SIMP p=3 Emin=1e-9",
+                       "form": "fp64 deflated PCG (Jacobi), 432 node-box groups x 6 rigid modes, dense coarse "
+                               "Cholesky, ||r|| < 1e-8 ||b||",
+                       "iterations": info["iters"], "true_rel_res": info["true_rel_res"], "compliance": C,
+                       "input_prep_s": t_prep, "omp_threads": cpu.threads(), "os_cpu_count": os.cpu_count(),
+                       "per_step_s": times},
+            "cpu_baseline": {"value": value, "unit": "s", "cores": cpu.threads(), "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
 
 
 def main():
@@ -230,6 +293,9 @@ def main():
     ap.add_argument("--form", default="mixed", choices=["mixed", "fp64"],
                     help="timed solver: FP64 refinement around FP32 deflated PCG, or plain FP64 deflated PCG")
     ap.add_argument("--delta", type=float, default=1e-1, help="mixed form: FP64 residual update each time the FP32 residual drops by this factor")
+    ap.add_argument("--ref-steps", type=int, default=1, help="reference arm: full CPU solves timed (at most --steps)")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the 20-iteration OC run and the batched workload that ride along in the line")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -239,14 +305,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        ref = cpu_reference()
-        line = {"metric": METRIC, "value": ref["value"], "unit": "s", "impl": "reference", "n_gpus": args.gpus,
-                "steps": 1, "warmup": 0, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f64", "data": "synthetic",
-                "config": {"workload": "192x96x96 hex8 cantilever solve to rel-residual 1e-8 (5,447,811 DOF)"},
-                "cpu_baseline": ref, "e2e": {"value": ref["value"], "unit": "s", "h2d_bytes_per_step": 0,
-                                             "d2h_bytes_per_step": 0}}
-        print(json.dumps(line))
+        reference_arm(args)
         return
 
     import torch
@@ -343,14 +402,29 @@ def main():
         ach = nbytes / t_mv / 1e9
         rl[prec] = {"bound": "hbm", "kernel": KERNEL[prec] + " matrix-free K(s)u",
                     "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak, "peak_kind": peak_kind,
-                    "traffic": TRAFFIC.get(prec), "launch_ms": t_mv * 1e3, "algorithmic_bytes": int(nbytes)}
+                    "traffic": TRAFFIC.get(prec), "traffic_source": TRAFFIC_SOURCE, "launch_ms": t_mv * 1e3,
+                    "algorithmic_bytes": int(nbytes)}
     main_prec = "f32" if args.form == "mixed" else "f64"
+
+    # the other two workloads of the benchmarked configurations, outside the timed
+    # region: a 20-iteration OC run on this grid (mixed solver) and the batched form
+    extra = {}
+    if not args.no_extra and world == 1:
+        from pyto_b200 import kernel_bench as KB
+        try:
+            extra["oc20"] = KB.run_oc(nel, 20, "mixed", args.groups)
+        except Exception as ex:  # pragma: no cover
+            extra["oc20"] = {"error": str(ex)}
+        try:
+            extra["batch"] = KB.run_batch(64, reps=3, tune=True)
+        except Exception as ex:  # pragma: no cover
+            extra["batch"] = {"error": str(ex)}
 
     if rank == 0:
         cpu = None
         if not args.no_cpu and world == 1:
             try:
-                cpu = cpu_reference()
+                cpu = cpu_sample(info_other.iters if other == "fp64" else iters)
             except Exception as ex:  # pragma: no cover
                 cpu = {"value": None, "error": str(ex)}
         line = {
@@ -371,7 +445,7 @@ def main():
                                        f"(reference box partition), dense FP64 coarse inverse",
                        "iterations": iters, "refinement_cycles": cycles, "true_rel_res": trr, "l2": "inputs larger than L2 (~0.6 GB moved per "
                                                                           "iteration)",
-                       "parallelism": f"replicas x{world}"},
+                       "parallelism": f"replicas x{world}", **extra},
             "e2e": {"value": e2e, "unit": "s", "h2d_bytes_per_step": int(rho_host.numel() * 8),
                     "d2h_bytes_per_step": int(u_host.numel() * 8)},
             "gpu_launches": int(launches),

@@ -204,7 +204,9 @@ int pyto_tensor_core_status(int reset);
  * array inside the library (~64 KB held on every GPU that loads it until process
  * exit); launches needing more than 8192 matvec blocks return PYTO_ERR_TOO_LARGE.  The
  * first call on a device looks up the array's device address and should precede any
- * stream capture; calls that overlap on the GPU race on the shared array. */
+ * stream capture; calls that overlap on the GPU race on the shared array.  The address
+ * is kept for the life of the process: after a cudaDeviceReset (or any reset of the
+ * device's primary context) this entry point must not be called again in that process. */
 int pyto_matvec_dot_noalloc(const pyto_operator_t* op, const double* s, const uint8_t* mask,
                             const double* u, double* y, int mode, double* dot, void* stream);
 /* Jacobi data: diag(K)[3n+c] = kdiag[c] * sum_{e ni n} s_e.  Writes winv[n] = 1/sum s

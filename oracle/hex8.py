@@ -26,7 +26,7 @@ __all__ = [
     "compliance_and_gradient", "postprocess", "pnorm_stress_and_sensitivity",
     "solution_dotproduct_and_gradient", "smoothing_filter",
     "volume_constraint", "oc_update", "elements_with_forces", "topopt_oc",
-    "cantilever_bc", "matvec_free",
+    "cantilever_bc", "matvec_free", "matvec_ebe",
 ]
 
 
@@ -238,6 +238,38 @@ def matvec_free(mesh, s, Ke, u, fixed):
     v[fixed] = 0.0
     y = K @ v
     y[fixed] = 0.0
+    return y
+
+
+def matvec_ebe(nel, s, Ke, u, fixed=None, chunk=1 << 20):
+    """K(s) u without assembling K, for grids too large for a CSR on the host:
+    y = sum_e s_e Ke u_e scattered to the element's 24 DOFs (the action of the
+    matrix assembled at src/hex_structural_fea.py:87-102), element corners in the
+    order of src/hex_mesher.py:120-124.  With ``fixed`` the reduced operator of
+    src/bound_cond.py:40-70 is applied on full-length vectors (fixed DOFs of u
+    read as 0, of y written as 0).  Elements are processed in z-slabs of about
+    ``chunk`` elements, so memory stays a few times the vector size."""
+    nx, ny, nz = (int(v) for v in nel)
+    sx, sy = nx + 1, ny + 1
+    U = np.array(u, dtype=np.float64, copy=True)
+    if fixed is not None:
+        U[np.asarray(fixed)] = 0.0
+    U = U.reshape(nz + 1, sy, sx, 3)
+    Y = np.zeros_like(U)
+    S = np.asarray(s, dtype=np.float64).reshape(nz, ny, nx)
+    corners = [(0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0), (0, 0, 1), (1, 0, 1), (1, 1, 1), (0, 1, 1)]
+    dz = max(1, chunk // max(1, nx * ny))
+    for z0 in range(0, nz, dz):
+        z1 = min(nz, z0 + dz)
+        ue = np.concatenate([U[z0 + c[2]:z1 + c[2], c[1]:c[1] + ny, c[0]:c[0] + nx, :] for c in corners],
+                            axis=-1).reshape(-1, 24)
+        ye = (ue @ Ke.T) * S[z0:z1].reshape(-1, 1)
+        ye = ye.reshape(z1 - z0, ny, nx, 24)
+        for k, c in enumerate(corners):
+            Y[z0 + c[2]:z1 + c[2], c[1]:c[1] + ny, c[0]:c[0] + nx, :] += ye[..., 3 * k:3 * k + 3]
+    y = Y.reshape(-1)
+    if fixed is not None:
+        y[np.asarray(fixed)] = 0.0
     return y
 
 

@@ -160,8 +160,12 @@ _WS: dict = {}
 
 def workspace(nbytes: int, device, tag: str = "ws") -> torch.Tensor:
     """A cached uint8 device buffer of at least nbytes (grows, never shrinks).
-    Buffers are keyed by tag so concurrent uses on one stream do not alias."""
-    key = (str(device), tag)
+
+    Buffers are keyed by (device, current stream, tag): uses under one tag on one
+    stream are ordered by that stream, and a buffer is only ever used on the stream
+    it was allocated on, so when a grown buffer replaces it the caching allocator
+    reuses the old block only after the work already queued on that stream."""
+    key = (str(device), stream_ptr(device), tag)
     buf = _WS.get(key)
     if buf is None or buf.numel() < nbytes:
         buf = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device)

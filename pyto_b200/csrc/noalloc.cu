@@ -13,7 +13,10 @@
 // process exits.  Its host-side name is only a stand-in for the device
 // symbol, so its device address is looked up with cudaGetSymbolAddress, once
 // per device, the first time the entry point runs with that device current;
-// that first call should therefore come before any stream capture.  All calls
+// that first call should therefore come before any stream capture.  The cached
+// address is not refreshed: a cudaDeviceReset (or a reset of the primary
+// context) can move the array, so after one this entry point must not be
+// called again in the same process.  All calls
 // share the one array: the completion counter is cleared at every call, and
 // two calls whose kernels overlap on the GPU (different streams, or different
 // host threads) race on it, so callers must order them.

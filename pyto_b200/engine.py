@@ -355,7 +355,12 @@ class BatchSolver:
     element scaling and the right-hand side.  Problems that share one DeviceDeflation
     are load cases of one design (same grid and s): its coarse inverse is built once
     per launch.  ``launch()`` solves all of them; rewrite the s and b tensors in place
-    and launch again for new designs and loads.  Solutions are in ``self.u``."""
+    and launch again for new designs and loads.  Solutions are in ``self.u``.
+
+    The graph holds the device addresses of every buffer it reads.  Only the contents
+    of s and b may change between launches: a grid whose fixed DOFs were reset (which
+    rebuilds its deflation space's boundary lists) or a deflation space whose lists
+    were rebuilt makes ``launch()`` raise; build a new BatchSolver then."""
 
     def __init__(self, problems, rtol=1e-8, max_iters=5000, stop_rule=0):
         self.problems = list(problems)
@@ -364,12 +369,16 @@ class BatchSolver:
             raise ValueError("empty batch")
         self.items = (A.BatchItem * n)()
         self.u, self._ws = [], []
+        self._captured = []  # per problem: what the graph's kernel arguments point at
         dev = None
         for k, (grid, defl, s, b) in enumerate(self.problems):
             dev = grid.device
             defl.sync(grid)
             if not defl.use_boundary_lists or defl.struct.bel_count <= 0:
                 raise ValueError("batched solves need the boundary element lists of the deflation space")
+            # the references keep the captured buffers alive (no address reuse while the
+            # graph exists); launch() compares them with the current ones
+            self._captured.append((grid, grid.mask_version, defl, defl.bel_ptr, defl.bel_list, defl.bel_meta))
             nb = A.ws_bytes(grid.op, A.WS_DPCG)
             ws = torch.empty(nb, dtype=torch.uint8, device=dev)  # one workspace per problem
             u = torch.zeros(grid.ndof, dtype=F64, device=dev)
@@ -382,7 +391,15 @@ class BatchSolver:
         self.handle = C.c_void_p()
         A.call("pyto_batch_create", self.items, n, C.byref(self.cfg), C.byref(self.handle), A.stream_ptr(dev))
 
+    def _check_captured(self):
+        for k, (grid, version, defl, bptr, blist, bmeta) in enumerate(self._captured):
+            if grid.mask_version != version or defl.mask_version != version or defl.bel_ptr is not bptr \
+                    or defl.bel_list is not blist or defl.bel_meta is not bmeta:
+                raise RuntimeError(f"batch problem {k}: the fixed DOFs or the deflation boundary lists changed "
+                                   "after the batch was created; create a new BatchSolver")
+
     def launch(self):
+        self._check_captured()
         A.call("pyto_batch_launch", self.handle, A.stream_ptr(self.device))
         return self
 

@@ -127,14 +127,19 @@ def main(argv=None):
 
 
 def oc_bench(a):
+    print(json.dumps(run_oc(tuple(int(v) for v in a.nel.split(",")), a.iters, a.precision, a.groups,
+                            a.warm_start)))
+
+
+def run_oc(nel, n_iters=20, precision="mixed", groups=432, warm_start=False):
     """OC topology optimisation through the reference-named driver (topopt_ocm) on the
     cantilever: rho0 = volfrac, sensitivity filter r = 1.5, volfrac 0.3, move 0.2, each
-    FEA solve by the deflated PCG (432 node-box groups x 6 modes, rtol 1e-8)."""
+    FEA solve by the deflated PCG (node-box groups x 6 modes, rtol 1e-8).  Returns the
+    wall time of n_iters design iterations after a one-iteration warm-up."""
     from . import bound_cond, hex_structural_fea, linear_solvers, mat_lib, topopt_common as tc, topopt_ocm
     from . import topopt_material_model as tmm
     from .deflation import DeflationSolver
     tmm._EVOID_RELATIVE = 1e-9
-    nel = tuple(int(v) for v in a.nel.split(","))
     mesh = HexMesher()
     mesh.grid_mesh(nel, (1.0, 1.0, 1.0))
     f, fixed = cantilever(mesh)
@@ -142,9 +147,9 @@ def oc_bench(a):
     bc = bound_cond.BC(force=f, fixed_dofs=fixed, dirichlet_values=np.zeros(len(fixed)))
     mat = mat_lib.create_material_with_defaults("unit", youngs_modulus=1.0, poissons_ratio=0.3)
     ds = DeflationSolver(modes=6, shift=1e-14, shift_relative=True)
-    ds.create_deflation_groups(mesh, a.groups)
+    ds.create_deflation_groups(mesh, groups)
     fe = hex_structural_fea.HexStructuralFEA(mesh=mesh, mat_prop=mat, bc=bc, solver=linear_solvers.Solvers.DPCG,
-                                             dsolver=ds, rtol=1e-8, precision=a.precision, warm_start=a.warm_start)
+                                             dsolver=ds, rtol=1e-8, precision=precision, warm_start=warm_start)
     params = tc.TOParams(Constraints=[(tc.TO_QOI.VOLUME_FRACTION, None, 0.3)], RelativeFilterRadius=1.5)
     run = lambda n: topopt_ocm.topopt_optimality_criteria(tc.FEA_MODE.STRUCTURAL, fe, params, maxIterations=n,
                                                           plot_progress=False, print_progress=False,
@@ -162,29 +167,34 @@ def oc_bench(a):
     iters.clear()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    sol, hist, ok, msg, nfea = run(a.iters)
+    sol, hist, ok, msg, nfea = run(n_iters)
     torch.cuda.synchronize()
     t = time.perf_counter() - t0
     obj = [float(v) for v in hist["objective"]]
-    print(json.dumps({"kernel": "oc", "precision": a.precision, "warm_start": a.warm_start, "nel": nel,
-                      "iterations": a.iters, "fea_solves": int(nfea), "krylov_iterations": sum(iters), "s": t,
-                      "ms_per_iteration": 1e3 * t / max(1, nfea), "objective_first": obj[0],
-                      "objective_last": obj[-1], "volfrac_last": float(hist["volfrac"][-1])}))
+    return {"kernel": "oc", "precision": precision, "warm_start": warm_start, "nel": list(nel),
+            "iterations": n_iters, "fea_solves": int(nfea), "krylov_iterations": sum(iters), "s": t,
+            "ms_per_iteration": 1e3 * t / max(1, nfea), "objective_first": obj[0],
+            "objective_last": obj[-1], "volfrac_last": float(hist["volfrac"][-1])}
 
 
 def batch_bench(a):
+    print(json.dumps(run_batch(a.designs, a.reps, tune=not a.no_tune)))
+
+
+def run_batch(designs=64, reps=3, tune=True):
     """Batched workload: designs of uneven size plus one multi-load-case design, solved
-    to rel-residual 1e-8 by one CUDA-graph launch, against a loop of single solves."""
+    to rel-residual 1e-8 by one CUDA-graph launch (device time per launch, CUDA events),
+    against a loop of single host-polled solves of the same problems."""
     from .autotune import autotune
     from .batch import batch_problems
     from .engine import BatchSolver
     t0 = time.perf_counter()
-    probs = batch_problems(n_designs=a.designs)
-    tune = {}
-    if not a.no_tune:
+    probs = batch_problems(n_designs=designs)
+    tuned = {}
+    if tune:
         for g, _, _, _ in probs:
-            if g.nel not in tune:
-                tune[g.nel] = autotune(g, reps=5)
+            if g.nel not in tuned:
+                tuned[g.nel] = autotune(g, reps=5)
     t_build = time.perf_counter() - t0
     bs = BatchSolver(probs, rtol=1e-8, max_iters=5000)
     bs.launch()
@@ -192,11 +202,11 @@ def batch_bench(a):
     st = torch.cuda.current_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(st)
-    for _ in range(a.reps):
+    for _ in range(reps):
         bs.launch()
     e1.record(st)
     e1.synchronize()
-    t_graph = e0.elapsed_time(e1) / 1e3 / a.reps
+    t_graph = e0.elapsed_time(e1) / 1e3 / reps
     infos = bs.status()
     # the same problems one at a time through the plain (host-polled) solver
     for g, defl, s, b in probs[:2]:
@@ -211,16 +221,16 @@ def batch_bench(a):
     e1.synchronize()
     t_loop = e0.elapsed_time(e1) / 1e3
     n = len(probs)
-    print(json.dumps({"kernel": "batch", "problems": n, "designs": a.designs,
-                      "dofs": int(sum(g.ndof for g, _, _, _ in probs)),
-                      "graph_s": t_graph, "graph_solves_per_s": n / t_graph,
-                      "loop_s": t_loop, "loop_solves_per_s": n / t_loop, "speedup": t_loop / t_graph,
-                      "all_converged": all(i.converged for i in infos),
-                      "max_true_rel_res": max(i.true_rel_res for i in infos),
-                      "graph_iters": int(sum(i.iters for i in infos)), "loop_iters": int(loop_iters),
-                      "build_s": t_build,
-                      "tuned": {f"{k[0]}x{k[1]}x{k[2]}": {p: v[0] for p, v in r.items()} for k, r in tune.items()}}))
     bs.close()
+    return {"kernel": "batch", "problems": n, "designs": designs,
+            "dofs": int(sum(g.ndof for g, _, _, _ in probs)),
+            "graph_s": t_graph, "graph_solves_per_s": n / t_graph,
+            "loop_s": t_loop, "loop_solves_per_s": n / t_loop, "speedup": t_loop / t_graph,
+            "all_converged": all(i.converged for i in infos),
+            "max_true_rel_res": max(i.true_rel_res for i in infos),
+            "graph_iters": int(sum(i.iters for i in infos)), "loop_iters": int(loop_iters),
+            "build_s": t_build,
+            "tuned": {f"{k[0]}x{k[1]}x{k[2]}": {p: v[0] for p, v in r.items()} for k, r in tuned.items()}}
 
 
 if __name__ == "__main__":

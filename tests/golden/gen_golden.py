@@ -62,8 +62,12 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--slow", action="store_true")
+    ap.add_argument("--cfg13", action="store_true",
+                    help="only the 60x30x30 tight-tolerance goldens (rho = 0.3 and the OC iterate-5 design)")
     args = ap.parse_args()
     install_shim(args.ref)
+    if args.cfg13:
+        return cfg13()
     import bound_cond
     import deflation
     import hex_element_stiffness as hes
@@ -260,6 +264,64 @@ def main():
         h, v, c, _ = run_oc((60, 30, 30), linear_solvers.Solvers.PCG, 10)
         np.savez_compressed(os.path.join(HERE, "cfg1_oc10.npz"), objective=h, volfrac=v, change=c)
     print("golden vectors written to", HERE)
+
+
+def cfg13():
+    """60x30x30 cantilever goldens at rtol 1e-12 (compliance parity to 1e-10):
+    rho = 0.3 uniform, and the design after 5 OC updates of the reference's own OC
+    loop (PCG at rtol 1e-8, sensitivity filter r = 1.5, volfrac 0.3, move 0.2).
+    The reference's PCG path (scipy cg, src/linear_solvers.py:164-168) solves both."""
+    import bound_cond
+    import hex_mesher
+    import hex_structural_fea
+    import linear_solvers
+    import mat_lib
+    import topopt_common
+    import topopt_material_model as tmm
+    import topopt_obj_cons_sensitivities as toc
+    import topopt_ocm
+
+    tmm._EVOID_RELATIVE = 1e-9
+    nel = (60, 30, 30)
+
+    def fea(rtol):
+        m = hex_mesher.HexMesher()
+        m.grid_mesh(nel, (1.0, 1.0, 1.0))
+        m.createEdofMatStructural()
+        m.find_connected_components = lambda *a, **k: [np.arange(m.num_elems)]
+        f, fixed = cantilever(m)
+        bc = bound_cond.BC(force=f, fixed_dofs=fixed, dirichlet_values=np.zeros(len(fixed)))
+        mat = mat_lib.create_material_with_defaults("unit", youngs_modulus=1.0, poissons_ratio=0.3)
+        fe = hex_structural_fea.HexStructuralFEA(mesh=m, mat_prop=mat, bc=bc, solver=linear_solvers.Solvers.PCG,
+                                                 rtol=rtol)
+        fe.plot_pseudo_density_realtime = lambda *a, **k: None
+        return m, fe
+
+    def tight(rho, name):
+        m, fe = fea(1e-12)
+        u = fe.solve(rho, tmm.MaterialModel.SIMP)
+        C, _ = toc.compute_compliance_and_gradient(topopt_common.FEA_MODE.STRUCTURAL, u, rho, fe, fe.elem_stiff[0],
+                                                   tmm.MaterialModel.SIMP)
+        sample = np.arange(0, m.num_nodes * 3, 997)
+        np.savez_compressed(os.path.join(HERE, name), rho=rho, C=C, max_def=fe.max_deformation,
+                            u_absmax=np.abs(u).max(), sample_idx=sample, u_sample=u[sample])
+        print(name, "C =", repr(C))
+
+    tight(0.3 * np.ones(int(np.prod(nel))), "cfg1_pcg_tight.npz")
+    m, fe = fea(1e-8)
+    params = topopt_common.TOParams(Constraints=[(topopt_common.TO_QOI.VOLUME_FRACTION, None, 0.3)],
+                                    RelativeFilterRadius=1.5)
+    xs = []
+    orig = fe.solve
+
+    def solve_rec(x, mm=tmm.MaterialModel.SIMP):
+        xs.append(np.array(x, copy=True))
+        return orig(x, mm)
+    fe.solve = solve_rec
+    topopt_ocm.topopt_optimality_criteria(topopt_common.FEA_MODE.STRUCTURAL, fe, params, maxIterations=5,
+                                          plot_progress=False, print_progress=False, binarize_topology=False)
+    # xs[k] is the design of the k-th solve; xs[5] is the design after 5 OC updates
+    tight(xs[5], "cfg3_oc5_pcg_tight.npz")
 
 
 if __name__ == "__main__":

@@ -130,7 +130,7 @@ def test_gradients_match_central_differences(nel, groups, nsample, solver, rtol)
     gC, = torch.autograd.grad(C, xg, retain_graph=True)
     gP, = torch.autograd.grad(pn, xg)
     act = np.flatnonzero(prob.grid.active.cpu().numpy())
-    idx = np.random.default_rng(123).choice(act, nsample, replace=False)
+    idx = np.random.default_rng(1).choice(act, nsample, replace=False)  # the FD sample: seed 1
     h = 1e-6
     for i in idx:
         dC, dP = _exact_differences(prob, x, int(i), h)

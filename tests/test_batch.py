@@ -63,3 +63,22 @@ def test_autotune_picks_a_variant_and_keeps_results():
     assert (g.op.tune & 0xFF) - 1 == res["f64"][0] and ((g.op.tune >> 8) & 0xFF) - 1 == res["f32"][0]
     y1 = g.matvec(s, u)
     assert (y1 - y0).abs().max().item() <= 1e-13 * y0.abs().max().item()
+
+
+def test_batch_refuses_launch_after_fixed_dofs_change():
+    """The graph holds the addresses of the deflation boundary lists: resetting a
+    grid's fixed DOFs (which rebuilds them at the next sync) must stop the launch."""
+    from pyto_b200.batch import batch_problems
+    from pyto_b200.engine import BatchSolver
+    probs = batch_problems(n_designs=2, min_nx=16, max_nx=16, multi_nel=None, n_loads=0, seed=5)
+    bs = BatchSolver(probs, rtol=1e-8)
+    bs.launch()
+    assert all(i.converged for i in bs.status())
+    g, defl, s, b = probs[0]
+    nx, ny, nz = g.nel
+    n = np.arange(g.nnodes)
+    fixed = np.concatenate([3 * n[n % (nx + 1) == 0] + c for c in range(3)])
+    g.set_fixed_dofs(np.sort(fixed))  # same set, new mask version
+    with pytest.raises(RuntimeError, match="create a new BatchSolver"):
+        bs.launch()
+    bs.close()
