@@ -18,16 +18,17 @@ import numpy as np
 import torch
 
 from . import _capi as A
+from ._enum import NamedEnum
 
 DEFAULT_TOL = 1.0e-6
 
 
-class Preconditioners(enum.Enum):
+class Preconditioners(NamedEnum):
     JACOBI = enum.auto()
     ILU = enum.auto()
 
 
-class Solvers(enum.Enum):
+class Solvers(NamedEnum):
     SPSOLVE = enum.auto()
     PCG = enum.auto()
     PYAMG = enum.auto()
@@ -43,6 +44,9 @@ class SolverError(RuntimeError):
 
 class StiffnessOperator:
     """K(s) = sum_e s_e Ke on a HexGrid, applied matrix-free on the GPU."""
+
+    #: marks this library's operator for a PyTO linear_solvers.solve that dispatches here
+    is_pyto_operator = True
 
     def __init__(self, grid, s):
         self.grid = grid

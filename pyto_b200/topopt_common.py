@@ -8,25 +8,26 @@ from typing import Tuple
 
 import numpy as np
 
+from ._enum import NamedEnum
 from .topopt_material_model import MaterialModel
 
 DIRECT_SOLVER_DOF_CUTOFF = 100000
 
 
-class TO_METHODS(enum.Enum):
+class TO_METHODS(NamedEnum):
     DENSITYMMA = enum.auto()
     DENSITYOCM = enum.auto()
     PARETO = enum.auto()
     LEVELSET = enum.auto()
 
 
-class FEA_MODE(enum.Enum):
+class FEA_MODE(NamedEnum):
     STRUCTURAL = enum.auto()
     THERMAL = enum.auto()
     THERMO_STRUCTURAL = enum.auto()
 
 
-class TO_QOI(enum.Enum):
+class TO_QOI(NamedEnum):
     VOLUME_FRACTION = enum.auto()
     VOLUME = enum.auto()
     MASS = enum.auto()

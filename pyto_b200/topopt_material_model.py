@@ -13,6 +13,8 @@ import enum
 
 import numpy as np
 
+from ._enum import NamedEnum
+
 _SIMP_STRUCTURAL_PENALTY_MIN = 1
 _SIMP_STRUCTURAL_PENALTY_MAX = 6.0
 _SIMP_THERMAL_PENALTY_MIN = 1
@@ -28,7 +30,7 @@ _MASS_LOW = 0
 _PNORM_EXPONENT = 6
 
 
-class MaterialModel(enum.Enum):
+class MaterialModel(NamedEnum):
     SIMP = enum.auto()
     RAMP = enum.auto()
     SIMPPLUS = enum.auto()

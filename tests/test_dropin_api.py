@@ -180,3 +180,38 @@ def test_nonzero_dirichlet_values():
     K = O.assemble_K(mo, O.simp_scaling(rho, 3.0, tmm._EVOID_RELATIVE), O.ke_hex8(1.0, 0.3))
     uref, _ = O.solve_fixed(K, f, fixed, g=gval)
     np.testing.assert_allclose(u, uref, rtol=0, atol=1e-9 * np.abs(uref).max())
+
+
+def test_caller_enums_from_another_module():
+    """A PyTO caller passes its own enum members (PyTO's Solvers, MaterialModel,
+    FEA_MODE classes, not this package's): the same-named members select the same
+    solver, material model and FEA mode."""
+    import enum
+
+    from pyto_b200 import hex_structural_fea, linear_solvers, topopt_obj_cons_sensitivities as toc
+
+    class Solvers(enum.Enum):  # stand-ins with PyTO's class and member names
+        SPSOLVE = enum.auto()
+        PCG = enum.auto()
+        PYAMG = enum.auto()
+        DPCG = enum.auto()
+
+    class MaterialModel(enum.Enum):
+        SIMP = enum.auto()
+        RAMP = enum.auto()
+
+    class FEA_MODE(enum.Enum):
+        STRUCTURAL = enum.auto()
+        THERMAL = enum.auto()
+
+    d = golden("cantilever_12x6x6_direct.npz")
+    m, fe = _setup()
+    fe.solver = Solvers.PCG
+    u = fe.solve(d["rho"], MaterialModel.SIMP)
+    np.testing.assert_allclose(u, d["u"], rtol=0, atol=1e-9 * np.abs(d["u"]).max())
+    C, dC = toc.compute_compliance_and_gradient(FEA_MODE.STRUCTURAL, u, d["rho"], fe, fe.elem_stiff[0],
+                                                MaterialModel.SIMP)
+    assert abs(C - float(d["C"])) <= 1e-10 * float(d["C"])
+    v = linear_solvers.solve(fe.stiff_mtrx, d["f"], Solvers.SPSOLVE, fe.bc, rtol=1e-12)
+    np.testing.assert_allclose(v, d["u"], rtol=0, atol=1e-9 * np.abs(d["u"]).max())
+    assert isinstance(fe, hex_structural_fea.HexStructuralFEA)
