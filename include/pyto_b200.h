@@ -256,6 +256,39 @@ int pyto_dpcg_mixed_solve(const pyto_operator_t* op, const double* s, const uint
                           const pyto_solve_cfg_t* cfg, double delta, pyto_solve_status_t* status,
                           void* ws, size_t ws_bytes, void* stream);
 
+/* ---- building blocks of a deflated PCG split across ranks --------------------------- */
+/* No reference counterpart: PyTO solves on one host.  These are the pieces of
+ * DeflationSolver.deflatedPCG (src/deflation.py:504-584) for a grid cut into slabs of node
+ * planes, one slab per rank; the host composes them between its collectives (halo
+ * exchange of the slab's boundary planes before each operator application, sums over
+ * ranks of the dot products, of the restricted coarse vectors and of the coarse matrix).
+ * A rank marks its halo nodes as fixed (all 3 bits) in `mask`, so outputs, dots and
+ * restrictions cover its own nodes only.  All vectors are FP64 on the slab's grid. */
+/* defl->coarse_inv = W_f^T K(s) W_f (dense nc x nc, no shift, not inverted: the sum over
+ * ranks of each rank's elements gives the global matrix).  PYTO_WS_DPCG workspace. */
+int pyto_coarse_assemble(const pyto_operator_t* op, const double* s, const uint8_t* mask,
+                         pyto_deflation_t* defl, void* ws, size_t ws_bytes, void* stream);
+/* defl->coarse_inv: E on entry, (sym(E) + shift I)^-1 on exit (vanishing rows -> identity,
+ * shift as in pyto_dpcg_setup).  PYTO_WS_DPCG workspace. */
+int pyto_coarse_invert(const pyto_operator_t* op, pyto_deflation_t* defl, void* ws, size_t ws_bytes,
+                       void* stream);
+/* v[nc] = W_f^T y over the nodes whose DOFs `mask` leaves free (deterministic order).
+ * PYTO_WS_DPCG workspace. */
+int pyto_coarse_restrict(const pyto_operator_t* op, const pyto_deflation_t* defl, const uint8_t* mask,
+                         const double* y, double* v, void* ws, size_t ws_bytes, void* stream);
+/* mu = defl->coarse_inv v (dense FP64 GEMV). */
+int pyto_coarse_apply(const pyto_deflation_t* defl, const double* v, double* mu, void* stream);
+/* p = a z + b p - W mu on free DOFs, 0 on fixed ones (z may be NULL: a z = 0). */
+int pyto_coarse_prolong(const pyto_operator_t* op, const pyto_deflation_t* defl, const uint8_t* mask,
+                        const double* mu, double a, const double* z, double b, double* p, void* stream);
+/* x += alpha p (when p and x are given), r -= alpha q (when q is given), z = M r (Jacobi
+ * data of pyto_jacobi: winv, flags), and dots[0] = r.r, dots[1] = r.z over the free DOFs
+ * (device, deterministic).  p and x are both given or both NULL.  PYTO_WS_REDUCE
+ * workspace. */
+int pyto_cg_update(const pyto_operator_t* op, const double* winv, const uint8_t* flags, double alpha,
+                   const double* p, const double* q, double* x, double* r, double* z, double* dots, void* ws,
+                   size_t ws_bytes, void* stream);
+
 /* ---- batched solves in one CUDA graph ---------------------------------------------- */
 /* One independent deflated PCG problem of a batch (no reference counterpart: PyTO
  * solves one problem per call).  op and defl are read when the batch is created; the

@@ -93,6 +93,12 @@ SIGNATURES = {
                                   C.POINTER(SolveStatus), _P, C.c_size_t, _P]),
     "pyto_dpcg_mixed_solve": (C.c_int, [_OP, _P, _P, C.POINTER(Deflation), _P, _P, C.POINTER(SolveCfg), C.c_double,
                                         C.POINTER(SolveStatus), _P, C.c_size_t, _P]),
+    "pyto_coarse_assemble": (C.c_int, [_OP, _P, _P, C.POINTER(Deflation), _P, C.c_size_t, _P]),
+    "pyto_coarse_invert": (C.c_int, [_OP, C.POINTER(Deflation), _P, C.c_size_t, _P]),
+    "pyto_coarse_restrict": (C.c_int, [_OP, C.POINTER(Deflation), _P, _P, _P, _P, C.c_size_t, _P]),
+    "pyto_coarse_apply": (C.c_int, [C.POINTER(Deflation), _P, _P, _P]),
+    "pyto_coarse_prolong": (C.c_int, [_OP, C.POINTER(Deflation), _P, _P, C.c_double, _P, C.c_double, _P, _P]),
+    "pyto_cg_update": (C.c_int, [_OP, _P, _P, C.c_double, _P, _P, _P, _P, _P, _P, _P, C.c_size_t, _P]),
     "pyto_batch_create": (C.c_int, [C.POINTER(BatchItem), C.c_int, C.POINTER(SolveCfg), C.POINTER(C.c_void_p), _P]),
     "pyto_batch_launch": (C.c_int, [_P, _P]),
     "pyto_batch_status": (C.c_int, [_P, C.POINTER(SolveStatus), _P]),

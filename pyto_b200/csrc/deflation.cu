@@ -1570,10 +1570,11 @@ static int gemv_smem_ok(long long nc) {
 
 using namespace pyto;
 
-// Coarse operator set-up launches (no host synchronisation: safe under stream
-// capture).  With nchunks > 0 the boundary-list chunk tables must be built.
-static int dpcg_setup_launch(const pyto_operator_t* op, const double* s, const uint8_t* mask,
-                             const pyto_deflation_t* defl, const DpcgWs& W, int nchunks, cudaStream_t st) {
+// Coarse operator assembly E = W_f^T K(s) W_f into defl->coarse_inv (no host
+// synchronisation: safe under stream capture).  With nchunks > 0 the boundary-list
+// chunk tables must be built.
+static int coarse_assemble_launch(const pyto_operator_t* op, const double* s, const uint8_t* mask,
+                                  const pyto_deflation_t* defl, const DpcgWs& W, int nchunks, cudaStream_t st) {
   const DeflP dp = make_deflp(op, defl);
   const GridDims g = make_dims(op);
   double* E = defl->coarse_inv;
@@ -1607,6 +1608,15 @@ static int dpcg_setup_launch(const pyto_operator_t* op, const double* s, const u
                                                          defl->nbr_list, E);
     PYTO_COUNT(1);
   }
+  PYTO_LAUNCH_CHECK();
+  return PYTO_OK;
+}
+
+// E (in defl->coarse_inv) -> (sym(E) + shift I)^-1 in place: symmetrise, identity for
+// vanishing rows, diagonal shift, blocked sweep inversion.
+static int coarse_invert_launch(const pyto_deflation_t* defl, const DpcgWs& W, cudaStream_t st) {
+  double* E = defl->coarse_inv;
+  const long long n = (long long)defl->ngroups * defl->modes;
   if (defl->shift_relative) {
     k_diag_mean<<<1, 256, 0, st>>>(n, E, W.part);
     PYTO_COUNT(1);
@@ -1636,6 +1646,12 @@ static int dpcg_setup_launch(const pyto_operator_t* op, const double* s, const u
   PYTO_COUNT(1);
   PYTO_LAUNCH_CHECK();
   return PYTO_OK;
+}
+
+static int dpcg_setup_launch(const pyto_operator_t* op, const double* s, const uint8_t* mask,
+                             const pyto_deflation_t* defl, const DpcgWs& W, int nchunks, cudaStream_t st) {
+  const int rc = coarse_assemble_launch(op, s, mask, defl, W, nchunks, st);
+  return rc ? rc : coarse_invert_launch(defl, W, st);
 }
 
 extern "C" int pyto_dpcg_setup(const pyto_operator_t* op, const double* s, const uint8_t* mask,
@@ -2394,5 +2410,186 @@ extern "C" int pyto_batch_destroy(pyto_batch_t b) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
   delete b;
+  return PYTO_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Building blocks of a deflated PCG whose vectors are split across ranks (slabs
+// of node planes).  The host composes them between its collectives: halo
+// exchange before each operator application, a sum over ranks of the dot
+// products, of the restricted coarse vectors and of the coarse matrix.  A rank
+// marks its halo nodes as fixed in the mask it passes here, so outputs, dot
+// products and restrictions cover its own nodes only.
+// ---------------------------------------------------------------------------
+namespace pyto {
+
+// v[g*modes + a] = sum over chunks c of part[(g*nch + c)*6 + a], chunks in order
+__global__ void k_restrict_sum(long long nc, int modes, int nch, const double* __restrict__ part,
+                               double* __restrict__ v) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nc;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long gg = i / modes, a = i - gg * modes;
+    double t = 0.0;
+    for (int c = 0; c < nch; ++c) t += part[(gg * nch + c) * 6 + a];
+    v[i] = t;
+  }
+}
+
+// p = a z + b p - W mu on free DOFs, 0 on fixed ones (z may be null: a z = 0)
+__global__ void __launch_bounds__(256) k_prolong_axpby(GridDims g, DeflP dp, const int32_t* __restrict__ ngrp,
+                                                       const double* __restrict__ gc, const double* __restrict__ mu,
+                                                       const uint8_t* __restrict__ fl, double a,
+                                                       const double* __restrict__ z, double b,
+                                                       double* __restrict__ p) {
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < g.nnodes;
+       n += (long long)gridDim.x * blockDim.x) {
+    double w[3];
+    prolong_node(g, dp, n, ngrp, gc, mu, w);
+    const int f = fl[n];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const long long i = 3 * n + c;
+      double v = -w[c];
+      if (z) v = fma(a, z[i], v);
+      if (b != 0.0) v = fma(b, p[i], v);
+      p[i] = ((f >> c) & 1) ? 0.0 : v;
+    }
+  }
+}
+
+// x += alpha p (if p, x given); r -= alpha q (if q given); z = M r (Jacobi,
+// src/linear_solvers.py:71-87); the sums r.r and r.z over the free DOFs
+// (deterministic cross-block reduction) -> dots
+__global__ void __launch_bounds__(kNodeThreads) k_cg_update(GridDims g, Prec pc, const double* __restrict__ w,
+                                                            const uint8_t* __restrict__ fl, double alpha,
+                                                            const double* __restrict__ p,
+                                                            const double* __restrict__ q, double* __restrict__ x,
+                                                            double* __restrict__ r, double* __restrict__ z,
+                                                            double* __restrict__ part, unsigned* __restrict__ counter,
+                                                            double* __restrict__ dots) {
+  __shared__ double sred[kNodeThreads / 32];
+  double rr = 0.0, rz = 0.0;
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < g.nnodes;
+       n += (long long)gridDim.x * blockDim.x) {
+    const int f = fl[n];
+    const double wn = w[n];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const long long i = 3 * n + c;
+      double ri = r[i];
+      if (q) {
+        ri = fma(-alpha, q[i], ri);
+        r[i] = ri;
+      }
+      if (p && x) x[i] = fma(alpha, p[i], x[i]);
+      const double zi = jacobi_apply(ri, f, c, wn, pc);
+      z[i] = zi;
+      if (!((f >> c) & 1)) {
+        rr = fma(ri, ri, rr);
+        rz = fma(ri, zi, rz);
+      }
+    }
+  }
+  double v[2] = {block_sum<kNodeThreads>(rr, sred), block_sum<kNodeThreads>(rz, sred)};
+  grid_reduce<2>(v, part, counter, gridDim.x, [&](const double* tot) {
+    dots[0] = tot[0];
+    dots[1] = tot[1];
+  });
+}
+
+}  // namespace pyto
+
+extern "C" int pyto_coarse_assemble(const pyto_operator_t* op, const double* s, const uint8_t* mask,
+                                    pyto_deflation_t* defl, void* ws, size_t ws_bytes, void* stream) {
+  if (!op || !s || !defl_ok(defl)) return PYTO_ERR_ARG;
+  const DeflP dp = make_deflp(op, defl);
+  if (dp.nc > kMaxCoarse) return PYTO_ERR_TOO_LARGE;
+  size_t need = 0;
+  DpcgWs W = carve_dpcg(op, dp.nc, ws, ws_bytes, &need);
+  if (!ws || ws_bytes < need) return PYTO_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int nchunks = chunk_setup(defl, W, st);
+  if (nchunks < 0) return nchunks;
+  return coarse_assemble_launch(op, s, mask, defl, W, nchunks, st);
+}
+
+extern "C" int pyto_coarse_invert(const pyto_operator_t* op, pyto_deflation_t* defl, void* ws, size_t ws_bytes,
+                                  void* stream) {
+  if (!op || !defl_ok(defl)) return PYTO_ERR_ARG;
+  const DeflP dp = make_deflp(op, defl);
+  int rc0 = gemv_smem_ok(dp.nc);
+  if (rc0) return rc0;
+  size_t need = 0;
+  DpcgWs W = carve_dpcg(op, dp.nc, ws, ws_bytes, &need);
+  if (!ws || ws_bytes < need) return PYTO_ERR_WORKSPACE;
+  return coarse_invert_launch(defl, W, (cudaStream_t)stream);
+}
+
+extern "C" int pyto_coarse_restrict(const pyto_operator_t* op, const pyto_deflation_t* defl, const uint8_t* mask,
+                                    const double* y, double* v, void* ws, size_t ws_bytes, void* stream) {
+  if (!op || !mask || !y || !v || !defl_ok(defl)) return PYTO_ERR_ARG;
+  const DeflP dp = make_deflp(op, defl);
+  if (dp.nc > kMaxCoarse) return PYTO_ERR_TOO_LARGE;
+  size_t need = 0;
+  DpcgWs W = carve_dpcg(op, dp.nc, ws, ws_bytes, &need);
+  if (!ws || ws_bytes < need) return PYTO_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  const GridDims g = make_dims(op);
+  const int nch = (defl->max_group_nodes + kRestrictChunk - 1) / kRestrictChunk;
+  k_restrict<double><<<dp.ngroups * nch, 256, 0, st>>>(g, dp, defl->group_ptr, defl->group_nodes,
+                                                       defl->group_center, mask, y, nch, W.rpart);
+  PYTO_COUNT(1);
+  k_restrict_sum<<<(int)std::min<long long>((dp.nc + 255) / 256, 4 * kNumSMs), 256, 0, st>>>(dp.nc, dp.modes, nch,
+                                                                                             W.rpart, v);
+  PYTO_COUNT(1);
+  PYTO_LAUNCH_CHECK();
+  return PYTO_OK;
+}
+
+extern "C" int pyto_coarse_apply(const pyto_deflation_t* defl, const double* v, double* mu, void* stream) {
+  if (!defl_ok(defl) || !v || !mu || v == mu) return PYTO_ERR_ARG;
+  const long long nc = (long long)defl->ngroups * defl->modes;
+  if (nc > kMaxCoarse) return PYTO_ERR_TOO_LARGE;
+  int rc0 = gemv_smem_ok(nc);
+  if (rc0) return rc0;
+  cudaStream_t st = (cudaStream_t)stream;
+  if ((nc & 1) == 0 && ((uintptr_t)v & 15) == 0) {
+    k_gemv_rows<<<(int)((nc + 3) / 4), 128, 0, st>>>(nc, defl->coarse_inv, v, mu, nullptr);
+  } else {
+    const size_t shm = (size_t)nc * sizeof(double);
+    const int nb = (int)std::min<long long>((nc + 7) / 8, 8 * kNumSMs);
+    k_gemv<<<nb, 256, shm, st>>>(nc, defl->coarse_inv, v, mu, nullptr);
+  }
+  PYTO_COUNT(1);
+  PYTO_LAUNCH_CHECK();
+  return PYTO_OK;
+}
+
+extern "C" int pyto_coarse_prolong(const pyto_operator_t* op, const pyto_deflation_t* defl, const uint8_t* mask,
+                                   const double* mu, double a, const double* z, double b, double* p, void* stream) {
+  if (!op || !mask || !mu || !p || !defl_ok(defl)) return PYTO_ERR_ARG;
+  const GridDims g = make_dims(op);
+  const int nb = (int)std::min<long long>((g.nnodes + 255) / 256, 8 * kNumSMs);
+  k_prolong_axpby<<<nb, 256, 0, (cudaStream_t)stream>>>(g, make_deflp(op, defl), defl->node_group,
+                                                        defl->group_center, mu, mask, a, z, b, p);
+  PYTO_COUNT(1);
+  PYTO_LAUNCH_CHECK();
+  return PYTO_OK;
+}
+
+extern "C" int pyto_cg_update(const pyto_operator_t* op, const double* winv, const uint8_t* flags, double alpha,
+                              const double* p, const double* q, double* x, double* r, double* z, double* dots,
+                              void* ws, size_t ws_bytes, void* stream) {
+  if (!op || !winv || !flags || !r || !z || !dots || (!p != !x)) return PYTO_ERR_ARG;
+  Carver cv{(char*)ws, 0, ws_bytes};
+  unsigned* counter = cv.take<unsigned>(64);
+  double* part = cv.take<double>(2 * (size_t)kNodeBlocks);
+  if (!cv.ok()) return PYTO_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  PYTO_CUDA(cudaMemsetAsync(counter, 0, 64 * sizeof(unsigned), st));
+  k_cg_update<<<kNodeBlocks, kNodeThreads, 0, st>>>(make_dims(op), make_prec(op), winv, flags, alpha, p, q, x, r, z,
+                                                    part, counter, dots);
+  PYTO_COUNT(1);
+  PYTO_LAUNCH_CHECK();
   return PYTO_OK;
 }
