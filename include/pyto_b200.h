@@ -126,7 +126,7 @@ typedef struct pyto_deflation {
 int pyto_version(void);
 /* sizeof of this library's ABI structs, for bindings to check their layout:
  * 0 pyto_operator_t, 1 pyto_solve_cfg_t, 2 pyto_solve_status_t, 3 pyto_deflation_t,
- * 4 pyto_batch_item_t; 0 for other values.  No reference counterpart. */
+ * 4 pyto_batch_item_t, 5 pyto_thermal_t; 0 for other values.  No reference counterpart. */
 size_t pyto_struct_size(int which);
 /* Description of the last CUDA call of this thread that failed inside the library
  * (file:line, the call, the CUDA error); "" if none.  No reference counterpart. */
@@ -360,6 +360,45 @@ int pyto_filter(const pyto_operator_t* op, double rel_radius, int mode, const do
 int pyto_oc_update(const pyto_operator_t* op, double* x, const double* dc, const uint8_t* active,
                    long long n_active, double volfrac, double move, double xmin, double xmax,
                    double* change_out, void* ws, size_t ws_bytes, void* stream);
+
+/* ---- thermal hex8 (one temperature DOF per node) ----------------------------------- */
+/* Grid + the 8x8 conduction matrix of a box element.  For a box element Ke[a][b] depends
+ * only on which coordinates of corners a and b differ: kxor[d] with d = bits(a) ^ bits(b),
+ * bits = the corner's (x, y, z) offsets as bits 0, 1, 2. */
+typedef struct pyto_thermal {
+  int32_t nelx, nely, nelz, pad;
+  double hx, hy, hz;
+  double k;          /* conductivity of Ke */
+  double ke[64];     /* 8x8 Ke, row-major, reference corner order */
+  double kxor[8];    /* Ke as a function of the differing offset bits */
+} pyto_thermal_t;
+/* 8x8 conduction Ke of a box hex8, 2x2x2 Gauss.  Replaces
+ * hex_element_stiffness.hex8_stiffness_matrix_thermal (src/hex_element_stiffness.py:340-385). */
+int pyto_ke_hex8_thermal(double k, double hx, double hy, double hz, double* ke_out);
+/* Fill *t (ke may be NULL: Ke = pyto_ke_hex8_thermal(k, h)); a given Ke without the box
+ * symmetry is refused (PYTO_ERR_ARG).  Replaces the set-up of HexThermalFEA.__init__
+ * (src/hex_thermal_fea.py:19-52). */
+int pyto_thermal_init(pyto_thermal_t* t, int32_t nelx, int32_t nely, int32_t nelz, double hx, double hy,
+                      double hz, double k, const double* ke);
+/* mask[n] = 1 for the fixed-temperature nodes (nnodes bytes, cleared first). */
+int pyto_thermal_mask(const pyto_thermal_t* t, const int64_t* fixed_nodes, int64_t n_fixed, uint8_t* mask,
+                      void* stream);
+/* Bytes of workspace of pyto_thermal_pcg_solve (also enough for the dot / total
+ * reductions of pyto_thermal_matvec and pyto_thermal_energy). */
+size_t pyto_thermal_workspace_bytes(const pyto_thermal_t* t);
+/* T-field operator y = K(s) u with masking per mode (as pyto_matvec); optional *dot =
+ * u_masked . y.  Replaces the COO assembly of HexThermalFEA.solve (src/hex_thermal_fea.py:69-117). */
+int pyto_thermal_matvec(const pyto_thermal_t* t, const double* s, const uint8_t* mask, const double* u, double* y,
+                        int mode, double* dot, void* ws, size_t ws_bytes, void* stream);
+/* Jacobi PCG on the reduced thermal system (scipy cg semantics, src/linear_solvers.py:164-168);
+ * stop rules 0 and 1 as pyto_pcg_solve. */
+int pyto_thermal_pcg_solve(const pyto_thermal_t* t, const double* s, const uint8_t* mask, const double* b,
+                           double* u, const pyto_solve_cfg_t* cfg, pyto_solve_status_t* status, void* ws,
+                           size_t ws_bytes, void* stream);
+/* ce[e] = u_e^T Ke v_e (v NULL: v = u); with total: *total = sum s_e ce_e (device).  Replaces
+ * the thermal branch of compute_compliance_and_gradient (src/topopt_obj_cons_sensitivities.py:148-179). */
+int pyto_thermal_energy(const pyto_thermal_t* t, const double* u, const double* v, const double* s, double* ce,
+                        double* total, void* ws, size_t ws_bytes, void* stream);
 
 #ifdef __cplusplus
 }

@@ -27,6 +27,7 @@ __all__ = [
     "solution_dotproduct_and_gradient", "smoothing_filter",
     "volume_constraint", "oc_update", "elements_with_forces", "topopt_oc",
     "cantilever_bc", "matvec_free", "matvec_ebe",
+    "ke_hex8_thermal", "assemble_K_thermal", "thermal_scaling", "thermal_sensitivity",
 ]
 
 
@@ -139,6 +140,51 @@ def ke_hex8(E: float, nu: float, elem_size=(1.0, 1.0, 1.0)) -> np.ndarray:
             b[5, 3 * l + 2] = grad[l, 0]
         ke += b.T @ c @ b * np.linalg.det(jac) * wts[gp]
     return ke
+
+
+def ke_hex8_thermal(k: float, elem_size=(1.0, 1.0, 1.0)) -> np.ndarray:
+    """8x8 conduction Ke of a box hex8, 2x2x2 Gauss (src/hex_element_stiffness.py:340-385):
+    Ke = sum_g k B^T B det(J) w with B the 3x8 physical shape-function gradients."""
+    dx, dy, dz = elem_size
+    nodes = np.array([[0, dx, dx, 0, 0, dx, dx, 0],
+                      [0, 0, dy, dy, 0, 0, dy, dy],
+                      [0, 0, 0, 0, dz, dz, dz, dz]], dtype=float).T
+    g = np.array([-0.5773502691896257, 0.5773502691896257])
+    xis = np.array([-1, 1, 1, -1, -1, 1, 1, -1.0])
+    etas = np.array([-1, -1, 1, 1, -1, -1, 1, 1.0])
+    zetas = np.array([-1, -1, -1, -1, 1, 1, 1, 1.0])
+    ke = np.zeros((8, 8))
+    for xi in g:
+        for eta in g:
+            for zeta in g:
+                dN = np.stack([0.125 * xis * (1 + eta * etas) * (1 + zeta * zetas),
+                               0.125 * (1 + xi * xis) * etas * (1 + zeta * zetas),
+                               0.125 * (1 + xi * xis) * (1 + eta * etas) * zetas], axis=1)
+                jac = dN.T @ nodes
+                b = np.linalg.solve(jac, dN.T)  # (3, 8) physical gradients
+                ke += k * b.T @ b * np.linalg.det(jac)
+    return ke
+
+
+def assemble_K_thermal(mesh: dict, s: np.ndarray, Ke8: np.ndarray) -> sp.csr_matrix:
+    """COO assembly of sum_e s_e Ke on the node DOFs (edofMatThermal = elemArray;
+    src/hex_thermal_fea.py:44-48, :98-112)."""
+    ea = mesh["elemArray"].astype(np.int64)
+    I = np.repeat(ea, 8, axis=1).ravel()
+    J = np.tile(ea, (1, 8)).ravel()
+    V = np.einsum("ij,e->eij", Ke8, s).ravel()
+    n = mesh["num_nodes"]
+    return sp.coo_matrix((V, (I, J)), shape=(n, n)).tocsr()
+
+
+def thermal_scaling(x, penal=1.0, kvoid=1e-8):
+    """SIMP conductivity ``Kvoid + x^p (1-Kvoid)`` (src/topopt_material_model.py:109-110)."""
+    return kvoid + (x ** penal) * (1.0 - kvoid)
+
+
+def thermal_sensitivity(x, penal=1.0, kvoid=1e-8):
+    """``p x^(p-1) (1-Kvoid)`` (src/topopt_material_model.py:151-152)."""
+    return penal * (x ** (penal - 1.0)) * (1.0 - kvoid)
 
 
 # --------------------------------------------------------------------------

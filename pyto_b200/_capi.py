@@ -67,8 +67,15 @@ class BatchItem(C.Structure):
                 ("ws_bytes", C.c_size_t)]
 
 
+class Thermal(C.Structure):
+    _fields_ = [("nelx", C.c_int32), ("nely", C.c_int32), ("nelz", C.c_int32), ("pad", C.c_int32),
+                ("hx", C.c_double), ("hy", C.c_double), ("hz", C.c_double), ("k", C.c_double),
+                ("ke", C.c_double * 64), ("kxor", C.c_double * 8)]
+
+
 _P = C.c_void_p
 _OP = C.POINTER(Operator)
+_TH = C.POINTER(Thermal)
 SIGNATURES = {
     "pyto_version": (C.c_int, []),
     "pyto_struct_size": (C.c_size_t, [C.c_int]),
@@ -99,6 +106,15 @@ SIGNATURES = {
     "pyto_coarse_apply": (C.c_int, [C.POINTER(Deflation), _P, _P, _P]),
     "pyto_coarse_prolong": (C.c_int, [_OP, C.POINTER(Deflation), _P, _P, C.c_double, _P, C.c_double, _P, _P]),
     "pyto_cg_update": (C.c_int, [_OP, _P, _P, C.c_double, _P, _P, _P, _P, _P, _P, _P, C.c_size_t, _P]),
+    "pyto_ke_hex8_thermal": (C.c_int, [C.c_double] * 4 + [_P]),
+    "pyto_thermal_init": (C.c_int, [_TH, C.c_int32, C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
+                                    C.c_double, _P]),
+    "pyto_thermal_mask": (C.c_int, [_TH, _P, C.c_int64, _P, _P]),
+    "pyto_thermal_workspace_bytes": (C.c_size_t, [_TH]),
+    "pyto_thermal_matvec": (C.c_int, [_TH, _P, _P, _P, _P, C.c_int, _P, _P, C.c_size_t, _P]),
+    "pyto_thermal_pcg_solve": (C.c_int, [_TH, _P, _P, _P, _P, C.POINTER(SolveCfg), C.POINTER(SolveStatus), _P,
+                                         C.c_size_t, _P]),
+    "pyto_thermal_energy": (C.c_int, [_TH, _P, _P, _P, _P, _P, _P, C.c_size_t, _P]),
     "pyto_batch_create": (C.c_int, [C.POINTER(BatchItem), C.c_int, C.POINTER(SolveCfg), C.POINTER(C.c_void_p), _P]),
     "pyto_batch_launch": (C.c_int, [_P, _P]),
     "pyto_batch_status": (C.c_int, [_P, C.POINTER(SolveStatus), _P]),
@@ -188,6 +204,17 @@ def make_operator(nelx, nely, nelz, h=(1.0, 1.0, 1.0), E=1.0, nu=0.3, ke=None) -
     call("pyto_operator_init", C.byref(op), int(nelx), int(nely), int(nelz), float(h[0]), float(h[1]), float(h[2]),
          float(E), float(nu), kep)
     return op
+
+
+def make_thermal(nelx, nely, nelz, h=(1.0, 1.0, 1.0), k=1.0, ke=None) -> Thermal:
+    t = Thermal()
+    kep = None
+    if ke is not None:
+        ke = np.ascontiguousarray(np.asarray(ke, dtype=np.float64).reshape(8, 8))
+        kep = ke.ctypes.data_as(C.c_void_p)
+    call("pyto_thermal_init", C.byref(t), int(nelx), int(nely), int(nelz), float(h[0]), float(h[1]), float(h[2]),
+         float(k), kep)
+    return t
 
 
 def ws_bytes(op: Operator, kind: int) -> int:

@@ -47,6 +47,7 @@ extern "C" size_t pyto_struct_size(int which) {
     case 2: return sizeof(pyto_solve_status_t);
     case 3: return sizeof(pyto_deflation_t);
     case 4: return sizeof(pyto_batch_item_t);
+    case 5: return sizeof(pyto_thermal_t);
     default: return 0;
   }
 }

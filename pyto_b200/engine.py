@@ -248,6 +248,85 @@ class HexGrid:
         return ch
 
 
+class ThermalGrid:
+    """A box grid of hex8 elements with one temperature DOF per node on one CUDA
+    device (the thermal path: pyto_thermal_*)."""
+
+    def __init__(self, nel, elem_size=(1.0, 1.0, 1.0), k=1.0, ke=None, device=None):
+        if not torch.cuda.is_available():
+            raise RuntimeError("pyto_b200 needs a CUDA device (sm_100a); no CPU path exists")
+        self.device = torch.device(device if device is not None else "cuda")
+        self.nel = tuple(int(n) for n in nel)
+        self.h = tuple(float(v) for v in elem_size)
+        self.th = A.make_thermal(*self.nel, self.h, k, ke)
+        nx, ny, nz = self.nel
+        self.nnodes = (nx + 1) * (ny + 1) * (nz + 1)
+        self.nelem = nx * ny * nz
+        self.ndof = self.nnodes
+        self.mask = torch.zeros(self.nnodes, dtype=torch.uint8, device=self.device)
+        self.active = None
+
+    @property
+    def thp(self):
+        return C.byref(self.th)
+
+    def _st(self):
+        return A.stream_ptr(self.device)
+
+    def _ws(self):
+        n = int(A.lib().pyto_thermal_workspace_bytes(self.thp))
+        buf = A.workspace(n, self.device, "thermal")
+        return A.ptr(buf), buf.numel()
+
+    tensor = HexGrid.tensor
+
+    def set_fixed_nodes(self, nodes):
+        nd = self.tensor(np.asarray(nodes, dtype=np.int64).ravel() if not isinstance(nodes, torch.Tensor) else nodes,
+                         dtype=torch.int64)
+        A.call("pyto_thermal_mask", self.thp, A.ptr(nd) if nd.numel() else None, int(nd.numel()), A.ptr(self.mask),
+               self._st())
+        return self
+
+    def simp(self, x, penal=1.0, kvoid=1e-8, want_ds=True):
+        """Thermal SIMP s = kvoid + x^p (1 - kvoid) (the structural kernel's formula)."""
+        x = self.tensor(x)
+        s = torch.empty_like(x)
+        ds = torch.empty_like(x) if want_ds else None
+        A.call("pyto_simp", A.ptr(x), None, int(x.numel()), float(penal), float(kvoid), A.ptr(s), A.ptr(ds),
+               self._st())
+        return s, ds
+
+    def matvec(self, s, u, mode=A.MASK_IN | A.MASK_OUT, out=None, dot=False):
+        y = out if out is not None else torch.empty(self.ndof, dtype=F64, device=self.device)
+        d = torch.empty(1, dtype=F64, device=self.device) if dot else None
+        wsp, wsn = self._ws() if dot else (None, 0)
+        A.call("pyto_thermal_matvec", self.thp, A.ptr(s), A.ptr(self.mask), A.ptr(u), A.ptr(y), int(mode), A.ptr(d),
+               wsp, wsn, self._st())
+        return (y, d) if dot else y
+
+    def pcg(self, s, b, rtol=1e-8, max_iters=100000, stop_rule=0, x0=None, check_every=25, out=None):
+        """Jacobi PCG on the reduced thermal system (fixed nodes of the result are 0)."""
+        u = out if out is not None else torch.empty(self.ndof, dtype=F64, device=self.device)
+        if x0 is not None:
+            u.copy_(x0)
+        cfg = HexGrid._cfg(rtol, max_iters, stop_rule, check_every, x0 is not None)
+        stt = A.SolveStatus()
+        wsp, wsn = self._ws()
+        rc = A.call("pyto_thermal_pcg_solve", self.thp, A.ptr(s), A.ptr(self.mask), A.ptr(b), A.ptr(u),
+                    C.byref(cfg), C.byref(stt), wsp, wsn, self._st(), allow=(A.OK, A.NOT_CONVERGED, A.ERR_BREAKDOWN))
+        return u, SolveInfo(bool(stt.converged), int(stt.iters), bool(stt.breakdown), float(stt.rel_res),
+                            float(stt.true_rel_res), rc)
+
+    def energy(self, u, v=None, s=None):
+        """ce_e = u_e^T Ke v_e; with s also sum_e s_e ce_e (device scalar)."""
+        ce = torch.empty(self.nelem, dtype=F64, device=self.device)
+        tot = torch.empty(1, dtype=F64, device=self.device) if s is not None else None
+        wsp, wsn = self._ws() if s is not None else (None, 0)
+        A.call("pyto_thermal_energy", self.thp, A.ptr(u), A.ptr(v), A.ptr(s), A.ptr(ce), A.ptr(tot), wsp, wsn,
+               self._st())
+        return (ce, tot) if s is not None else ce
+
+
 class DeviceDeflation:
     """Device data of a deflation space (node groups + rigid modes).
 

@@ -70,6 +70,20 @@ class StiffnessOperator:
         raise TypeError("pyto_b200 operators are matrix-free; no assembled matrix exists")
 
 
+class ThermalOperator(StiffnessOperator):
+    """K(s) = sum_e s_e Ke of the thermal path (8x8 Ke, one DOF per node) on a
+    ThermalGrid, applied matrix-free on the GPU."""
+
+    def diagonal(self):
+        """diag K = Ke[a][a] sum_{e ni n} s_e; the node sums come from the operator with
+        Ke replaced by the all-ones matrix / 8, applied to a vector of ones."""
+        from .engine import ThermalGrid
+        g = self.grid
+        ones = ThermalGrid(g.nel, g.h, 1.0, ke=np.full((8, 8), 0.125), device=g.device)
+        sums = ones.matvec(self.s, torch.ones(g.ndof, dtype=torch.float64, device=g.device), mode=0)
+        return float(g.th.kxor[0]) * sums
+
+
 def _prepare_rhs(A0: StiffnessOperator, b0, bc):
     g = A0.grid
     b = g.tensor(b0)
@@ -93,7 +107,13 @@ def solve(A0, b0, solver: Solvers, bc, **kwargs):
     b, lift = _prepare_rhs(A0, b0, bc)
     rtol = kwargs.get("rtol", DEFAULT_TOL)
     strict = kwargs.get("strict", False)
-    if solver == Solvers.PCG:
+    if isinstance(A0, ThermalOperator):
+        # the thermal path has the Jacobi PCG only; the direct solvers run it to 1e-12
+        if solver not in tuple(Solvers):
+            raise ValueError("Unknown solver type")
+        tol = rtol if solver in (Solvers.PCG, Solvers.DPCG, Solvers.PYAMG) else min(rtol, 1e-12)
+        u, info = g.pcg(A0.s, b, rtol=tol, max_iters=kwargs.get("maxiter", 10 * g.ndof), stop_rule=0)
+    elif solver == Solvers.PCG:
         u, info = g.pcg(A0.s, b, rtol=rtol, max_iters=kwargs.get("maxiter", 10 * g.ndof), stop_rule=0)
     elif solver == Solvers.DPCG:
         dsolver = kwargs["dsolver"]

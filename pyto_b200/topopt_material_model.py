@@ -118,6 +118,33 @@ def get_structural_material_model_sensitivity(x, material_model: MaterialModel):
     raise ValueError("Invalid material model specified.")
 
 
+def get_thermal_material_model_scaling(x, material_model: MaterialModel):
+    """Conductivity scaling (src/topopt_material_model.py:98-117); None: x itself."""
+    if material_model is None:
+        return x
+    if material_model == MaterialModel.SIMP:
+        return _KVOID_RELATIVE + (x ** _SIMP_THERMAL_PENALTY) * (1 - _KVOID_RELATIVE)
+    if material_model == MaterialModel.RAMP:
+        return _KVOID_RELATIVE + x * (1 - _KVOID_RELATIVE) / (1 + (1 - x) * _RAMP_PENALTY)
+    if material_model == MaterialModel.SIMPPLUS:
+        return ((_KVOID_RELATIVE + (x ** _SIMP_THERMAL_PENALTY) * (1 - _KVOID_RELATIVE)) + _KVOID_RELATIVE * x) / 2
+    raise ValueError("Invalid material model specified.")
+
+
+def get_thermal_material_model_sensitivity(x, material_model: MaterialModel):
+    """d(conductivity scaling)/dx (src/topopt_material_model.py:142-161)."""
+    if material_model is None:
+        return x * 0 + 1
+    if material_model == MaterialModel.SIMP:
+        return _SIMP_THERMAL_PENALTY * (x ** (_SIMP_THERMAL_PENALTY - 1)) * (1 - _KVOID_RELATIVE)
+    if material_model == MaterialModel.RAMP:
+        return ((1 - _KVOID_RELATIVE) / (1 + (1 - x) * _RAMP_PENALTY) ** 2) * (1 + _RAMP_PENALTY * (1 - x))
+    if material_model == MaterialModel.SIMPPLUS:
+        return (_SIMP_THERMAL_PENALTY * (x ** (_SIMP_THERMAL_PENALTY - 1)) * (1 - _KVOID_RELATIVE)
+                + _KVOID_RELATIVE) / 2
+    raise ValueError("Invalid material model specified.")
+
+
 def get_stress_relaxation_factor() -> float:
     return _SIMP_STRESS_RELAXATION
 

@@ -62,10 +62,30 @@ def compute_compliance(sol, x, fe_solver, KE, material_model):
     return float(C.item())
 
 
+def _thermal_compliance_and_gradient(sol, x, fe_solver, KE, material_model):
+    """Thermal branch: C = sum_e s_e T_e^T Ke T_e, dC = -ds T_e^T Ke T_e with the
+    conductivity scaling (src/topopt_obj_cons_sensitivities.py:162-175)."""
+    g = fe_solver.grid
+    if KE is not None and not np.allclose(np.asarray(KE), fe_solver.elem_stiff[0], rtol=1e-14, atol=0):
+        raise NotImplementedError("the thermal path uses the FEA object's own element matrix")
+    u = fe_solver.sol_dev if (fe_solver.sol_dev is not None and (sol is fe_solver.sol_dev or sol is fe_solver._sol_np)) \
+        else g.tensor(sol)
+    xd = g.tensor(x)
+    if material_model == tmm.MaterialModel.SIMP:
+        s, ds = g.simp(xd, tmm._SIMP_THERMAL_PENALTY, tmm._KVOID_RELATIVE)
+    else:
+        s = tmm.get_thermal_material_model_scaling(xd, material_model).contiguous()
+        ds = tmm.get_thermal_material_model_sensitivity(xd, material_model).contiguous()
+    ce, C = g.energy(u, s=s)
+    return float(C.item()), _out(-ds * ce, x)
+
+
 def compute_compliance_and_gradient(feaMode, sol, x, fe_solver, KE, material_model):
     """(C, dC/dx = -ds u_e^T Ke u_e) (src/topopt_obj_cons_sensitivities.py:148-179)."""
+    if feaMode == FEA_MODE.THERMAL:
+        return _thermal_compliance_and_gradient(sol, x, fe_solver, KE, material_model)
     if feaMode != FEA_MODE.STRUCTURAL:
-        raise NotImplementedError("only the structural mode is on the GPU path")
+        raise NotImplementedError("only the structural and thermal modes are on the GPU path")
     g = _grid(fe_solver, KE)
     s, ds = _scale(g, g.tensor(x), material_model)
     ce, C = g.energy(_u(fe_solver, sol), s=s)

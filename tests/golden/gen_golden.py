@@ -62,12 +62,16 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--slow", action="store_true")
+    ap.add_argument("--thermal", action="store_true", help="only the thermal hex8 goldens")
     ap.add_argument("--cfg13", action="store_true",
                     help="only the 60x30x30 tight-tolerance goldens (rho = 0.3 and the OC iterate-5 design)")
     args = ap.parse_args()
     install_shim(args.ref)
+    ap_thermal = "--thermal" in sys.argv
     if args.cfg13:
         return cfg13()
+    if ap_thermal:
+        return thermal()
     import bound_cond
     import deflation
     import hex_element_stiffness as hes
@@ -264,6 +268,45 @@ def main():
         h, v, c, _ = run_oc((60, 30, 30), linear_solvers.Solvers.PCG, 10)
         np.savez_compressed(os.path.join(HERE, "cfg1_oc10.npz"), objective=h, volfrac=v, change=c)
     print("golden vectors written to", HERE)
+
+
+def thermal():
+    """Thermal hex8 goldens: Ke (src/hex_element_stiffness.py:340-385) for two element
+    sizes, and one HexThermalFEA solve (src/hex_thermal_fea.py:19-117) of a 12x6x6 heat
+    sink: temperature 0 on the x = 0 face, a uniform unit heat load shared by all
+    nodes, SIMP thermal scaling of rho ~ U[0.01, 1] (seed 0), direct solver; the
+    thermal compliance and its gradient (src/topopt_obj_cons_sensitivities.py:148-179)."""
+    import bound_cond
+    import hex_element_stiffness as hes
+    import hex_mesher
+    import hex_thermal_fea
+    import linear_solvers
+    import mat_lib
+    import topopt_common
+    import topopt_material_model as tmm
+    import topopt_obj_cons_sensitivities as toc
+
+    tmm._KVOID_RELATIVE = 1e-3
+    tmm._SIMP_THERMAL_PENALTY = 3
+    out = {f"ke_{tag}": hes.hex8_stiffness_matrix_thermal(k, h)
+           for tag, (k, h) in {"unit": (1.0, (1.0, 1.0, 1.0)), "box": (50.0, (1.0, 0.5, 2.0))}.items()}
+    for tag, nel, h in (("12x6x6", (12, 6, 6), (1.0, 1.0, 1.0)), ("9x5x4_box", (9, 5, 4), (1.0, 0.5, 2.0))):
+        m = hex_mesher.HexMesher()
+        m.grid_mesh(nel, h)
+        m.createEdofMatThermal()
+        fixed = np.sort(m.getNodesOnBoundingBoxPlane(0, True))
+        f = np.full(m.num_nodes, 1.0 / m.num_nodes)
+        bc = bound_cond.BC(force=f, fixed_dofs=fixed, dirichlet_values=np.zeros(len(fixed)))
+        mat = mat_lib.create_material_with_defaults("unit", thermal_conductivity=1.0)
+        fe = hex_thermal_fea.HexThermalFEA(mesh=m, mat_prop=mat, bc=bc, solver=linear_solvers.Solvers.SPSOLVE)
+        rho = np.random.default_rng(0).uniform(0.01, 1.0, m.num_elems)
+        T = fe.solve(rho, tmm.MaterialModel.SIMP)
+        C, dC = toc.compute_compliance_and_gradient(topopt_common.FEA_MODE.THERMAL, T, rho, fe, fe.elem_stiff[0],
+                                                    tmm.MaterialModel.SIMP)
+        out.update({f"{tag}_rho": rho, f"{tag}_f": f, f"{tag}_fixed": fixed, f"{tag}_T": T, f"{tag}_C": C,
+                    f"{tag}_dC": dC, f"{tag}_edof": m.edofMatThermal})
+        print(tag, "C =", repr(C))
+    np.savez_compressed(os.path.join(HERE, "thermal.npz"), kvoid=1e-3, penal=3.0, **out)
 
 
 def cfg13():

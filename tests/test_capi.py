@@ -29,9 +29,9 @@ def test_library_exports_every_declared_symbol():
 def test_ctypes_structs_match_the_c_layout():
     """The ctypes mirrors of the ABI structs have the C compiler's sizes."""
     L = A.lib()
-    for which, cls in enumerate((A.Operator, A.SolveCfg, A.SolveStatus, A.Deflation, A.BatchItem)):
+    for which, cls in enumerate((A.Operator, A.SolveCfg, A.SolveStatus, A.Deflation, A.BatchItem, A.Thermal)):
         assert L.pyto_struct_size(which) == C.sizeof(cls), cls.__name__
-    assert L.pyto_struct_size(5) == 0
+    assert L.pyto_struct_size(6) == 0
 
 
 @pytest.mark.parametrize("tag,E,nu,h", [("unit", 1.0, 0.3, (1, 1, 1)), ("box", 1.0, 0.3, (1.0, 0.5, 2.0)),
@@ -93,3 +93,19 @@ def test_autotuner_variants_are_the_ones_the_library_accepts():
                     assert rc == A.ERR_ARG, (which, v, rc)
     finally:
         assert L.pyto_tune(0, 2) == 0 and L.pyto_tune(1, 16) == 0  # library defaults
+
+
+@pytest.mark.parametrize("tag,k,h", [("unit", 1.0, (1.0, 1.0, 1.0)), ("box", 50.0, (1.0, 0.5, 2.0))])
+def test_thermal_ke_matches_reference(tag, k, h):
+    """pyto_ke_hex8_thermal (host code, no GPU) against the reference's Ke, and the
+    operator set-up's box-symmetry check."""
+    d = golden("thermal.npz")
+    ke = np.zeros(64)
+    assert A.lib().pyto_ke_hex8_thermal(k, *h, ke.ctypes.data_as(C.c_void_p)) == 0
+    np.testing.assert_allclose(ke.reshape(8, 8), d[f"ke_{tag}"], rtol=1e-13, atol=1e-13)
+    t = A.make_thermal(4, 3, 2, h, k)
+    np.testing.assert_allclose(np.array(t.ke).reshape(8, 8), d[f"ke_{tag}"], rtol=1e-13, atol=1e-13)
+    bad = d[f"ke_{tag}"].copy()
+    bad[0, 1] += 0.1 * abs(bad[0, 0])
+    with pytest.raises(A.PytoError):
+        A.make_thermal(4, 3, 2, h, k, ke=bad)

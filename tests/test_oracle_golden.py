@@ -146,3 +146,27 @@ def test_matvec_ebe_against_reference_solution(name, nel, h):
     v = np.random.default_rng(3).normal(size=d["u"].shape)
     yref = O.matvec_free(m, s, Ke, v, d["fixed"])
     assert np.abs(O.matvec_ebe(nel, s, Ke, v, d["fixed"]) - yref).max() <= 1e-13 * np.abs(yref).max()
+
+
+def test_thermal_ke_and_solve_match_reference():
+    """Thermal hex8: the oracle's Ke, assembly and direct solve against the
+    reference's HexThermalFEA (tests/golden/thermal.npz)."""
+    d = golden("thermal.npz")
+    np.testing.assert_allclose(O.ke_hex8_thermal(1.0, (1.0, 1.0, 1.0)), d["ke_unit"], rtol=1e-13, atol=1e-15)
+    np.testing.assert_allclose(O.ke_hex8_thermal(50.0, (1.0, 0.5, 2.0)), d["ke_box"], rtol=1e-13, atol=1e-13)
+    import scipy.sparse.linalg as spl
+    for tag, nel, h in (("12x6x6", (12, 6, 6), (1.0, 1.0, 1.0)), ("9x5x4_box", (9, 5, 4), (1.0, 0.5, 2.0))):
+        m = O.grid_mesh(*nel, h)
+        assert np.array_equal(m["elemArray"], d[f"{tag}_edof"])
+        Ke = O.ke_hex8_thermal(1.0, h)
+        s = O.thermal_scaling(d[f"{tag}_rho"], float(d["penal"]), float(d["kvoid"]))
+        K = O.assemble_K_thermal(m, s, Ke)
+        fixed = d[f"{tag}_fixed"]
+        free = np.setdiff1d(np.arange(m["num_nodes"]), fixed)
+        T = np.zeros(m["num_nodes"])
+        T[free] = spl.spsolve(K[free][:, free].tocsc(), d[f"{tag}_f"][free])
+        np.testing.assert_allclose(T, d[f"{tag}_T"], rtol=1e-10, atol=1e-12 * np.abs(T).max())
+        ce = (T[m["elemArray"]] @ Ke * T[m["elemArray"]]).sum(1)
+        assert abs(np.sum(s * ce) - float(d[f"{tag}_C"])) <= 1e-10 * float(d[f"{tag}_C"])
+        dC = -O.thermal_sensitivity(d[f"{tag}_rho"], float(d["penal"]), float(d["kvoid"])) * ce
+        np.testing.assert_allclose(dC, d[f"{tag}_dC"], rtol=1e-9, atol=1e-12 * np.abs(dC).max())
