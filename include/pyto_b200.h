@@ -353,6 +353,22 @@ int pyto_pnorm_adjoint(const pyto_operator_t* op, const double* u, const double*
  * NULL) restricts H to active elements (inactive outputs are 0). */
 int pyto_filter(const pyto_operator_t* op, double rel_radius, int mode, const double* x,
                 const double* w, const double* hs, const uint8_t* active, double* y, void* stream);
+/* Symmetry / extrusion map F of the element field of a full box grid (no active mask):
+ * y = F(x o pre) / post (pre, post may be NULL; y must not alias x).  kind
+ * PYTO_SYM_MIRROR: F x = (x + x[mirror about the mid-plane normal to axis]) / 2
+ * (createX/Y/ZSymmetryFilter, src/topopt_filters.py:292-393); PYTO_SYM_EXTRUDE: the
+ * reference's extrusion average along axis, whose lines are visited from their first
+ * element, which joins its line twice (createX/Y/ZExtrudeFilter, src/topopt_filters.py:
+ * 595-716).  Both maps are symmetric.  The composed filter H = H_s F_1 F_2 ... of
+ * createFilters (src/topopt_common.py:127-159) applies them before pyto_filter. */
+#define PYTO_SYM_MIRROR 0
+#define PYTO_SYM_EXTRUDE 1
+int pyto_symmetry_filter(const pyto_operator_t* op, int kind, int axis, const double* x, const double* pre,
+                         const double* post, double* y, void* stream);
+/* y = x o mul / (div1 o div2) over n entries (each factor may be NULL); the elementwise
+ * step of the composed filters.  No reference counterpart (numpy broadcasting there). */
+int pyto_vec_scale(int64_t n, const double* x, const double* mul, const double* div1, const double* div2,
+                   double* y, void* stream);
 /* One OC update with bisection on the volume multiplier (src/topopt_ocm.py:244-283),
  * the same bisection sequence as the reference.  x is updated in place; *change_out
  * (device) = max |x_new - x_old|.  dc is the filtered objective gradient.  With an active

@@ -28,6 +28,7 @@ __all__ = [
     "volume_constraint", "oc_update", "elements_with_forces", "topopt_oc",
     "cantilever_bc", "matvec_free", "matvec_ebe",
     "ke_hex8_thermal", "assemble_K_thermal", "thermal_scaling", "thermal_sensitivity",
+    "mirror_filter", "extrude_filter",
 ]
 
 
@@ -588,6 +589,44 @@ def smoothing_filter(mesh: dict, rel_filter_radius: float = 1.5):
                       shape=(mesh["num_elems"],) * 2).tocsc()
     Hs = np.array(H.sum(1)).squeeze()
     return H, Hs
+
+
+def mirror_filter(mesh: dict, axis: int) -> sp.csr_matrix:
+    """Mirror-symmetry filter about the mid-plane normal to `axis` on a full box grid
+    (createX/Y/ZSymmetryFilter, src/topopt_filters.py:292-393): row i holds 0.5 at i
+    and 0.5 at its mirror element, or 1.0 at i when i is its own mirror."""
+    n = (mesh["nelx"], mesh["nely"], mesh["nelz"])
+    ne = mesh["num_elems"]
+    e = np.arange(ne)
+    ijk = [e % n[0], (e // n[0]) % n[1], e // (n[0] * n[1])]
+    ijk[axis] = n[axis] - 1 - ijk[axis]
+    m = ijk[0] + n[0] * (ijk[1] + n[1] * ijk[2])
+    return (sp.coo_matrix((np.full(ne, 0.5), (e, e)), shape=(ne, ne))
+            + sp.coo_matrix((np.full(ne, 0.5), (e, m)), shape=(ne, ne))).tocsr()
+
+
+def extrude_filter(mesh: dict, axis: int) -> sp.csr_matrix:
+    """Extrusion filter along `axis` on a full box grid (createX/Y/ZExtrudeFilter,
+    src/topopt_filters.py:595-716): for each line of elements along axis, visited from
+    its lowest element id, the matching elements are the whole line plus that first
+    element once more, so with n elements per line and w = 1/(n+1) the summed COO
+    entries are w between two other elements, 2w between the first and another, 4w
+    on the first's diagonal."""
+    n = (mesh["nelx"], mesh["nely"], mesh["nelz"])
+    ne = mesh["num_elems"]
+    stride = (1, n[0], n[0] * n[1])[axis]
+    e = np.arange(ne)
+    first = e[((e // stride) % n[axis]) == 0]
+    rows, cols, vals = [], [], []
+    w = 1.0 / (n[axis] + 1)
+    for e0 in first:
+        match = [e0 + t * stride for t in range(n[axis])] + [e0]
+        for a in match:
+            for b in match:
+                rows.append(a)
+                cols.append(b)
+                vals.append(w)
+    return sp.coo_matrix((vals, (rows, cols)), shape=(ne, ne)).tocsr()
 
 
 # --------------------------------------------------------------------------

@@ -19,6 +19,7 @@ OK, NOT_CONVERGED = 0, 1
 ERR_ARG, ERR_CUDA, ERR_WORKSPACE, ERR_BREAKDOWN, ERR_TOO_LARGE = -1, -2, -3, -4, -5
 MASK_IN, MASK_OUT = 1, 2
 FILTER_RAW, FILTER_DENSITY, FILTER_CHAIN, FILTER_SENS, FILTER_HS = 0, 1, 2, 3, 4
+SYM_MIRROR, SYM_EXTRUDE = 0, 1
 WS_REDUCE, WS_PCG, WS_DPCG, WS_OC, WS_DPCG_MIXED = 0, 1, 2, 3, 4
 
 
@@ -124,6 +125,8 @@ SIGNATURES = {
     "pyto_pnorm_sum": (C.c_int, [_OP, _P, C.c_double, _P, _P, C.c_size_t, _P]),
     "pyto_pnorm_adjoint": (C.c_int, [_OP, _P, _P, C.c_double, C.c_double, _P, _P, _P, _P, _P]),
     "pyto_filter": (C.c_int, [_OP, C.c_double, C.c_int, _P, _P, _P, _P, _P, _P]),
+    "pyto_symmetry_filter": (C.c_int, [_OP, C.c_int, C.c_int, _P, _P, _P, _P, _P]),
+    "pyto_vec_scale": (C.c_int, [C.c_int64, _P, _P, _P, _P, _P, _P]),
     "pyto_oc_update": (C.c_int, [_OP, _P, _P, _P, C.c_longlong, C.c_double, C.c_double, C.c_double, C.c_double, _P,
                                  _P, C.c_size_t, _P]),
 }

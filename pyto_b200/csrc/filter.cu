@@ -183,3 +183,115 @@ extern "C" int pyto_filter(const pyto_operator_t* op, double rel_radius, int mod
     default: return PYTO_ERR_ARG;
   }
 }
+
+// ---------------------------------------------------------------------------
+// Symmetry and extrusion maps of the element field on a full box grid
+// (src/topopt_filters.py:292-393 mirror symmetry, :595-716 extrusion), composed
+// with the smoothing filter as H = H_s F_1 F_2 ... (src/topopt_common.py:127-159).
+// ---------------------------------------------------------------------------
+namespace pyto {
+
+__device__ __forceinline__ void elem_ijk(const GridDims& g, long long e, int& i, int& j, int& k) {
+  i = (int)(e % g.nx);
+  const long long r = e / g.nx;
+  j = (int)(r % g.ny);
+  k = (int)(r / g.ny);
+}
+
+// y_e = (F (x o pre))_e / post_e (pre, post may be null).  Mirror about the mid-plane
+// normal to `axis`: F x = (x + x[mirror]) / 2 (the self-mirrored middle layer keeps x).
+__global__ void k_mirror(GridDims g, int axis, const double* __restrict__ x, const double* __restrict__ pre,
+                         const double* __restrict__ post, double* __restrict__ y) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < g.nelem;
+       e += (long long)gridDim.x * blockDim.x) {
+    int i, j, k;
+    elem_ijk(g, e, i, j, k);
+    if (axis == 0) i = g.nx - 1 - i;
+    else if (axis == 1) j = g.ny - 1 - j;
+    else k = g.nz - 1 - k;
+    const long long m = i + (long long)g.nx * (j + (long long)g.ny * k);
+    const double a = x[e] * (pre ? pre[e] : 1.0), b = x[m] * (pre ? pre[m] : 1.0);
+    double v = 0.5 * (a + b);
+    if (post) v /= post[e];
+    y[e] = v;
+  }
+}
+
+// Extrusion along `axis`, with the reference's weights: the element lines along axis
+// are visited from the one with the lowest element id, whose first element joins its
+// own line twice, so with n elements per line and w = 1/(n+1):
+//   (F x)_e = w (sum_line x + x_first) * (2 if e is the line's first element else 1).
+// One thread per line.
+__global__ void k_extrude(GridDims g, int axis, const double* __restrict__ x, const double* __restrict__ pre,
+                          const double* __restrict__ post, double* __restrict__ y) {
+  const int n = axis == 0 ? g.nx : axis == 1 ? g.ny : g.nz;
+  const long long stride = axis == 0 ? 1 : axis == 1 ? g.nx : (long long)g.nx * g.ny;
+  const long long nlines = g.nelem / n;
+  for (long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x; l < nlines;
+       l += (long long)gridDim.x * blockDim.x) {
+    long long e0;  // first element of line l
+    if (axis == 0) e0 = l * g.nx;
+    else if (axis == 1) e0 = (l % g.nx) + (l / g.nx) * (long long)g.nx * g.ny;
+    else e0 = l;
+    double sum = 0.0;
+    for (int t = 0; t < n; ++t) {
+      const long long e = e0 + t * stride;
+      sum += x[e] * (pre ? pre[e] : 1.0);
+    }
+    sum += x[e0] * (pre ? pre[e0] : 1.0);
+    const double w = 1.0 / (n + 1);
+    for (int t = 0; t < n; ++t) {
+      const long long e = e0 + t * stride;
+      double v = (t == 0 ? 2.0 : 1.0) * w * sum;
+      if (post) v /= post[e];
+      y[e] = v;
+    }
+  }
+}
+
+// y = x o mul / (div1 o div2) (each factor optional)
+__global__ void k_vec_scale(long long n, const double* __restrict__ x, const double* __restrict__ mul,
+                            const double* __restrict__ div1, const double* __restrict__ div2,
+                            double* __restrict__ y) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    double v = x[i];
+    if (mul) v *= mul[i];
+    if (div1) v /= div1[i];
+    if (div2) v /= div2[i];
+    y[i] = v;
+  }
+}
+
+}  // namespace pyto
+
+extern "C" int pyto_symmetry_filter(const pyto_operator_t* op, int kind, int axis, const double* x,
+                                    const double* pre, const double* post, double* y, void* stream) {
+  if (!op || !x || !y || x == y || axis < 0 || axis > 2) return PYTO_ERR_ARG;
+  const GridDims g = make_dims(op);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (kind == PYTO_SYM_MIRROR) {
+    const int nb = (int)std::min<long long>((g.nelem + 255) / 256, 8 * kNumSMs);
+    k_mirror<<<nb, 256, 0, st>>>(g, axis, x, pre, post, y);
+  } else if (kind == PYTO_SYM_EXTRUDE) {
+    const int n = axis == 0 ? g.nx : axis == 1 ? g.ny : g.nz;
+    const long long nlines = g.nelem / n;
+    const int nb = (int)std::min<long long>((nlines + 127) / 128, 8 * kNumSMs);
+    k_extrude<<<nb, 128, 0, st>>>(g, axis, x, pre, post, y);
+  } else {
+    return PYTO_ERR_ARG;
+  }
+  PYTO_COUNT(1);
+  PYTO_LAUNCH_CHECK();
+  return PYTO_OK;
+}
+
+extern "C" int pyto_vec_scale(int64_t n, const double* x, const double* mul, const double* div1,
+                              const double* div2, double* y, void* stream) {
+  if (!x || !y || n < 0) return PYTO_ERR_ARG;
+  if (n == 0) return PYTO_OK;
+  const int nb = (int)std::min<long long>((n + 255) / 256, 8 * kNumSMs);
+  k_vec_scale<<<nb, 256, 0, (cudaStream_t)stream>>>(n, x, mul, div1, div2, y);
+  PYTO_COUNT(1);
+  PYTO_LAUNCH_CHECK();
+  return PYTO_OK;
+}

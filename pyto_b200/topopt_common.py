@@ -85,12 +85,21 @@ def find_elements_with_fixedDOF(mesh, bc, nDOFPerNode) -> np.ndarray:
 
 
 def createFilters(fe_solver, to_params):
-    """Smoothing filter (src/topopt_common.py:127-159); the symmetry / extrusion
-    filters composed into H there are outside the GPU path."""
-    from .topopt_filters import createSmoothingFilter
-    for flag in ("XSymmetry", "YSymmetry", "ZSymmetry", "ExtrudeX", "ExtrudeY", "ExtrudeZ"):
-        if getattr(to_params, flag):
-            raise NotImplementedError(f"{flag} filters are outside the GPU path")
+    """Smoothing filter composed with the symmetry / extrusion filters the flags ask for,
+    in the reference's order (src/topopt_common.py:127-159); returns (H, Hs).  Angular
+    symmetry is outside the GPU path (see topopt_filters)."""
+    from . import topopt_filters as tf
     if to_params.XAxisAngularSymmetry or to_params.YAxisAngularSymmetry or to_params.ZAxisAngularSymmetry:
         raise NotImplementedError("angular symmetry filters are outside the GPU path")
-    return createSmoothingFilter(fe_solver.mesh, rel_filter_radius=to_params.RelativeFilterRadius)
+    H, Hs = tf.createSmoothingFilter(fe_solver.mesh, rel_filter_radius=to_params.RelativeFilterRadius)
+    maps = []
+    for flag, fn in (("XSymmetry", tf.createXSymmetryFilter), ("YSymmetry", tf.createYSymmetryFilter),
+                     ("ZSymmetry", tf.createZSymmetryFilter), ("ExtrudeY", tf.createYExtrudeFilter),
+                     ("ExtrudeX", tf.createXExtrudeFilter), ("ExtrudeZ", tf.createZExtrudeFilter)):
+        if getattr(to_params, flag):
+            maps.append(fn(fe_solver.mesh))
+    if not maps:
+        return H, Hs
+    for m in maps:
+        H = H * m
+    return H, H.hs().cpu().numpy()

@@ -63,10 +63,13 @@ def main():
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--slow", action="store_true")
     ap.add_argument("--thermal", action="store_true", help="only the thermal hex8 goldens")
+    ap.add_argument("--filters", action="store_true", help="only the symmetry / extrusion filter goldens")
     ap.add_argument("--cfg13", action="store_true",
                     help="only the 60x30x30 tight-tolerance goldens (rho = 0.3 and the OC iterate-5 design)")
     args = ap.parse_args()
     install_shim(args.ref)
+    if "--filters" in sys.argv:
+        return sym_filters()
     ap_thermal = "--thermal" in sys.argv
     if args.cfg13:
         return cfg13()
@@ -268,6 +271,32 @@ def main():
         h, v, c, _ = run_oc((60, 30, 30), linear_solvers.Solvers.PCG, 10)
         np.savez_compressed(os.path.join(HERE, "cfg1_oc10.npz"), objective=h, volfrac=v, change=c)
     print("golden vectors written to", HERE)
+
+
+def sym_filters():
+    """Symmetry and extrusion filters (src/topopt_filters.py:292-393, :595-716) and their
+    composition with the smoothing filter by createFilters (src/topopt_common.py:127-159)
+    on small full grids."""
+    import hex_mesher
+    import topopt_common
+    import topopt_filters as tf
+
+    out = {}
+    for tag, nel, h in (("a", (7, 5, 4), (1.0, 1.0, 1.0)), ("b", (6, 3, 5), (1.0, 0.5, 2.0))):
+        m = hex_mesher.HexMesher()
+        m.grid_mesh(nel, h)
+        for name, fn in (("mx", tf.createXSymmetryFilter), ("my", tf.createYSymmetryFilter),
+                         ("mz", tf.createZSymmetryFilter), ("ex", tf.createXExtrudeFilter),
+                         ("ey", tf.createYExtrudeFilter), ("ez", tf.createZExtrudeFilter)):
+            Hc = fn(m).tocoo()
+            out[f"{tag}_{name}_row"], out[f"{tag}_{name}_col"], out[f"{tag}_{name}_val"] = Hc.row, Hc.col, Hc.data
+        params = topopt_common.TOParams(RelativeFilterRadius=1.5, XSymmetry=True, ZSymmetry=True, ExtrudeY=True)
+        H, Hs = topopt_common.createFilters(types.SimpleNamespace(mesh=m), params)
+        Hc = H.tocoo()
+        out[f"{tag}_all_row"], out[f"{tag}_all_col"], out[f"{tag}_all_val"] = Hc.row, Hc.col, Hc.data
+        out[f"{tag}_all_Hs"] = Hs
+    np.savez_compressed(os.path.join(HERE, "sym_filters.npz"), **out)
+    print("sym_filters.npz written")
 
 
 def thermal():

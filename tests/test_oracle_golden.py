@@ -170,3 +170,24 @@ def test_thermal_ke_and_solve_match_reference():
         assert abs(np.sum(s * ce) - float(d[f"{tag}_C"])) <= 1e-10 * float(d[f"{tag}_C"])
         dC = -O.thermal_sensitivity(d[f"{tag}_rho"], float(d["penal"]), float(d["kvoid"])) * ce
         np.testing.assert_allclose(dC, d[f"{tag}_dC"], rtol=1e-9, atol=1e-12 * np.abs(dC).max())
+
+
+@pytest.mark.parametrize("tag,nel,h", [("a", (7, 5, 4), (1.0, 1.0, 1.0)), ("b", (6, 3, 5), (1.0, 0.5, 2.0))])
+def test_symmetry_and_extrusion_filters_match_reference(tag, nel, h):
+    """Mirror / extrusion filters and the composed H = H_s HX HZ HEY of createFilters
+    against the reference's matrices (tests/golden/sym_filters.npz)."""
+    import scipy.sparse as sp
+    d = golden("sym_filters.npz")
+    m = O.grid_mesh(*nel, h)
+    ne = m["num_elems"]
+
+    def ref(name):
+        return sp.coo_matrix((d[f"{tag}_{name}_val"], (d[f"{tag}_{name}_row"], d[f"{tag}_{name}_col"])),
+                             shape=(ne, ne)).toarray()
+    for name, M in (("mx", O.mirror_filter(m, 0)), ("my", O.mirror_filter(m, 1)), ("mz", O.mirror_filter(m, 2)),
+                    ("ex", O.extrude_filter(m, 0)), ("ey", O.extrude_filter(m, 1)), ("ez", O.extrude_filter(m, 2))):
+        np.testing.assert_allclose(M.toarray(), ref(name), rtol=1e-15, atol=1e-15, err_msg=name)
+    H, _ = O.smoothing_filter(m, 1.5)
+    Ht = H @ O.mirror_filter(m, 0) @ O.mirror_filter(m, 2) @ O.extrude_filter(m, 1)
+    np.testing.assert_allclose(Ht.toarray(), ref("all"), rtol=1e-13, atol=1e-15)
+    np.testing.assert_allclose(np.asarray(Ht.sum(1)).ravel(), d[f"{tag}_all_Hs"], rtol=1e-13)
