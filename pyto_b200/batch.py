@@ -47,13 +47,17 @@ def max_over_ranks(seconds, group=None):
     return float(t.item())
 
 
-def point_load(mesh: HexMesher, rng):
-    """Unit force at a random node of the x = L face, random direction."""
+def point_load(mesh: HexMesher, rng, direction=None):
+    """Unit force at a random node of the x = L face: along `direction` (e.g. -z), or in
+    a random direction."""
     ni = mesh.node_indices
     face = np.flatnonzero(ni[:, 0] == mesh.grid[0])
     node = int(rng.choice(face))
-    d = rng.normal(size=3)
-    d /= np.linalg.norm(d)
+    if direction is None:
+        d = rng.normal(size=3)
+        d /= np.linalg.norm(d)
+    else:
+        d = np.asarray(direction, dtype=np.float64)
     f = np.zeros(3 * mesh.num_nodes)
     f[3 * node:3 * node + 3] = d
     return f
@@ -81,14 +85,18 @@ def batch_shapes(n_designs=64, min_nx=32, max_nx=96, seed=0):
                                               for _ in range(n_designs))]
 
 
-def batch_problems(n_designs=64, min_nx=32, max_nx=96, multi_nel=(128, 64, 64), n_loads=8, seed=0, device=None,
+def batch_problems(n_designs=64, min_nx=32, max_nx=96, multi_nel=(128, 64, 64), n_loads=8, seed=None, device=None,
                    rank=0, world=1):
-    """The batched workload: n_designs cantilevers with nx drawn in [min_nx, max_nx]
-    (even, ny = nz = nx / 2), one point load each, plus one multi_nel design with
-    n_loads load cases (units of partitioning: each design, and the multi-load design
-    as a whole).  With world > 1 only this rank's contiguous, DOF-balanced share is
-    built.  Returns a list of (grid, defl, s, b)."""
-    shapes = batch_shapes(n_designs, min_nx, max_nx, seed)
+    """The batched workload: n_designs cantilevers with nx drawn from {min_nx, min_nx+2,
+    ..., max_nx} (ny = nz = nx / 2, seed 2), densities U[0.01, 1] (stream (2, k) for
+    design k), one unit -z point load each at a random node of the x = L face (stream
+    (3, k)), plus one multi_nel design with n_loads load cases, unit point loads in
+    random directions on that face (stream (4, k)).  Units of partitioning: each design,
+    and the multi-load design as a whole; with world > 1 only this rank's contiguous,
+    DOF-balanced share is built.  `seed` replaces all three seeds (tests).  Returns a
+    list of (grid, defl, s, b)."""
+    s_shape, s_dens, s_load, s_multi = (2, 2, 3, 4) if seed is None else (seed,) * 4
+    shapes = batch_shapes(n_designs, min_nx, max_nx, s_shape)
     units = [(nel, 1) for nel in shapes]
     if multi_nel is not None and n_loads > 0:
         units.append((tuple(multi_nel), n_loads))
@@ -97,8 +105,12 @@ def batch_problems(n_designs=64, min_nx=32, max_nx=96, multi_nel=(128, 64, 64), 
     out = []
     for k in range(lo, hi):
         nel, nloads = units[k]
-        rng = np.random.default_rng((seed, k))  # per-unit stream: the same data on any rank count
-        mesh, g, defl, s = make_design(nel, rng, device=device)
-        for _ in range(nloads):
-            out.append((g, defl, s, g.tensor(point_load(mesh, rng))))
+        # per-unit streams: the same data on any rank count
+        mesh, g, defl, s = make_design(nel, np.random.default_rng((s_dens, k)), device=device)
+        if nloads == 1:
+            out.append((g, defl, s, g.tensor(point_load(mesh, np.random.default_rng((s_load, k)), (0.0, 0.0, -1.0)))))
+        else:
+            rng = np.random.default_rng((s_multi, k))
+            for _ in range(nloads):
+                out.append((g, defl, s, g.tensor(point_load(mesh, rng))))
     return out

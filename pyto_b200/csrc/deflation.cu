@@ -267,9 +267,14 @@ __device__ __forceinline__ double mode_hat_from_base(const double* B, int stride
 // Row blocks E[G, :] from the boundary element lists: one CTA per list chunk
 // (chunk tables as for k_restrict_K), one entry per thread per pass.  For entry
 // (G, e) and every group H at a corner of e, s_e (Phi W_G|e)^T K^ (Phi W_H|e) is
-// added into a shared-memory accumulator of G's neighbour slots (the sums of
-// one CTA are formed with shared-memory atomics, so their order varies), which
-// is then added into E with global atomics.
+// added into a shared-memory accumulator of G's neighbour slots, which is then
+// added into E with global atomics.  The sums are formed in 64-bit fixed point with
+// a power-of-two scale per row group (2^gexp[G], chosen by k_group_scale so that the
+// sum of the magnitudes of all of G's contributions stays below 2^61): integer
+// addition is associative, so E does not depend on the order of the atomics and
+// the coarse operator, its inverse and the solve are bitwise reproducible.  Each
+// contribution is rounded once, to 2^-gexp[G], at most 2^-61 of that magnitude
+// bound.  E is accumulated as int64 bits in place; k_coarse_from_fixed converts it.
 // Only the blocks E[G, H] with H <= G are formed (E is symmetric; k_mirror_upper
 // copies them into E[H, G]), and the mode loops are unrolled (M = dp.modes).
 constexpr int kCrThreads = 128;
@@ -285,17 +290,19 @@ __global__ void __launch_bounds__(kCrThreads) k_coarse_rows2(GridDims g, KHat kh
                                                              const int32_t* __restrict__ cgrp,
                                                              const int32_t* __restrict__ nptr,
                                                              const int32_t* __restrict__ nlist,
-                                                             double* __restrict__ E) {
+                                                             const int* __restrict__ gexp,
+                                                             unsigned long long* __restrict__ E) {
   extern __shared__ double cr_smem[];
   double* sbase = cr_smem;                  // [2][32][kCrThreads] group base vectors
-  double* acc = cr_smem + 64 * kCrThreads;  // [nnb][36]
+  unsigned long long* acc = reinterpret_cast<unsigned long long*>(cr_smem + 64 * kCrThreads);  // [nnb][36]
   __shared__ int snb[128];
   const int ch = blockIdx.x;
   if (ch >= cptr[dp.ngroups]) return;
   const int G = cgrp[ch];
+  const double scale = ldexp(1.0, gexp[G]);
   const int nb0 = nptr[G], nnb = nptr[G + 1] - nb0;
   for (int t = threadIdx.x; t < nnb; t += blockDim.x) snb[t] = nlist[nb0 + t];
-  for (int t = threadIdx.x; t < nnb * 36; t += blockDim.x) acc[t] = 0.0;
+  for (int t = threadIdx.x; t < nnb * 36; t += blockDim.x) acc[t] = 0ull;
   __syncthreads();
   const double h[3] = {dp.hx, dp.hy, dp.hz};
   const int end = bptr[G + 1];
@@ -391,8 +398,8 @@ __global__ void __launch_bounds__(kCrThreads) k_coarse_rows2(GridDims g, KHat kh
           }
 #pragma unroll
           for (int a = 0; a < M; ++a) {
-            const double v = se * vab[a];
-            if (v != 0.0) atomicAdd(&acc[Sl[hi] * 36 + a * 6 + b], v);
+            const long long qv = __double2ll_rn(se * vab[a] * scale);
+            if (qv != 0) atomicAdd(&acc[Sl[hi] * 36 + a * 6 + b], (unsigned long long)qv);
           }
         }
       }
@@ -434,7 +441,8 @@ __global__ void __launch_bounds__(kCrThreads) k_coarse_rows2(GridDims g, KHat kh
 #pragma unroll
             for (int m = 1; m < 8; ++m) v = fma(Z[c][m], Hh[m], v);
           }
-          if (v != 0.0) atomicAdd(&acc[Sl[hi] * 36 + a * 6 + b], v);
+          const long long qv = __double2ll_rn(v * scale);
+          if (qv != 0) atomicAdd(&acc[Sl[hi] * 36 + a * 6 + b], (unsigned long long)qv);
         }
       }
     }
@@ -442,8 +450,58 @@ __global__ void __launch_bounds__(kCrThreads) k_coarse_rows2(GridDims g, KHat kh
   __syncthreads();
   for (int t = threadIdx.x; t < nnb * M * M; t += blockDim.x) {
     const int slot = t / (M * M), a = (t / M) % M, b = t % M;
-    const double v = acc[slot * 36 + a * 6 + b];
-    if (v != 0.0) atomicAdd(&E[((long long)G * M + a) * dp.nc + (long long)snb[slot] * M + b], v);
+    const unsigned long long v = acc[slot * 36 + a * 6 + b];
+    if (v != 0ull) atomicAdd(&E[((long long)G * M + a) * dp.nc + (long long)snb[slot] * M + b], v);
+  }
+}
+
+// Fixed-point scale of each row group G: gexp[G] = 61 - e with 2^e above
+//   B_G = |Ke|_rows * 8 * max(1, R_G) * max(1, R'_G) * sum_{e in G's list} |s_e|,
+// a bound of the sum of the magnitudes of G's contributions: a contribution of
+// element e is |s_e w_G^T Ke w_H| <= |s_e| |Ke|_2 |w_G| |w_H| over the element's 8
+// corners, |w| <= sqrt(8) max(1, |rel|) for any rigid mode, R_G the largest distance
+// from G's centre to a corner of G's element box, R'_G the same from the centres of
+// G's neighbour groups.  One block per group, deterministic reduction.
+__global__ void __launch_bounds__(256) k_group_scale(DeflP dp, double ke_rows, const double* __restrict__ s,
+                                                      const double* __restrict__ gc,
+                                                      const int32_t* __restrict__ gbox,
+                                                      const int32_t* __restrict__ bptr,
+                                                      const int32_t* __restrict__ blist,
+                                                      const int32_t* __restrict__ nptr,
+                                                      const int32_t* __restrict__ nlist, int* __restrict__ gexp) {
+  __shared__ double sred[8];
+  const int G = blockIdx.x;
+  double acc = 0.0;
+  for (int t = bptr[G] + threadIdx.x; t < bptr[G + 1]; t += blockDim.x) acc += fabs(s[blist[t]]);
+  const double ssum = block_sum<256>(acc, sred);
+  if (threadIdx.x != 0) return;
+  const int* bx = gbox + 6 * G;
+  const double lo[3] = {dp.hx * bx[0], dp.hy * bx[2], dp.hz * bx[4]};
+  const double hi[3] = {dp.hx * (bx[1] + 1), dp.hy * (bx[3] + 1), dp.hz * (bx[5] + 1)};
+  auto reach = [&](const double* c) {  // largest distance from c to a corner of the box
+    double r2 = 0.0;
+    for (int d = 0; d < 3; ++d) {
+      const double a = fmax(fabs(lo[d] - c[d]), fabs(hi[d] - c[d]));
+      r2 += a * a;
+    }
+    return sqrt(r2);
+  };
+  const double RG = reach(gc + 3 * (long long)G);
+  double RH = RG;
+  for (int k = nptr[G]; k < nptr[G + 1]; ++k) RH = fmax(RH, reach(gc + 3 * (long long)nlist[k]));
+  const double B = ke_rows * 8.0 * fmax(1.0, RG) * fmax(1.0, RH) * ssum;
+  int e = 0;
+  if (B > 0.0 && isfinite(B)) frexp(B, &e);  // B < 2^e
+  gexp[G] = (B > 0.0 && isfinite(B)) ? 61 - e : 0;
+}
+
+// E (int64 fixed-point bits of the blocks with H <= G) -> FP64 values
+__global__ void k_coarse_from_fixed(long long n, int modes, const int* __restrict__ gexp, double* E) {
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n * n;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long i = t / n;
+    const long long q = reinterpret_cast<const long long*>(E)[t];
+    E[t] = ldexp((double)q, -gexp[i / modes]);
   }
 }
 
@@ -1405,6 +1463,7 @@ struct DpcgWs {
   int32_t* cptr;       // boundary-list chunk table [ngroups+1]
   int32_t* cgrp;       // group of each chunk [kRkMaxChunks]
   unsigned* gcount;    // per-group chunk counters [ngroups]
+  int* gexp;           // fixed-point exponent of each row group of the coarse assembly
   double *P, *Rp, *U;  // sweep scratch
   // mixed-precision inner solve (FP32 vectors), carved only for the mixed solver
   float *r32, *p32, *q32, *z32, *x32, *b32, *s32;
@@ -1434,6 +1493,7 @@ static DpcgWs carve_dpcg(const pyto_operator_t* op, long long nc, void* ws, size
   W.cptr = cv.take<int32_t>((size_t)kMaxCoarse + 1);
   W.cgrp = cv.take<int32_t>((size_t)kRkMaxChunks);
   W.gcount = cv.take<unsigned>((size_t)kMaxCoarse);
+  W.gexp = cv.take<int>((size_t)kMaxCoarse);
   W.cv = cv.take<double>(2 * (nc > 0 ? nc : 1));  // k_restrict_K writes 6 slots per group
   W.mu = cv.take<double>(nc > 0 ? nc : 1);
   W.P = cv.take<double>(2 * kSweepB * kSweepB);
@@ -1591,14 +1651,27 @@ static int coarse_assemble_launch(const pyto_operator_t* op, const double* s, co
                                      (int)(64 * kCrThreads * sizeof(double) + 128 * 36 * sizeof(double))));
       attr.done();
     }
+    double ke_rows = 0.0;  // max absolute row sum of Ke (>= its spectral norm)
+    for (int i = 0; i < 24; ++i) {
+      double r = 0.0;
+      for (int j = 0; j < 24; ++j) r += fabs(op->ke[24 * i + j]);
+      ke_rows = std::max(ke_rows, r);
+    }
+    k_group_scale<<<dp.ngroups, 256, 0, st>>>(dp, ke_rows, s, defl->group_center, defl->group_box, defl->bel_ptr,
+                                             defl->bel_list, defl->nbr_ptr, defl->nbr_list, W.gexp);
+    PYTO_COUNT(1);
+    unsigned long long* Eq = reinterpret_cast<unsigned long long*>(E);
     if (dp.modes == 6)
       k_coarse_rows2<6><<<nchunks, kCrThreads, shm2, st>>>(g, make_khat(op), dp, s, mask, defl->node_group,
                                                           defl->group_center, defl->bel_ptr, defl->bel_list, W.cptr,
-                                                          W.cgrp, defl->nbr_ptr, defl->nbr_list, E);
+                                                          W.cgrp, defl->nbr_ptr, defl->nbr_list, W.gexp, Eq);
     else
       k_coarse_rows2<3><<<nchunks, kCrThreads, shm2, st>>>(g, make_khat(op), dp, s, mask, defl->node_group,
                                                           defl->group_center, defl->bel_ptr, defl->bel_list, W.cptr,
-                                                          W.cgrp, defl->nbr_ptr, defl->nbr_list, E);
+                                                          W.cgrp, defl->nbr_ptr, defl->nbr_list, W.gexp, Eq);
+    PYTO_COUNT(1);
+    k_coarse_from_fixed<<<(int)std::min<long long>((n * n + 255) / 256, 8 * kNumSMs), 256, 0, st>>>(n, dp.modes,
+                                                                                                   W.gexp, E);
     PYTO_COUNT(1);
     k_mirror_upper<<<(int)std::min<long long>((n * n + 255) / 256, 8 * kNumSMs), 256, 0, st>>>(n, dp.modes, E);
     PYTO_COUNT(1);

@@ -594,3 +594,29 @@ def test_lshape_active_mask():
     assert abs(C.item() - float(d["C"])) <= 1e-10 * float(d["C"])
     vm = g.stress(u, _dev(rho), 0.5, want=("vm",))["vm"].cpu().numpy()
     np.testing.assert_allclose(vm[d["active"]], d["vm"], rtol=1e-9)
+
+
+@pytest.mark.parametrize("modes", [6, 3])
+def test_coarse_setup_and_solves_bitwise_reproducible(modes):
+    """The coarse matrix is summed in fixed point (order-independent), so repeated
+    set-ups give the same bits, and so do repeated FP64 and mixed solves."""
+    from pyto_b200.engine import DeviceDeflation
+    nel = (48, 24, 24)
+    m = O.grid_mesh(*nel)
+    f, fixed = O.cantilever_bc(m)
+    g = _grid(nel, fixed=fixed)
+    s, _ = g.simp(_dev(np.random.default_rng(6).uniform(0.01, 1.0, m["num_elems"])), 3.0, 1e-9)
+    grp, cnt, cen = O.deflation_groups(m["node_xyz"], 60)
+    defl = DeviceDeflation(g, grp, cen, modes=modes, shift=1e-14, shift_relative=True)
+    g.dpcg_setup(s, defl)
+    e1 = defl.coarse_inv.clone()
+    for _ in range(3):
+        g.dpcg_setup(s, defl)
+        assert torch.equal(defl.coarse_inv, e1)
+    b = _dev(f)
+    u1, _ = g.dpcg(s, b, defl, rtol=1e-9, stop_rule=0)
+    u2, _ = g.dpcg(s, b, defl, rtol=1e-9, stop_rule=0)
+    assert torch.equal(u1, u2)
+    v1, _ = g.dpcg_mixed(s, b, defl, rtol=1e-9)
+    v2, _ = g.dpcg_mixed(s, b, defl, rtol=1e-9)
+    assert torch.equal(v1, v2)
