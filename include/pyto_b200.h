@@ -377,6 +377,31 @@ int pyto_oc_update(const pyto_operator_t* op, double* x, const double* dc, const
                    long long n_active, double volfrac, double move, double xmin, double xmax,
                    double* change_out, void* ws, size_t ws_bytes, void* stream);
 
+/* ---- MMA update of the density-based optimiser ------------------------------------- */
+/* One subproblem of the method of moving asymptotes (K. Svanberg's 2007 mmasub/subsolv,
+ * the algorithm of the third-party mmasub that src/mmaWrapper.py:91-94 calls) on the
+ * device, for n design variables and 1 <= m <= 4 constraints f_j(x) <= 0, in one
+ * cooperative kernel.  Device arrays: x (in: the current design, out: the subproblem's
+ * solution), xold1, xold2 (the two previous designs; may be NULL while iter <= 2),
+ * xmin, xmax (per-variable bounds, or NULL: xmin_s / xmax_s), df0dx [n], dfdx [m][n],
+ * low, upp (the asymptotes, updated), dual_out (may be NULL: y[m], z, lam[m], mu[m], zet,
+ * s[m], Newton steps).  Host arrays: fval, a, c, d [m].  The workspace also keeps the
+ * subproblem state read by pyto_mma_kkt.  No reference counterpart in this library's
+ * other entry points: PyTO's MMA runs on the host. */
+size_t pyto_mma_workspace_bytes(int64_t n, int m);
+int pyto_mma_update(int64_t n, int m, int iter, double* x, const double* xold1, const double* xold2,
+                    const double* xmin, const double* xmax, double xmin_s, double xmax_s, const double* df0dx,
+                    const double* fval, const double* dfdx, double* low, double* upp, double a0, const double* a,
+                    const double* c, const double* d, double move, double* dual_out, void* ws, size_t ws_bytes,
+                    void* stream);
+/* KKT residual of the original problem at the last update's solution, with the
+ * gradients evaluated there (kktcheck of the same package): kkt_out[0] = its 2-norm,
+ * kkt_out[1] = its max |.| (host doubles; synchronises the stream). */
+int pyto_mma_kkt(int64_t n, int m, const double* x, const double* xmin, const double* xmax, double xmin_s,
+                 double xmax_s, const double* df0dx, const double* fval, const double* dfdx, double a0,
+                 const double* a, const double* c, const double* d, double* kkt_out, void* ws, size_t ws_bytes,
+                 void* stream);
+
 /* ---- thermal hex8 (one temperature DOF per node) ----------------------------------- */
 /* Grid + the 8x8 conduction matrix of a box element.  For a box element Ke[a][b] depends
  * only on which coordinates of corners a and b differ: kxor[d] with d = bits(a) ^ bits(b),

@@ -116,6 +116,11 @@ SIGNATURES = {
     "pyto_thermal_pcg_solve": (C.c_int, [_TH, _P, _P, _P, _P, C.POINTER(SolveCfg), C.POINTER(SolveStatus), _P,
                                          C.c_size_t, _P]),
     "pyto_thermal_energy": (C.c_int, [_TH, _P, _P, _P, _P, _P, _P, C.c_size_t, _P]),
+    "pyto_mma_workspace_bytes": (C.c_size_t, [C.c_int64, C.c_int]),
+    "pyto_mma_update": (C.c_int, [C.c_int64, C.c_int, C.c_int, _P, _P, _P, _P, _P, C.c_double, C.c_double, _P, _P,
+                                  _P, _P, _P, C.c_double, _P, _P, _P, C.c_double, _P, _P, C.c_size_t, _P]),
+    "pyto_mma_kkt": (C.c_int, [C.c_int64, C.c_int, _P, _P, _P, C.c_double, C.c_double, _P, _P, _P, C.c_double, _P, _P,
+                               _P, _P, _P, C.c_size_t, _P]),
     "pyto_batch_create": (C.c_int, [C.POINTER(BatchItem), C.c_int, C.POINTER(SolveCfg), C.POINTER(C.c_void_p), _P]),
     "pyto_batch_launch": (C.c_int, [_P, _P]),
     "pyto_batch_status": (C.c_int, [_P, C.POINTER(SolveStatus), _P]),

@@ -191,3 +191,31 @@ def test_symmetry_and_extrusion_filters_match_reference(tag, nel, h):
     Ht = H @ O.mirror_filter(m, 0) @ O.mirror_filter(m, 2) @ O.extrude_filter(m, 1)
     np.testing.assert_allclose(Ht.toarray(), ref("all"), rtol=1e-13, atol=1e-15)
     np.testing.assert_allclose(np.asarray(Ht.sum(1)).ravel(), d[f"{tag}_all_Hs"], rtol=1e-13)
+
+
+def test_mma_restatement_reaches_the_kkt_point():
+    """The oracle's MMA (restated from the published algorithm; the reference's mmapy
+    is not installed) on a convex separable problem, min sum c_i / x_i s.t.
+    sum x_i <= V, reaches the closed-form optimum x_i = sqrt(c_i / lam)."""
+    from oracle import mma as M
+    rng = np.random.default_rng(0)
+    n = 50
+    cc = rng.uniform(1, 4, n)
+    V = 0.4 * n
+    x = np.full(n, 0.5)
+    xold1, xold2, low, upp = x.copy(), x.copy(), np.zeros(n), np.ones(n)
+    sc = None
+    for it in range(1, 80):
+        f0, df0 = np.sum(cc / x), -cc / x ** 2
+        sc = f0 if sc is None else sc
+        out = M.mmasub(1, n, it, x, np.full(n, 1e-3), np.ones(n), xold1, xold2, f0 / sc, df0 / sc,
+                       np.array([x.sum() / V - 1]), np.ones((1, n)) / V, low, upp, 1.0, np.zeros(1),
+                       np.full(1, 100.0), np.ones(1), 0.2)
+        xold2, xold1, x = xold1, x, out[0]
+        low, upp = out[-2], out[-1]
+    lo, hi = 1e-6, 1e6
+    for _ in range(200):
+        lam = np.sqrt(lo * hi)
+        xs = np.clip(np.sqrt(cc / lam), 1e-3, 1)
+        lo, hi = (lam, hi) if xs.sum() > V else (lo, lam)
+    assert np.abs(x - xs).max() < 1e-6
