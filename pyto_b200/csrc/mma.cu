@@ -437,17 +437,21 @@ int mma_grid_blocks() {
   return std::max(1, std::min(per_sm, 2)) * sms;
 }
 
+// the partials buffer is carved for the largest grid either kernel launches, so that
+// every array after it sits at the same offset for pyto_mma_update and pyto_mma_kkt
+constexpr int kMmaCarveBlocks = 4 * kNumSMs;
+
 struct MmaWs {
   double *alfa, *beta, *p0, *q0, *P, *Q, *xsi, *eta, *xo, *xsio, *etao, *part, *dual, *kpart;
   unsigned* counter;
 };
 
-static MmaWs carve_mma(long long n, int m, int nb, void* ws, size_t bytes, size_t* need) {
+static MmaWs carve_mma(long long n, int m, void* ws, size_t bytes, size_t* need) {
   Carver cv{(char*)ws, 0, bytes};
   MmaWs W;
   W.counter = cv.take<unsigned>(64);
   W.dual = cv.take<double>(32);
-  W.part = cv.take<double>(2 * (size_t)std::max(nb, 1) * kMmaSlots);
+  W.part = cv.take<double>(2 * (size_t)kMmaCarveBlocks * kMmaSlots);
   W.kpart = cv.take<double>(4 * (size_t)kNumSMs);
   W.alfa = cv.take<double>(n);
   W.beta = cv.take<double>(n);
@@ -471,7 +475,7 @@ using namespace pyto;
 extern "C" size_t pyto_mma_workspace_bytes(int64_t n, int m) {
   if (n <= 0 || m < 1 || m > kMmaMaxM) return 0;
   size_t need = 0;
-  carve_mma(n, m, 4 * kNumSMs, nullptr, 0, &need);
+  carve_mma(n, m, nullptr, 0, &need);
   return need;
 }
 
@@ -486,9 +490,9 @@ extern "C" int pyto_mma_update(int64_t n, int m, int iter, double* x, const doub
   if (iter > 2 && (!xold1 || !xold2)) return PYTO_ERR_ARG;
   int nb = mma_grid_blocks();
   if (nb <= 0) return PYTO_ERR_CUDA;
-  nb = (int)std::min<long long>(nb, std::max<long long>(1, (n + kMmaThreads - 1) / kMmaThreads));
+  nb = (int)std::min<long long>(std::min(nb, kMmaCarveBlocks), std::max<long long>(1, (n + kMmaThreads - 1) / kMmaThreads));
   size_t need = 0;
-  MmaWs W = carve_mma(n, m, nb, ws, ws_bytes, &need);
+  MmaWs W = carve_mma(n, m, ws, ws_bytes, &need);
   if (!ws || ws_bytes < need) return PYTO_ERR_WORKSPACE;
   MmaP P{};
   P.n = n;
@@ -542,7 +546,7 @@ extern "C" int pyto_mma_kkt(int64_t n, int m, const double* x, const double* xmi
   if (n <= 0 || m < 1 || m > kMmaMaxM || !x || !df0dx || !fval || !dfdx || !a || !c || !d || !kkt_out)
     return PYTO_ERR_ARG;
   size_t need = 0;
-  MmaWs W = carve_mma(n, m, 4 * kNumSMs, ws, ws_bytes, &need);
+  MmaWs W = carve_mma(n, m, ws, ws_bytes, &need);
   if (!ws || ws_bytes < need) return PYTO_ERR_WORKSPACE;
   cudaStream_t st = (cudaStream_t)stream;
   double host_dual[3 + 4 * kMmaMaxM];

@@ -37,7 +37,8 @@ def _timeit(fn, reps, warm=3):
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--kernel", default="matvec", choices=["matvec", "matvec32", "energy", "filter", "jacobi", "stress", "dpcg",
-                                                          "mixed", "pcg", "batch", "oc", "adjoint", "ocupdate"])
+                                                          "mixed", "pcg", "batch", "oc", "adjoint", "ocupdate",
+                                                          "thermal", "mma"])
     ap.add_argument("--iters", type=int, default=20, help="--kernel oc: OC iterations")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"], help="--kernel oc: DPCG form")
     ap.add_argument("--warm-start", action="store_true", help="--kernel oc: start each solve from the previous one")
@@ -59,6 +60,10 @@ def main(argv=None):
     if a.kernel == "oc":
         return oc_bench(a)
     nel = tuple(int(v) for v in a.nel.split(","))
+    if a.kernel == "thermal":
+        return thermal_bench(a, nel)
+    if a.kernel == "mma":
+        return mma_bench(a, nel)
     A.call("pyto_tune", 0, a.variant)
     if a.variant32 is not None:
         A.call("pyto_tune", 1, a.variant32)
@@ -175,6 +180,43 @@ def run_oc(nel, n_iters=20, precision="mixed", groups=432, warm_start=False):
             "iterations": n_iters, "fea_solves": int(nfea), "krylov_iterations": sum(iters), "s": t,
             "ms_per_iteration": 1e3 * t / max(1, nfea), "objective_first": obj[0],
             "objective_last": obj[-1], "volfrac_last": float(hist["volfrac"][-1])}
+
+
+def thermal_bench(a, nel):
+    """Thermal operator K(s) T (8x8 conduction Ke, one DOF per node), output mask only:
+    algorithmic bytes = 8 (T read) + 8 (y write) + 1 (mask) per node + 8 per element (s)."""
+    from .engine import ThermalGrid
+    g = ThermalGrid(nel)
+    g.set_fixed_nodes(np.flatnonzero(np.arange(g.nnodes) % (nel[0] + 1) == 0))
+    rng = np.random.default_rng(0)
+    s = g.tensor(rng.uniform(0.01, 1.0, g.nelem))
+    u = g.tensor(rng.normal(size=g.nnodes))
+    y = torch.empty_like(u)
+    t = _timeit(lambda: g.matvec(s, u, mode=A.MASK_OUT, out=y), a.reps, a.warm)
+    nbytes = 17 * g.nnodes + 8 * g.nelem
+    print(json.dumps({"kernel": "thermal", "nel": nel, "ms": t * 1e3, "algorithmic_bytes": nbytes,
+                      "GB_s": nbytes / t / 1e9}))
+
+
+def mma_bench(a, nel):
+    """One MMA update (one constraint) over the elements of the grid."""
+    from .topopt_mma import DeviceMMA
+    n = int(np.prod(nel))
+    rng = np.random.default_rng(0)
+    dev = torch.device("cuda")
+    T = lambda v: torch.as_tensor(v, dtype=torch.float64, device=dev)
+    x0 = T(rng.uniform(0.1, 0.9, n))
+    df0 = T(-rng.uniform(0.0, 2.0, n) / n)
+    dfdx = T(np.full((1, n), 1.0 / (0.3 * n)))
+    mm = DeviceMMA(n, 1, 1e-6, 1 - 1e-6, 0.2, dev)
+    x = x0.clone()
+
+    def fn():
+        x.copy_(x0)
+        mm.iter = 0
+        mm.update(x, df0, np.array([0.05]), dfdx)
+    t = _timeit(fn, a.reps, a.warm)
+    print(json.dumps({"kernel": "mma", "n": n, "ms": t * 1e3, "newton_steps": float(mm.dual[-1].item())}))
 
 
 def batch_bench(a):
