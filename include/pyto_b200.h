@@ -138,8 +138,10 @@ long long pyto_launch_count(void);
  * choice of the project's autotuner).  PYTO_KERNEL_MATVEC variants 0..3 (tile kernel,
  * default 2) and 8..10 (chunk-staged kernel: node-plane rows copied as 16-byte chunks,
  * faces and pending accumulators in registers; bitwise-equal results); PYTO_KERNEL_MATVEC32
- * variants 0..5, 8..11, 12..14 (chunk-staged, two element rows per thread) and 15..17
- * (the same with the two rows as packed FP32x2 lanes; default 16).  The chunk-staged
+ * variants 0..5, 8..11, 12..14 (chunk-staged, two element rows per thread), 15..17
+ * (the same with the two rows as packed FP32x2 lanes) and 18, 19 (packed, element core
+ * specialised to the block structure of an isotropic box / cube Ke, default 18; other
+ * Ke run variant 16's kernel).  The chunk-staged
  * variants need u and the mask 16-byte aligned and otherwise run the tile kernel.
  * Process-wide; not thread-safe against concurrent launches. */
 #define PYTO_KERNEL_MATVEC 0

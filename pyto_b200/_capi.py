@@ -14,6 +14,9 @@ import torch
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libpyto_b200.so")
+# library defaults of pyto_tune(PYTO_KERNEL_MATVEC / PYTO_KERNEL_MATVEC32, ...)
+MV64_DEFAULT = 2
+MV32_DEFAULT = 18
 
 OK, NOT_CONVERGED = 0, 1
 ERR_ARG, ERR_CUDA, ERR_WORKSPACE, ERR_BREAKDOWN, ERR_TOO_LARGE = -1, -2, -3, -4, -5

@@ -18,7 +18,7 @@ from . import _capi as A
 
 _CACHE: dict = {}
 VARIANTS = (0, 1, 2, 3, 8, 9, 10)  # 8-10: chunk-staged planes, faces and accumulators in registers
-VARIANTS_F32 = (0, 1, 2, 3, 4, 5, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17)  # 4, 5: tensor-core contraction
+VARIANTS_F32 = (0, 1, 2, 3, 4, 5, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18, 19)  # 4, 5: tensor-core contraction
 # (BF16 split); 12-14: chunk-staged with two element rows per thread; 15-17: the same
 # with the two rows as packed FP32x2 lanes
 

@@ -207,7 +207,13 @@ struct f32x2 {
 __device__ __forceinline__ f32x2 operator+(f32x2 a, f32x2 b) { return f32x2(__fadd2_rn(a.v, b.v)); }
 __device__ __forceinline__ f32x2 operator-(f32x2 a) { return f32x2(-a.v.x, -a.v.y); }
 __device__ __forceinline__ f32x2 operator-(f32x2 a, f32x2 b) {
-  return f32x2(__fadd2_rn(a.v, make_float2(-b.v.x, -b.v.y)));
+  // one packed subtraction (sub.rn.f32x2), each lane rounded as the scalar a - b
+  f32x2 r;
+  asm("{\n\t.reg .b64 pa, pb, pd;\n\tmov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
+      "sub.rn.f32x2 pd, pa, pb;\n\tmov.b64 {%0, %1}, pd;\n\t}"
+      : "=f"(r.v.x), "=f"(r.v.y)
+      : "f"(a.v.x), "f"(a.v.y), "f"(b.v.x), "f"(b.v.y));
+  return r;
 }
 __device__ __forceinline__ f32x2 operator*(f32x2 a, f32x2 b) { return f32x2(__fmul2_rn(a.v, b.v)); }
 __device__ __forceinline__ f32x2 fma(f32x2 a, f32x2 b, f32x2 c) { return f32x2(__ffma2_rn(a.v, b.v, c.v)); }

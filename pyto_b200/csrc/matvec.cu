@@ -107,6 +107,7 @@ __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_g
 }  // namespace pyto
 #include "matvec_chunked.cuh"
 #include "matvec_chunked2.cuh"
+#include "matvec_pair.cuh"
 namespace pyto {
 
 template <typename T, int TY, bool DOT, bool MASKIN, int MINB, bool TC = false>
@@ -606,6 +607,59 @@ static int launch_mvc2(const GridDims& g, const KHat& kh, const T* s, const uint
                                                              st, stop);
 }
 
+template <int TY, bool DOT, bool MI, int MINB, int KS>
+static int launch_pair_t(const GridDims& g, const KHatT<float>& kh, const float* s, const uint8_t* mask,
+                         const float* u, float* y, int mode, double* part, unsigned* counter, double* dot,
+                         cudaStream_t st, const int* stop) {
+  constexpr size_t smem = PairTile<TY>::bytes;
+  static PerDevice attr;
+  static std::atomic<int> slots{0};
+  if (attr.needed()) {
+    PYTO_CUDA(cudaFuncSetAttribute(k_matvec_pair<TY, DOT, MI, MINB, KS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem));
+    slots.store(resident_slots(k_matvec_pair<TY, DOT, MI, MINB, KS>, 32 * TY, smem));
+    attr.done();
+  }
+  const int bx = (g.sx + 30) / 31, by = (g.sy + 2 * TY - 2) / (2 * TY - 1);
+  const int zc = matvec_zc(bx, by, g.sz, slots.load());
+  const dim3 grid(bx, by, (g.sz + zc - 1) / zc);
+  k_matvec_pair<TY, DOT, MI, MINB, KS><<<grid, 32 * TY, smem, st>>>(g, kh, s, mask, u, y, zc, mode, part, counter,
+                                                                    dot, stop);
+  PYTO_COUNT(1);
+  PYTO_LAUNCH_CHECK();
+  return PYTO_OK;
+}
+
+template <int TY, int MINB, int KS>
+static int launch_pair_ks(const GridDims& g, const KHatT<float>& kt, const float* s, const uint8_t* mask,
+                          const float* u, float* y, int mode, double* part, unsigned* counter, double* dot,
+                          cudaStream_t st, const int* stop) {
+  const bool mi = (mode & PYTO_MASK_IN) && mask != nullptr;
+  if (dot)
+    return mi ? launch_pair_t<TY, true, true, MINB, KS>(g, kt, s, mask, u, y, mode, part, counter, dot, st, stop)
+              : launch_pair_t<TY, true, false, MINB, KS>(g, kt, s, mask, u, y, mode, part, counter, dot, st, stop);
+  return mi ? launch_pair_t<TY, false, true, MINB, KS>(g, kt, s, mask, u, y, mode, nullptr, nullptr, nullptr, st,
+                                                       stop)
+            : launch_pair_t<TY, false, false, MINB, KS>(g, kt, s, mask, u, y, mode, nullptr, nullptr, nullptr, st,
+                                                        stop);
+}
+
+// packed two-row kernel with the element core specialised to K^'s structure; a Ke
+// without that structure, or u / the mask not 16-byte aligned: k_matvec_chunked2 /
+// the tile kernel
+template <int TY, int MINB>
+static int launch_pair(const GridDims& g, const KHat& kh, const float* s, const uint8_t* mask, const float* u,
+                       float* y, int mode, double* part, unsigned* counter, double* dot, cudaStream_t st,
+                       const int* stop) {
+  const int ks = khat_structure(kh);
+  if (ks == KS_DENSE || ((uintptr_t)u & 15) || ((uintptr_t)mask & 15))
+    return launch_mvc2<float, TY, MINB, true>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
+  const KHatT<float> kt = make_khat_pair(kh, ks);
+  if (ks == KS_CUBE)
+    return launch_pair_ks<TY, MINB, KS_CUBE>(g, kt, s, mask, u, y, mode, part, counter, dot, st, stop);
+  return launch_pair_ks<TY, MINB, KS_BOX>(g, kt, s, mask, u, y, mode, part, counter, dot, st, stop);
+}
+
 // Tile variant of the FP64 matvec (2 = default: fastest measured at 192x96x96):
 //   0: 32x8 threads, 2 CTAs/SM (128 registers)   1: 32x8, 1 CTA/SM (no register cap)
 //   2: 32x4, 3 CTAs/SM                            3: 32x16, 1 CTA/SM
@@ -613,8 +667,9 @@ static int g_mv_variant = 2;
 // Tile variant of the FP32 matvec (same numbering; 4 and 5: the tile shapes of 0 and
 // 2 with the element core on the tensor cores, BF16 split hi/lo; 8-11: chunk-staged
 // kernel; 12-14: chunk-staged with two element rows per thread; 15-17: the same with
-// the two rows as packed FP32x2 lanes, 16 = default: fastest measured at 192x96x96)
-static int g_mv32_variant = 16;
+// the two rows as packed FP32x2 lanes; 18, 19: packed two-row kernel with the element
+// core specialised to K^'s structure, 18 = default: fastest measured at 192x96x96)
+static int g_mv32_variant = 18;
 
 int launch_matvec64(const pyto_operator_t* op, const double* s, const uint8_t* mask, const double* u, double* y,
                     int mode, double* part, unsigned* counter, double* dot, cudaStream_t st,
@@ -639,7 +694,9 @@ int launch_matvec32(const pyto_operator_t* op, const float* s, const uint8_t* ma
   const GridDims g = make_dims(op);
   const KHat kh = make_khat(op);
   const int tv = ((op->tune >> 8) & 0xff) - 1;
-  switch ((tv >= 0 && tv <= 5) || (tv >= 8 && tv <= 17) ? tv : g_mv32_variant) {
+  switch ((tv >= 0 && tv <= 5) || (tv >= 8 && tv <= 19) ? tv : g_mv32_variant) {
+    case 18: return launch_pair<4, 3>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
+    case 19: return launch_pair<8, 1>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
     case 15: return launch_mvc2<float, 8, 2, true>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
     case 16: return launch_mvc2<float, 4, 3, true>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
     case 17: return launch_mvc2<float, 8, 1, true>(g, kh, s, mask, u, y, mode, part, counter, dot, st, stop);
@@ -669,7 +726,7 @@ int set_matvec_variant(int v) {
 }
 
 int set_matvec32_variant(int v) {
-  if (v < 0 || (v > 5 && v < 8) || v > 17) return PYTO_ERR_ARG;
+  if (v < 0 || (v > 5 && v < 8) || v > 19) return PYTO_ERR_ARG;
   g_mv32_variant = v;
   return PYTO_OK;
 }

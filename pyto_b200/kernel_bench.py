@@ -52,6 +52,7 @@ def main(argv=None):
     ap.add_argument("--variant32", type=int, default=None, help="FP32 matvec tile variant (pyto_tune)")
     ap.add_argument("--delta", type=float, default=1e-1, help="reliable-update threshold for --kernel mixed")
     ap.add_argument("--mode", type=int, default=3, help="--kernel matvec/matvec32: BC mask mode (1 in, 2 out)")
+    ap.add_argument("--dot", action="store_true", help="--kernel matvec/matvec32: with the fused u.y (solver form)")
     ap.add_argument("--stop-rule", type=int, default=0, choices=[0, 1, 2], help="--kernel dpcg: stopping rule")
     ap.add_argument("--check-every", type=int, default=20, help="--kernel dpcg/mixed/pcg: iterations between host polls")
     a = ap.parse_args(argv)
@@ -76,11 +77,11 @@ def main(argv=None):
     u = g.tensor(rng.normal(size=g.ndof))
     y = torch.empty_like(u)
     if a.kernel == "matvec":
-        fn, nbytes = (lambda: g.matvec(s, u, mode=a.mode, out=y)), 48 * g.nnodes + 8 * g.nelem + g.nnodes
+        fn, nbytes = (lambda: g.matvec(s, u, mode=a.mode, out=y, dot=a.dot)), 48 * g.nnodes + 8 * g.nelem + g.nnodes
     elif a.kernel == "matvec32":
         s32, u32 = s.float(), u.float()
         y32 = torch.empty_like(u32)
-        fn, nbytes = (lambda: g.matvec_f32(s32, u32, mode=a.mode, out=y32)), 24 * g.nnodes + 4 * g.nelem + g.nnodes
+        fn, nbytes = (lambda: g.matvec_f32(s32, u32, mode=a.mode, out=y32, dot=a.dot)), 24 * g.nnodes + 4 * g.nelem + g.nnodes
     elif a.kernel == "energy":
         fn, nbytes = (lambda: g.energy(u, s=s)), 24 * g.nnodes + 16 * g.nelem
     elif a.kernel == "filter":
@@ -127,7 +128,7 @@ def main(argv=None):
                           "true_rel_res": info.true_rel_res}))
         return
     print(json.dumps({"kernel": a.kernel, "variant": a.variant if a.kernel != "matvec32" else a.variant32,
-                      "mode": a.mode, "nel": nel, "ms": t * 1e3, "algorithmic_bytes": int(nbytes),
+                      "mode": a.mode, "dot": a.dot, "nel": nel, "ms": t * 1e3, "algorithmic_bytes": int(nbytes),
                       "GB_s": nbytes / t / 1e9}))
 
 

@@ -92,7 +92,7 @@ def test_autotuner_variants_are_the_ones_the_library_accepts():
                 if rc:
                     assert rc == A.ERR_ARG, (which, v, rc)
     finally:
-        assert L.pyto_tune(0, 2) == 0 and L.pyto_tune(1, 16) == 0  # library defaults
+        assert L.pyto_tune(0, 2) == 0 and L.pyto_tune(1, 18) == 0  # library defaults
 
 
 @pytest.mark.parametrize("tag,k,h", [("unit", 1.0, (1.0, 1.0, 1.0)), ("box", 50.0, (1.0, 0.5, 2.0))])

@@ -73,13 +73,14 @@ def test_matvec_tile_variants(variant, nel):
             assert np.abs(y.cpu().numpy() - yref).max() <= 1e-13 * np.abs(yref).max()
             assert abs(dot.item() - uu @ yref) <= 1e-12 * abs(uu @ yref)
     finally:
-        A.call("pyto_tune", 0, 2)
+        A.call("pyto_tune", 0, A.MV64_DEFAULT)
 
 
 @pytest.mark.parametrize("nel", [(1, 1, 1), (33, 9, 17), (7, 20, 5), (70, 11, 30), (62, 14, 3), (96, 48, 40)])
 @pytest.mark.parametrize("f32", [False, True])
 def test_matvec_chunked_equals_tile_kernel(nel, f32):
-    """The chunk-staged kernels (variants 8-17; 12-17 with two element rows per thread, 15-17 packed FP32x2)
+    """The chunk-staged kernels (variants 8-19; 12-19 with two element rows per thread, 15-19 packed FP32x2,
+    18-19 with the element core specialised to the cube / box structure of K^)
     perform the tile kernel's arithmetic in the
     same order (up to the compiler's FMA contraction): equal results to a few ulps in every
     mask mode, with and without the fused dot product, and run to run bitwise; a u that
@@ -93,7 +94,7 @@ def test_matvec_chunked_equals_tile_kernel(nel, f32):
     s = _dev(rng.uniform(0.01, 1.0, m["num_elems"])).to(dt)
     ubuf = _dev(rng.normal(size=3 * m["num_nodes"] + 1)).to(dt)
     which, mv = (1, g.matvec_f32) if f32 else (0, g.matvec)
-    variants = (8, 9, 10, 11, 12, 13, 14, 15, 16, 17) if f32 else (8, 9, 10)
+    variants = (8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18, 19) if f32 else (8, 9, 10)
     try:
         for u in (ubuf[:-1], ubuf[1:]):
             for mode in (0, 1, 2, 3):
@@ -112,8 +113,8 @@ def test_matvec_chunked_equals_tile_kernel(nel, f32):
                     assert abs(d1.item() - d0.item()) <= (1e-5 if f32 else 1e-13) * abs(d0.item()), (v, mode)
                     assert torch.equal(y1, mv(s, u, mode=mode)), (v, mode)
     finally:
-        A.call("pyto_tune", 0, 2)
-        A.call("pyto_tune", 1, 8)
+        A.call("pyto_tune", 0, A.MV64_DEFAULT)
+        A.call("pyto_tune", 1, A.MV32_DEFAULT)
 
 
 def test_matvec_bitwise_deterministic():
@@ -317,15 +318,17 @@ def test_boundary_lists_follow_fixed_dofs():
     assert defl.bel_list.numel() == want
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17])
-def test_matvec_f32_matches_fp64(variant):
+@pytest.mark.parametrize("h", [(1.0, 1.0, 1.0), (1.0, 0.5, 2.0)])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 8, 9, 10, 11, 12, 13, 14, 15, 16, 17, 18, 19])
+def test_matvec_f32_matches_fp64(variant, h):
     """FP32 operator: relative error of K(s)u against the FP64 operator at FP32 rounding
-    (variants 4, 5: tensor-core contraction with BF16 split operands, ~2^-16)."""
+    (variants 4, 5: tensor-core contraction with BF16 split operands, ~2^-16).  A cube
+    element takes the cube form of variants 18, 19, the 1 x 0.5 x 2 box their box form."""
     from pyto_b200 import _capi as A
     nel = (33, 9, 17)
-    m = O.grid_mesh(*nel)
+    m = O.grid_mesh(*nel, h)
     _, fixed = O.cantilever_bc(m)
-    g = _grid(nel, fixed=fixed)
+    g = _grid(nel, h, fixed=fixed)
     rng = np.random.default_rng(7)
     s64 = _dev(rng.uniform(1e-3, 1.0, m["num_elems"]))
     u64 = _dev(rng.normal(size=3 * m["num_nodes"]))
@@ -334,7 +337,7 @@ def test_matvec_f32_matches_fp64(variant):
     try:
         y32 = g.matvec_f32(s32, u32)
     finally:
-        A.call("pyto_tune", 1, 8)
+        A.call("pyto_tune", 1, A.MV32_DEFAULT)
     assert A.lib().pyto_tensor_core_status(1) == 0
     y64 = g.matvec(s32.double(), u32.double())
     err = (y32.double() - y64).abs().max().item()
@@ -360,7 +363,7 @@ def test_mixed_solve_with_tensor_core_operator():
     try:
         u1, i1 = g.dpcg_mixed(s, b, defl, rtol=1e-9)
     finally:
-        A.call("pyto_tune", 1, 8)
+        A.call("pyto_tune", 1, A.MV32_DEFAULT)
     assert A.lib().pyto_tensor_core_status(1) == 0
     assert i0.converged and i1.converged and i1.true_rel_res <= 1e-9, i1
     _, C0 = g.energy(u0, s=s)
