@@ -113,7 +113,7 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def build(device, nel, groups, modes):
+def build(device, nel, groups, modes, agg=0, leaf=8):
     import torch
     from pyto_b200 import _capi as A
     from pyto_b200.deflation import DeflationSolver
@@ -126,12 +126,27 @@ def build(device, nel, groups, modes):
     grid = HexGrid(nel, (1.0, 1.0, 1.0), 1.0, 0.3, device=device).set_fixed_dofs(fixed)
     x = grid.tensor(uniform_density(nel, 0.01, 1.0, seed=0))
     rho = grid.filter(2.0, A.FILTER_DENSITY, x)
-    ds = DeflationSolver(modes=modes, shift=1e-14, shift_relative=True)
-    ds.create_deflation_groups(mesh, groups)
+    ds = DeflationSolver(modes=modes, shift=1e-14, shift_relative=True, nd_leaf=leaf)
+    if agg > 0:  # element-box aggregates (nested-dissection coarse solver where the dense one cannot hold them)
+        ds.create_deflation_groups_box(mesh, (agg, agg, agg), modes=modes)
+    else:
+        ds.create_deflation_groups(mesh, groups)
     defl = ds.device_deflation(grid)
     F = grid.tensor(f)
     torch.cuda.synchronize(device)
     return dict(mesh=mesh, grid=grid, rho=rho, F=F, f=f, defl=defl, ds=ds, x=x)
+
+
+def coarse_space_desc(P, args):
+    d, ds = P["defl"], P["ds"]
+    what = (f"{ds.ws_nGroups} node-box groups x {args.modes} rigid modes (reference box partition)" if args.agg <= 0
+            else f"{args.agg}x{args.agg}x{args.agg}-element aggregates ({ds.ws_nGroups} groups) x {args.modes} "
+                 + ("translations" if args.modes == 3 else "rigid modes"))
+    if d.coarse == "nd":
+        i = d.nd_info
+        return (f"{what}, {d.nc} coarse unknowns, FP64 nested-dissection factorisation ({i['nodes']} fronts, "
+                f"depth {i['depth']}, largest {i['max_front']}, {i['factor_flops'] / 1e9:.1f} GFLOP)")
+    return f"{what}, dense FP64 coarse inverse"
 
 
 def solve_step(P, rho=None, form="mixed"):
@@ -288,6 +303,10 @@ def main():
     ap.add_argument("--impl", default="pyto", choices=["pyto", "reference"])
     ap.add_argument("--groups", type=int, default=432, help="deflation groups (reference box partition)")
     ap.add_argument("--modes", type=int, default=6)
+    ap.add_argument("--agg", type=int, default=0,
+                    help="deflation by agg^3-element box aggregates instead of the reference partition "
+                         "(4 with --modes 3: the 4x4x4-aggregate, 3-translation coarse space)")
+    ap.add_argument("--leaf", type=int, default=8, help="nested-dissection leaf size (groups)")
     ap.add_argument("--nel", default=None, help="override grid, e.g. 96,48,48 (not a bench line)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--form", default="mixed", choices=["mixed", "fp64"],
@@ -318,7 +337,7 @@ def main():
     from pyto_b200 import _capi as A
 
     nel = tuple(int(v) for v in args.nel.split(",")) if args.nel else NEL
-    P = build(device, nel, args.groups, args.modes)
+    P = build(device, nel, args.groups, args.modes, args.agg, args.leaf)
     P["delta"] = args.delta
     g = P["grid"]
     other = "fp64" if args.form == "mixed" else "mixed"
@@ -441,8 +460,7 @@ def main():
                        "other_form_clocks": clk_other.summary(),
                        "compliance": c_main, "compliance_rel_diff_vs_other_form": abs(c_main - c_other) / abs(c_other),
                        "other_form_iterations": info_other.iters,
-                       "coarse_space": f"{P['ds'].ws_nGroups} node-box groups x {args.modes} rigid modes "
-                                       f"(reference box partition), dense FP64 coarse inverse",
+                       "coarse_space": coarse_space_desc(P, args),
                        "iterations": iters, "refinement_cycles": cycles, "true_rel_res": trr, "l2": "inputs larger than L2 (~0.6 GB moved per "
                                                                           "iteration)",
                        "parallelism": f"replicas x{world}", **extra},

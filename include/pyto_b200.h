@@ -88,6 +88,9 @@ typedef struct pyto_solve_status {
   double true_rel_res;  /* ||b - K u||_2 / ||b||_2 recomputed in FP64 at exit */
 } pyto_solve_status_t;
 
+/* Sparse coarse solver of a deflation space (nested dissection; see pyto_coarse_nd_plan). */
+typedef struct pyto_coarse_nd pyto_coarse_nd_t;
+
 /* Deflation space: node groups with rigid-body modes about the group centre.
  * modes = 6: columns [tx,ty,tz,rx,ry,rz] per group (src/deflation.py:386-457);
  * modes = 3: translations only.  All pointers are device pointers. */
@@ -120,6 +123,11 @@ typedef struct pyto_deflation {
    * the mask): bits 0-7 = corner k of the entry's element lies in the entry's group,
    * bit 8 = the element has a fixed DOF.  Rebuilt with the lists. */
   const uint16_t* bel_meta;    /* [bel_count] */
+  /* Optional sparse coarse solver (NULL: the dense coarse_inv).  When set (a plan bound
+   * to its device buffer), pyto_dpcg_setup assembles W_f^T K_ff W_f block-sparse and
+   * factors it by nested dissection, and pyto_dpcg_solve / pyto_dpcg_mixed_solve apply
+   * that factorisation; coarse_inv may then be NULL.  Needs the boundary lists. */
+  pyto_coarse_nd_t* coarse_nd;
 } pyto_deflation_t;
 
 /* ---- version / workspace ------------------------------------------------- */
@@ -150,7 +158,7 @@ long long pyto_launch_count(void);
                                   CUDA graphs; 0: launched one kernel at a time */
 int pyto_tune(int kernel, int variant);
 /* Bytes of workspace for a call of the given kind on this operator (for
- * PYTO_WS_DPCG: any coarse size up to 24576). */
+ * PYTO_WS_DPCG: up to 65536 groups; coarse sizes up to 24576 with the dense coarse inverse). */
 size_t pyto_workspace_bytes(const pyto_operator_t* op, int kind);
 
 /* ---- element matrices and operator set-up (host only, no GPU work) ------- */
@@ -290,6 +298,41 @@ int pyto_coarse_prolong(const pyto_operator_t* op, const pyto_deflation_t* defl,
 int pyto_cg_update(const pyto_operator_t* op, const double* winv, const uint8_t* flags, double alpha,
                    const double* p, const double* q, double* x, double* r, double* z, double* dots, void* ws,
                    size_t ws_bytes, void* stream);
+
+/* ---- sparse coarse solver: nested dissection on a box grid of groups ----------------- */
+/* The reference densifies W^T K W and solves it with a direct solver per iteration
+ * (src/deflation.py:517-521, 577); a dense coarse matrix limits the coarse space to a few
+ * thousand unknowns (82,944 for 4x4x4-element aggregates with 3 translations on a
+ * 192x96x96 grid would be 55 GB).  For groups on a regular gx x gy x gz box grid (group
+ * id = ix + gx (iy + gy iz), every neighbour within one box in each direction: the
+ * element-box aggregates of create_deflation_groups_box and the reference's node-box
+ * partition of a grid mesh), W^T K W is block-sparse with at most 27 neighbour blocks per
+ * group.  It is factored by nested dissection on that grid: boxes of groups are split
+ * recursively by separator planes (leaves: boxes of at most `leaf` groups); each tree node
+ * holds a dense frontal matrix over its own unknowns and its boundary (the groups around
+ * its box, all in ancestor separators); the node's own unknowns are eliminated by a
+ * blocked Gauss-Jordan sweep, and the Schur complement on its boundary is added into the
+ * parent's front.  A solve runs the tree up (frontal right-hand sides) and down (GEMVs
+ * with the stored -A_ss^-1 and A_bs A_ss^-1).  All sums are in a fixed order: the
+ * factorisation and the solves are bitwise reproducible.  No reference counterpart
+ * beyond the direct coarse solve it replaces. */
+/* Host-only planning (no GPU work).  nbr_ptr / nbr_list: host copies of the deflation's
+ * neighbour lists (pyto_deflation_t.nbr_ptr / nbr_list).  NULL on invalid arguments or a
+ * neighbour list that does not match the box grid (pyto_last_error says which). */
+pyto_coarse_nd_t* pyto_coarse_nd_plan(int32_t gx, int32_t gy, int32_t gz, int32_t modes, int32_t leaf,
+                                      const int32_t* nbr_ptr, const int32_t* nbr_list);
+/* Device bytes of the plan (index tables, the block-sparse coarse matrix, frontal matrices,
+ * their sweep scratch).  info (may be NULL) receives [0] tree nodes, [1] tree depth,
+ * [2] largest front (unknowns), [3] factorisation flops, [4] bytes read per solve. */
+size_t pyto_coarse_nd_bytes(const pyto_coarse_nd_t* plan, double* info);
+/* Bind the plan to a caller-owned device buffer of pyto_coarse_nd_bytes bytes (256-byte
+ * aligned) and copy the index tables into it (stream-ordered; the plan's host tables must
+ * stay alive until the copy has run: keep the plan until the stream is synchronised). */
+int pyto_coarse_nd_bind(pyto_coarse_nd_t* plan, void* dev_buf, size_t bytes, void* stream);
+/* mu[nc] = (W_f^T K_ff W_f + shift I)^-1 v with the factorisation of the last
+ * pyto_dpcg_setup (nc = groups x modes, both device vectors). */
+int pyto_coarse_nd_solve(const pyto_coarse_nd_t* plan, const double* v, double* mu, void* stream);
+void pyto_coarse_nd_free(pyto_coarse_nd_t* plan);
 
 /* ---- batched solves in one CUDA graph ---------------------------------------------- */
 /* One independent deflated PCG problem of a batch (no reference counterpart: PyTO

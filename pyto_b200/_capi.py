@@ -62,7 +62,7 @@ class Deflation(C.Structure):
                 ("shift", C.c_double), ("shift_relative", C.c_int32), ("max_group_nodes", C.c_int32),
                 ("group_box", C.c_void_p), ("nbr_ptr", C.c_void_p), ("nbr_list", C.c_void_p), ("max_nbr", C.c_int32),
                 ("bel_count", C.c_int32), ("bel_ptr", C.c_void_p), ("bel_list", C.c_void_p),
-                ("bel_meta", C.c_void_p)]
+                ("bel_meta", C.c_void_p), ("coarse_nd", C.c_void_p)]
 
 
 class BatchItem(C.Structure):
@@ -82,6 +82,11 @@ _OP = C.POINTER(Operator)
 _TH = C.POINTER(Thermal)
 SIGNATURES = {
     "pyto_version": (C.c_int, []),
+    "pyto_coarse_nd_plan": (C.c_void_p, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P, _P]),
+    "pyto_coarse_nd_bytes": (C.c_size_t, [_P, _P]),
+    "pyto_coarse_nd_bind": (C.c_int, [_P, _P, C.c_size_t, _P]),
+    "pyto_coarse_nd_solve": (C.c_int, [_P, _P, _P, _P]),
+    "pyto_coarse_nd_free": (None, [_P]),
     "pyto_struct_size": (C.c_size_t, [C.c_int]),
     "pyto_last_error": (C.c_char_p, []),
     "pyto_launch_count": (C.c_longlong, []),
@@ -170,6 +175,12 @@ def call(fn: str, *args, allow=(OK,)) -> int:
                 err = PytoError(fn, rc, detail.decode(errors="replace"))
         raise err
     return rc
+
+
+def last_error() -> str:
+    """The library's description of the last failure of this thread ("" if none)."""
+    d = lib().pyto_last_error()
+    return d.decode(errors="replace") if d else ""
 
 
 def ptr(t):

@@ -21,11 +21,12 @@
 #include <algorithm>
 #include <vector>
 
+#include "coarse_nd.cuh"
 #include "krylov.cuh"
+#include "sweep.cuh"
 
 namespace pyto {
 
-constexpr int kSweepB = 64;
 // boundary-list chunks: kRkChunk list entries per CTA of the K-restriction and
 // of the coarse assembly
 constexpr int kRkThreads = 128;
@@ -278,7 +279,9 @@ __device__ __forceinline__ double mode_hat_from_base(const double* B, int stride
 // Only the blocks E[G, H] with H <= G are formed (E is symmetric; k_mirror_upper
 // copies them into E[H, G]), and the mode loops are unrolled (M = dp.modes).
 constexpr int kCrThreads = 128;
-template <int M>
+// BSR: E is block-sparse in the neighbour-slot order (block (G, nbr_list[nbr_ptr[G] + j])
+// at slot nbr_ptr[G] + j, M x M row-major): the nested-dissection coarse solver.
+template <int M, bool BSR = false>
 __global__ void __launch_bounds__(kCrThreads) k_coarse_rows2(GridDims g, KHat kh, DeflP dp,
                                                              const double* __restrict__ s,
                                                              const uint8_t* __restrict__ mask,
@@ -451,7 +454,10 @@ __global__ void __launch_bounds__(kCrThreads) k_coarse_rows2(GridDims g, KHat kh
   for (int t = threadIdx.x; t < nnb * M * M; t += blockDim.x) {
     const int slot = t / (M * M), a = (t / M) % M, b = t % M;
     const unsigned long long v = acc[slot * 36 + a * 6 + b];
-    if (v != 0ull) atomicAdd(&E[((long long)G * M + a) * dp.nc + (long long)snb[slot] * M + b], v);
+    if (v != 0ull) {
+      if (BSR) atomicAdd(&E[((long long)(nb0 + slot) * M + a) * M + b], v);
+      else atomicAdd(&E[((long long)G * M + a) * dp.nc + (long long)snb[slot] * M + b], v);
+    }
   }
 }
 
@@ -545,91 +551,9 @@ __global__ void k_coarse_finish(long long nc, double* E, double shift, const dou
 // blocked sweep inversion: after all pivot blocks A = -E^-1
 //   P = A_KK^-1, U = P A_K:, A_ij -= A_iK U_Kj, A_Kj = U_Kj, A_iK = U_Ki^T, A_KK = -P
 // ---------------------------------------------------------------------------
-// Element k of a 4-vector held in registers, by selects (a dynamic index would put
-// the array in local memory).
-__device__ __forceinline__ double pick4(double v0, double v1, double v2, double v3, int k) {
-  double r = v0;
-  r = (k == 1) ? v1 : r;
-  r = (k == 2) ? v2 : r;
-  r = (k == 3) ? v3 : r;
-  return r;
-}
-
-// In-place sweep of the symmetric 64 x 64 block held by 256 threads (thread (ty, tx)
-// owns rows ty + 16a, columns tx + 16b), pivots 0..63 in order:
-//   M_pp -> -1/M_pp,  M_pj -> M_pj/M_pp,  M_ip -> M_ip/M_pp,  M_ij -= M_ip M_pj / M_pp,
-// leaving -M^-1.  Padding pivots (identity rows/columns beyond bk) are decoupled, so they
-// are swept with the rest.  The owners of row p publish it (raw and divided by the
-// pivot) in a double-buffered shared row, so each pivot costs one barrier, and the
-// pivot loop stays rolled: the code is executed 64 times from the instruction cache
-// instead of once per pivot from L2.  The block stays bitwise symmetric (M_ip is read
-// as M_pi).  sm: >= 2 * 130 doubles.
-__device__ __forceinline__ void sweep_pivot_rolled(double (&R)[4][4], double* sm) {
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-#pragma unroll 1
-  for (int p = 0; p < 64; ++p) {
-    double* row = sm + (p & 1) * 130;  // [0, 64): M_p:, [64, 128): M_p: / M_pp, 128: 1 / M_pp
-    const int pr = p & 15, pa = p >> 4;
-    if (ty == pr) {  // half a warp: the owners of row p
-      double v[4];
-#pragma unroll
-      for (int b = 0; b < 4; ++b) v[b] = pick4(R[0][b], R[1][b], R[2][b], R[3][b], pa);
-      const unsigned half = 0xFFFFu << (16 * (ty & 1));
-      const double mpp = __shfl_sync(half, pick4(v[0], v[1], v[2], v[3], pa), pr, 16);
-      const double ip = 1.0 / mpp;
-#pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        row[tx + 16 * b] = v[b];
-        row[64 + tx + 16 * b] = v[b] * ip;
-      }
-      if (tx == 0) row[128] = ip;
-    }
-    __syncthreads();
-    double mip[4], rcj[4];
-#pragma unroll
-    for (int a = 0; a < 4; ++a) mip[a] = row[ty + 16 * a];
-#pragma unroll
-    for (int b = 0; b < 4; ++b) rcj[b] = row[64 + tx + 16 * b];
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int b = 0; b < 4; ++b) R[a][b] = fma(-mip[a], rcj[b], R[a][b]);
-    if (ty == pr) {  // row p: M_pj / M_pp
-#pragma unroll
-      for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b)
-          if (a == pa) R[a][b] = rcj[b];
-    }
-    if (tx == pr) {  // column p: M_ip / M_pp (= M_pi / M_pp), and the pivot itself
-      const double ip = row[128];
-#pragma unroll
-      for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b)
-          if (b == pa) R[a][b] = (ty + 16 * a == p) ? -ip : mip[a] * ip;
-    }
-  }
-  __syncthreads();  // the caller may reuse sm
-}
-
 __global__ void __launch_bounds__(256) k_sweep_pivot(long long n, int k0, int bk, const double* __restrict__ A,
                                                      double* __restrict__ P) {
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  double R[4][4];
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const int i = ty + 16 * a, j = tx + 16 * b;
-      R[a][b] = (i < bk && j < bk) ? A[(k0 + i) * n + (k0 + j)] : (i == j ? 1.0 : 0.0);
-    }
-  __shared__ double sm[2 * 130];
-  sweep_pivot_rolled(R, sm);
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) P[(ty + 16 * a) * kSweepB + tx + 16 * b] = -R[a][b];  // P = A_KK^-1
+  sweep_pivot_block(n, k0, bk, A, P);
 }
 
 // Rp = A_K: (copy), U = P Rp   (16 columns per block).  Only the lower tiles
@@ -638,27 +562,7 @@ __global__ void __launch_bounds__(256) k_sweep_pivot(long long n, int k0, int bk
 __global__ void __launch_bounds__(256) k_sweep_panel(long long n, int k0, int bk, const double* __restrict__ A,
                                                      const double* __restrict__ P, double* __restrict__ Rp,
                                                      double* __restrict__ U) {
-  __shared__ double sP[kSweepB][kSweepB];
-  __shared__ double sR[kSweepB][17];
-  for (int t = threadIdx.x; t < kSweepB * kSweepB; t += blockDim.x) sP[t / kSweepB][t % kSweepB] = P[t];
-  const long long j0 = (long long)blockIdx.x * 16;
-  for (int t = threadIdx.x; t < kSweepB * 16; t += blockDim.x) {
-    const int i = t / 16, jj = t % 16;
-    const long long j = j0 + jj;
-    double v = 0.0;
-    if (i < bk && j < n) v = (j < k0 + kSweepB) ? A[(k0 + i) * n + j] : A[j * n + (k0 + i)];
-    sR[i][jj] = v;
-    if (i < bk && j < n) Rp[i * n + j] = v;
-  }
-  __syncthreads();
-  for (int t = threadIdx.x; t < kSweepB * 16; t += blockDim.x) {
-    const int i = t / 16, jj = t % 16;
-    const long long j = j0 + jj;
-    if (i >= bk || j >= n) continue;
-    double acc = 0.0;
-    for (int k = 0; k < bk; ++k) acc = fma(sP[i][k], sR[k][jj], acc);
-    U[i * n + j] = acc;
-  }
+  sweep_panel_cols(n, k0, bk, A, P, Rp, U, (long long)blockIdx.x * 16);
 }
 
 // tile update of the lower 64x64 tiles (ti >= tj, one CTA each, 1-D grid),
@@ -668,9 +572,6 @@ __global__ void __launch_bounds__(256) k_sweep_panel(long long n, int k0, int bk
 __global__ void __launch_bounds__(256, 3) k_sweep_update(long long n, int k0, int bk, double* __restrict__ A,
                                                       const double* __restrict__ P, const double* __restrict__ Rp,
                                                       const double* __restrict__ U, int k1, double* __restrict__ Pn) {
-  __shared__ double sLU[2][32][65];  // [0]: A_iK for the tile rows (Rp[k][i]); [1]: U_Kj for the tile cols
-  double(&sL)[32][65] = sLU[0];
-  double(&sU)[32][65] = sLU[1];
   const long long ntiles = gridDim.x;
   long long b = blockIdx.x;
   if (k1 >= 0) {  // rotate the numbering so that block 0 is tile (k1/64, k1/64)
@@ -681,77 +582,7 @@ __global__ void __launch_bounds__(256, 3) k_sweep_update(long long n, int k0, in
   while (ti * (ti + 1) / 2 > b) --ti;
   while ((ti + 1) * (ti + 2) / 2 <= b) ++ti;
   const long long tj = b - ti * (ti + 1) / 2;
-  const long long i0 = ti * 64, j0 = tj * 64;
-  const bool rowK = (i0 == k0), colK = (j0 == k0);
-  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-  if (rowK || colK) {
-    for (int t = threadIdx.x; t < 64 * 64; t += blockDim.x) {
-      const int ii = t / 64, jj = t % 64;
-      const long long i = i0 + ii, j = j0 + jj;
-      if (i >= n || j >= n) continue;
-      double v;
-      if (rowK && colK) v = (ii < bk && jj < bk) ? -P[ii * kSweepB + jj] : A[i * n + j];
-      else if (rowK) v = (ii < bk) ? U[ii * n + j] : A[i * n + j];
-      else v = (jj < bk) ? U[jj * n + i] : A[i * n + j];
-      A[i * n + j] = v;
-    }
-    return;
-  }
-  double acc[4][4];
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-  for (int kc = 0; kc < bk; kc += 32) {
-    __syncthreads();
-    for (int t = threadIdx.x; t < 32 * 64; t += blockDim.x) {
-      const int k = t / 64, c = t % 64;
-      const bool kin = kc + k < bk;
-      sL[k][c] = (kin && i0 + c < n) ? Rp[(kc + k) * n + i0 + c] : 0.0;
-      sU[k][c] = (kin && j0 + c < n) ? U[(kc + k) * n + j0 + c] : 0.0;
-    }
-    __syncthreads();
-#pragma unroll 4
-    for (int k = 0; k < 32; ++k) {
-      double l[4], u[4];
-#pragma unroll
-      for (int a = 0; a < 4; ++a) l[a] = sL[k][ty + 16 * a];
-#pragma unroll
-      for (int b = 0; b < 4; ++b) u[b] = sU[k][tx + 16 * b];
-#pragma unroll
-      for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = fma(l[a], u[b], acc[a][b]);
-    }
-  }
-  const bool pivot_next = k1 >= 0 && i0 == k1 && j0 == k1;
-  const int bk1 = (int)std::min<long long>(kSweepB, n - k1);
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const long long i = i0 + ty + 16 * a, j = j0 + tx + 16 * b;
-      if (i < n && j < n) {
-        const double v = A[i * n + j] - acc[a][b];
-        A[i * n + j] = v;
-        acc[a][b] = v;
-      }
-    }
-  if (!pivot_next) return;
-  // the next pivot block, as k_sweep_pivot would load it (identity padding)
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const int i = ty + 16 * a, j = tx + 16 * b;
-      if (!(i < bk1 && j < bk1)) acc[a][b] = (i == j) ? 1.0 : 0.0;
-    }
-  __syncthreads();
-  sweep_pivot_rolled(acc, &sLU[0][0][0]);  // sL, sU are free now
-#pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) Pn[(ty + 16 * a) * kSweepB + tx + 16 * b] = -acc[a][b];
+  sweep_update_tile(n, k0, bk, A, P, Rp, U, ti, tj, k1, Pn);
 }
 
 // E^-1 = -A: negate the lower tiles (diagonal tiles in full) and mirror them
@@ -1469,7 +1300,9 @@ struct DpcgWs {
   float *r32, *p32, *q32, *z32, *x32, *b32, *s32;
 };
 
-constexpr long long kMaxCoarse = 24576;  // coarse vector staged in shared memory (192 KB)
+constexpr long long kMaxCoarse = 24576;  // dense coarse path: coarse vector staged in shared memory (192 KB)
+constexpr long long kMaxGroups = 65536;  // groups of a deflation space (the per-group workspace tables)
+constexpr long long kMaxNdCoarse = 6 * kMaxGroups;  // coarse unknowns of the nested-dissection path
 constexpr double kReliableDelta = 1e-2;  // FP64 residual replacement each time ||r|| drops 100-fold
 constexpr int kReliableSegment = 100;    // and at least every this many iterations
 constexpr int kReliablePoll = 20;        // replacement triggers tested at least this often
@@ -1490,15 +1323,16 @@ static DpcgWs carve_dpcg(const pyto_operator_t* op, long long nc, void* ws, size
   W.w = cv.take<double>(g.nnodes);
   W.fl = cv.take<uint8_t>(g.nnodes);
   W.rpart = cv.take<double>((size_t)6 * kRestrictMaxBlocks);
-  W.cptr = cv.take<int32_t>((size_t)kMaxCoarse + 1);
+  W.cptr = cv.take<int32_t>((size_t)kMaxGroups + 1);
   W.cgrp = cv.take<int32_t>((size_t)kRkMaxChunks);
-  W.gcount = cv.take<unsigned>((size_t)kMaxCoarse);
-  W.gexp = cv.take<int>((size_t)kMaxCoarse);
+  W.gcount = cv.take<unsigned>((size_t)kMaxGroups);
+  W.gexp = cv.take<int>((size_t)kMaxGroups);
   W.cv = cv.take<double>(2 * (nc > 0 ? nc : 1));  // k_restrict_K writes 6 slots per group
   W.mu = cv.take<double>(nc > 0 ? nc : 1);
+  const long long ncd = std::min(nc > 0 ? nc : 1, kMaxCoarse);  // dense sweep scratch
   W.P = cv.take<double>(2 * kSweepB * kSweepB);
-  W.Rp = cv.take<double>(kSweepB * (nc > 0 ? nc : 1));
-  W.U = cv.take<double>(kSweepB * (nc > 0 ? nc : 1));
+  W.Rp = cv.take<double>(kSweepB * ncd);
+  W.U = cv.take<double>(kSweepB * ncd);
   if (mixed) {
     W.r32 = cv.take<float>(3 * g.nnodes);
     W.p32 = cv.take<float>(3 * g.nnodes);
@@ -1514,7 +1348,7 @@ static DpcgWs carve_dpcg(const pyto_operator_t* op, long long nc, void* ws, size
 
 size_t dpcg_workspace_bytes(const pyto_operator_t* op, bool mixed) {
   size_t need = 0;
-  carve_dpcg(op, kMaxCoarse, nullptr, 0, &need, mixed);
+  carve_dpcg(op, kMaxNdCoarse, nullptr, 0, &need, mixed);
   return need;
 }
 
@@ -1531,11 +1365,24 @@ static DeflP make_deflp(const pyto_operator_t* op, const pyto_deflation_t* d) {
 
 static bool defl_ok(const pyto_deflation_t* d) {
   if (!(d && d->ngroups > 0 && (d->modes == 3 || d->modes == 6) && d->node_group && d->group_ptr &&
-        d->group_nodes && d->group_center && d->coarse_inv && d->group_box && d->nbr_ptr && d->nbr_list &&
+        d->group_nodes && d->group_center && (d->coarse_inv || d->coarse_nd) && d->group_box && d->nbr_ptr &&
+        d->nbr_list &&
         d->max_group_nodes > 0 && d->max_nbr > 0 && d->max_nbr <= 128))
     return false;
   const long long nch = (d->max_group_nodes + kRestrictChunk - 1) / kRestrictChunk;
-  return (long long)d->ngroups * nch <= kRestrictMaxBlocks;
+  return (long long)d->ngroups * nch <= kRestrictMaxBlocks && d->ngroups <= kMaxGroups;
+}
+
+// v[g*modes + a] = sum over chunks c of part[(g*nch + c)*6 + a], chunks in order
+__global__ void k_restrict_sum(long long nc, int modes, int nch, const double* __restrict__ part,
+                               double* __restrict__ v) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nc;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long gg = i / modes, a = i - gg * modes;
+    double t = 0.0;
+    for (int c = 0; c < nch; ++c) t += part[(gg * nch + c) * 6 + a];
+    v[i] = t;
+  }
 }
 
 // mu = Einv W_f^T y
@@ -1546,6 +1393,12 @@ static int coarse_solve(const GridDims& g, const DeflP& dp, const pyto_deflation
   k_restrict<T><<<dp.ngroups * nch, 256, 0, st>>>(g, dp, d->group_ptr, d->group_nodes, d->group_center, W.fl, y,
                                                   nch, W.rpart);
   PYTO_COUNT(1);
+  if (d->coarse_nd) {
+    k_restrict_sum<<<(int)std::min<long long>((dp.nc + 255) / 256, 4 * kNumSMs), 256, 0, st>>>(dp.nc, dp.modes,
+                                                                                               nch, W.rpart, W.cv);
+    PYTO_COUNT(1);
+    return nd_solve(d->coarse_nd, W.cv, W.mu, S, st);
+  }
   const size_t shm = (size_t)dp.nc * sizeof(double);
   const int nb = (int)std::min<long long>((dp.nc + 7) / 8, 4 * kNumSMs);
   k_coarse_gemv<<<nb, 256, shm, st>>>(dp.nc, dp.modes, nch, d->coarse_inv, W.rpart, W.mu, S);
@@ -1564,7 +1417,10 @@ static int coarse_update_K(const pyto_operator_t* op, const GridDims& g, const D
                                                   d->group_center, d->bel_ptr, d->bel_list, W.cptr, W.cgrp, z,
                                                   W.rpart, W.gcount, W.cv, S, d->bel_meta);
   PYTO_COUNT(1);
-  if ((dp.nc & 1) == 0) {
+  if (d->coarse_nd) {
+    const int rc = nd_solve(d->coarse_nd, W.cv, W.mu, first ? nullptr : S, st);
+    if (rc) return rc;
+  } else if ((dp.nc & 1) == 0) {
     k_gemv_rows<<<(int)((dp.nc + 3) / 4), 128, 0, st>>>(dp.nc, d->coarse_inv, W.cv, W.mu, first ? nullptr : S);
   } else {
     const size_t shm = (size_t)dp.nc * sizeof(double);
@@ -1613,6 +1469,15 @@ static int chunk_setup(const pyto_deflation_t* d, const DpcgWs& W, cudaStream_t 
   return rc ? rc : nch;
 }
 
+// W_f^T K z from the boundary lists when they are short; with more list entries than half
+// the elements (fine aggregates: most elements straddle groups, each in several lists) a
+// full matvec K z and a node-wise restriction move fewer bytes.  The lists are still used
+// by the coarse assembly.
+static bool restrict_from_lists(const pyto_deflation_t* d, const GridDims& g, int nchunks) {
+  if (nchunks <= 0) return false;
+  return d->bel_count <= 0 || 2LL * d->bel_count <= g.nelem;
+}
+
 static int gemv_smem_ok(long long nc) {
   static PerDevice attr;
   if (attr.needed()) {
@@ -1637,18 +1502,23 @@ static int coarse_assemble_launch(const pyto_operator_t* op, const double* s, co
                                   const pyto_deflation_t* defl, const DpcgWs& W, int nchunks, cudaStream_t st) {
   const DeflP dp = make_deflp(op, defl);
   const GridDims g = make_dims(op);
-  double* E = defl->coarse_inv;
+  const bool nd = defl->coarse_nd != nullptr;
+  if (nd && nchunks <= 0) return PYTO_ERR_ARG;  // the block-sparse assembly needs the boundary lists
+  double* E = nd ? nd_matrix(defl->coarse_nd) : defl->coarse_inv;
+  if (!E) return PYTO_ERR_ARG;
   const long long n = dp.nc;
-  PYTO_CUDA(cudaMemsetAsync(E, 0, (size_t)n * n * sizeof(double), st));
+  PYTO_CUDA(cudaMemsetAsync(E, 0, nd ? (size_t)nd_matrix_bytes(defl->coarse_nd) : (size_t)n * n * sizeof(double),
+                            st));
   const size_t shm = (size_t)defl->max_nbr * 36 * sizeof(double);
   if (nchunks > 0) {
     const size_t shm2 = shm + 64 * kCrThreads * sizeof(double);
     static PerDevice attr;
     if (attr.needed()) {
-      PYTO_CUDA(cudaFuncSetAttribute(k_coarse_rows2<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(64 * kCrThreads * sizeof(double) + 128 * 36 * sizeof(double))));
-      PYTO_CUDA(cudaFuncSetAttribute(k_coarse_rows2<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(64 * kCrThreads * sizeof(double) + 128 * 36 * sizeof(double))));
+      const int need = (int)(64 * kCrThreads * sizeof(double) + 128 * 36 * sizeof(double));
+      PYTO_CUDA(cudaFuncSetAttribute(k_coarse_rows2<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, need));
+      PYTO_CUDA(cudaFuncSetAttribute(k_coarse_rows2<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, need));
+      PYTO_CUDA(cudaFuncSetAttribute(k_coarse_rows2<6, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, need));
+      PYTO_CUDA(cudaFuncSetAttribute(k_coarse_rows2<3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, need));
       attr.done();
     }
     double ke_rows = 0.0;  // max absolute row sum of Ke (>= its spectral norm)
@@ -1661,6 +1531,19 @@ static int coarse_assemble_launch(const pyto_operator_t* op, const double* s, co
                                              defl->bel_list, defl->nbr_ptr, defl->nbr_list, W.gexp);
     PYTO_COUNT(1);
     unsigned long long* Eq = reinterpret_cast<unsigned long long*>(E);
+    if (nd) {  // converted, symmetrised and shifted by nd_factor
+      if (dp.modes == 6)
+        k_coarse_rows2<6, true><<<nchunks, kCrThreads, shm2, st>>>(
+            g, make_khat(op), dp, s, mask, defl->node_group, defl->group_center, defl->bel_ptr, defl->bel_list,
+            W.cptr, W.cgrp, defl->nbr_ptr, defl->nbr_list, W.gexp, Eq);
+      else
+        k_coarse_rows2<3, true><<<nchunks, kCrThreads, shm2, st>>>(
+            g, make_khat(op), dp, s, mask, defl->node_group, defl->group_center, defl->bel_ptr, defl->bel_list,
+            W.cptr, W.cgrp, defl->nbr_ptr, defl->nbr_list, W.gexp, Eq);
+      PYTO_COUNT(1);
+      PYTO_LAUNCH_CHECK();
+      return PYTO_OK;
+    }
     if (dp.modes == 6)
       k_coarse_rows2<6><<<nchunks, kCrThreads, shm2, st>>>(g, make_khat(op), dp, s, mask, defl->node_group,
                                                           defl->group_center, defl->bel_ptr, defl->bel_list, W.cptr,
@@ -1724,14 +1607,18 @@ static int coarse_invert_launch(const pyto_deflation_t* defl, const DpcgWs& W, c
 static int dpcg_setup_launch(const pyto_operator_t* op, const double* s, const uint8_t* mask,
                              const pyto_deflation_t* defl, const DpcgWs& W, int nchunks, cudaStream_t st) {
   const int rc = coarse_assemble_launch(op, s, mask, defl, W, nchunks, st);
-  return rc ? rc : coarse_invert_launch(defl, W, st);
+  if (rc) return rc;
+  if (defl->coarse_nd)
+    return nd_factor(defl->coarse_nd, defl->nbr_ptr, defl->nbr_list, W.gexp, defl->shift, defl->shift_relative,
+                     st);
+  return coarse_invert_launch(defl, W, st);
 }
 
 extern "C" int pyto_dpcg_setup(const pyto_operator_t* op, const double* s, const uint8_t* mask,
                                pyto_deflation_t* defl, void* ws, size_t ws_bytes, void* stream) {
   if (!op || !s || !defl_ok(defl)) return PYTO_ERR_ARG;
   const DeflP dp = make_deflp(op, defl);
-  int rc0 = gemv_smem_ok(dp.nc);
+  int rc0 = gemv_smem_ok(defl->coarse_nd ? 0 : dp.nc);
   if (rc0) return rc0;
   size_t need = 0;
   DpcgWs W = carve_dpcg(op, dp.nc, ws, ws_bytes, &need);
@@ -1849,7 +1736,7 @@ static int dpcg_run(const pyto_operator_t* op, const T* s, const uint8_t* mask, 
   // p0 = z - W Einv W^T K z
   const int nchunks = chunk_setup(defl, W, st);
   if (nchunks < 0) return nchunks;
-  const bool lists = nchunks > 0;
+  const bool lists = restrict_from_lists(defl, g, nchunks);
   if (lists) {
     if ((rc = coarse_update_K(op, g, dp, defl, s, V.z, V.p, W, nchunks, W.S, 1, st))) return rc;
   } else {
@@ -2056,7 +1943,7 @@ static int dpcg_reliable(const pyto_operator_t* op, const double* s, const uint8
   }
   const int nchunks = chunk_setup(defl, W, st);
   if (nchunks < 0) return nchunks;
-  const bool lists = nchunks > 0;
+  const bool lists = restrict_from_lists(defl, g, nchunks);
   k_state_init2<<<1, 1, 0, st>>>(W.S, cfg->rtol, cfg->max_iters, 0);
   PYTO_COUNT(1);
   // start: the coarse solution u = W Einv W_f^T b (src/deflation.py:532-537), or the
@@ -2190,7 +2077,7 @@ extern "C" int pyto_dpcg_mixed_solve(const pyto_operator_t* op, const double* s,
   if (!(cfg->rtol > 0.0) || !(delta > 0.0) || !(delta < 1.0) || cfg->max_iters < 0) return PYTO_ERR_ARG;
   if (((uintptr_t)b | (uintptr_t)u | (uintptr_t)defl->node_group) & 15) return PYTO_ERR_ARG;
   const DeflP dp = make_deflp(op, defl);
-  int rc = gemv_smem_ok(dp.nc);
+  int rc = gemv_smem_ok(defl->coarse_nd ? 0 : dp.nc);
   if (rc) return rc;
   size_t need = 0;
   DpcgWs W = carve_dpcg(op, dp.nc, ws, ws_bytes, &need, true);
@@ -2205,7 +2092,7 @@ extern "C" int pyto_dpcg_solve(const pyto_operator_t* op, const double* s, const
   if (!(cfg->rtol >= 0.0) || cfg->max_iters < 0 || cfg->stop_rule < 0 || cfg->stop_rule > 2) return PYTO_ERR_ARG;
   if (((uintptr_t)b | (uintptr_t)u | (uintptr_t)defl->node_group) & 15) return PYTO_ERR_ARG;
   const DeflP dp = make_deflp(op, defl);
-  int rc = gemv_smem_ok(dp.nc);
+  int rc = gemv_smem_ok(defl->coarse_nd ? 0 : dp.nc);
   if (rc) return rc;
   size_t need = 0;
   DpcgWs W = carve_dpcg(op, dp.nc, ws, ws_bytes, &need);
@@ -2365,6 +2252,8 @@ extern "C" int pyto_batch_create(const pyto_batch_item_t* items, int n, const py
                                  pyto_batch_t* out, void* stream) {
   if (!items || n <= 0 || !cfg || !out) return PYTO_ERR_ARG;
   if (!(cfg->rtol >= 0.0) || cfg->max_iters <= 0 || cfg->stop_rule < 0 || cfg->stop_rule > 1) return PYTO_ERR_ARG;
+  for (int i = 0; i < n; ++i)  // the batched graph uses the dense coarse inverse
+    if (!items[i].defl || items[i].defl->coarse_nd) return PYTO_ERR_ARG;
   *out = nullptr;
   (void)stream;  // nothing runs at creation: the capture uses a private non-blocking stream
   cudaStream_t st = nullptr;
@@ -2496,18 +2385,6 @@ extern "C" int pyto_batch_destroy(pyto_batch_t b) {
 // ---------------------------------------------------------------------------
 namespace pyto {
 
-// v[g*modes + a] = sum over chunks c of part[(g*nch + c)*6 + a], chunks in order
-__global__ void k_restrict_sum(long long nc, int modes, int nch, const double* __restrict__ part,
-                               double* __restrict__ v) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nc;
-       i += (long long)gridDim.x * blockDim.x) {
-    const long long gg = i / modes, a = i - gg * modes;
-    double t = 0.0;
-    for (int c = 0; c < nch; ++c) t += part[(gg * nch + c) * 6 + a];
-    v[i] = t;
-  }
-}
-
 // p = a z + b p - W mu on free DOFs, 0 on fixed ones (z may be null: a z = 0)
 __global__ void __launch_bounds__(256) k_prolong_axpby(GridDims g, DeflP dp, const int32_t* __restrict__ ngrp,
                                                        const double* __restrict__ gc, const double* __restrict__ mu,
@@ -2574,7 +2451,7 @@ __global__ void __launch_bounds__(kNodeThreads) k_cg_update(GridDims g, Prec pc,
 
 extern "C" int pyto_coarse_assemble(const pyto_operator_t* op, const double* s, const uint8_t* mask,
                                     pyto_deflation_t* defl, void* ws, size_t ws_bytes, void* stream) {
-  if (!op || !s || !defl_ok(defl)) return PYTO_ERR_ARG;
+  if (!op || !s || !defl_ok(defl) || defl->coarse_nd) return PYTO_ERR_ARG;  // the dense coarse matrix only
   const DeflP dp = make_deflp(op, defl);
   if (dp.nc > kMaxCoarse) return PYTO_ERR_TOO_LARGE;
   size_t need = 0;
@@ -2588,7 +2465,7 @@ extern "C" int pyto_coarse_assemble(const pyto_operator_t* op, const double* s, 
 
 extern "C" int pyto_coarse_invert(const pyto_operator_t* op, pyto_deflation_t* defl, void* ws, size_t ws_bytes,
                                   void* stream) {
-  if (!op || !defl_ok(defl)) return PYTO_ERR_ARG;
+  if (!op || !defl_ok(defl) || defl->coarse_nd) return PYTO_ERR_ARG;
   const DeflP dp = make_deflp(op, defl);
   int rc0 = gemv_smem_ok(dp.nc);
   if (rc0) return rc0;
@@ -2620,7 +2497,7 @@ extern "C" int pyto_coarse_restrict(const pyto_operator_t* op, const pyto_deflat
 }
 
 extern "C" int pyto_coarse_apply(const pyto_deflation_t* defl, const double* v, double* mu, void* stream) {
-  if (!defl_ok(defl) || !v || !mu || v == mu) return PYTO_ERR_ARG;
+  if (!defl_ok(defl) || defl->coarse_nd || !v || !mu || v == mu) return PYTO_ERR_ARG;
   const long long nc = (long long)defl->ngroups * defl->modes;
   if (nc > kMaxCoarse) return PYTO_ERR_TOO_LARGE;
   int rc0 = gemv_smem_ok(nc);

@@ -1,0 +1,228 @@
+// Blocked Gauss-Jordan sweep of a symmetric matrix held in its lower 64 x 64 tiles
+// (the diagonal tiles in full), as device functions of one 256-thread CTA; used by the
+// dense coarse inverse (deflation.cu) and by the frontal matrices of the
+// nested-dissection coarse solver (coarse_nd.cu).  After sweeping pivot blocks K:
+//   P = A_KK^-1, U = P A_K:, A_ij -= A_iK U_Kj, A_Kj = U_Kj, A_iK = U_Ki^T, A_KK = -P,
+// so sweeping all pivots leaves -A^-1, and sweeping the leading pivots s of
+// [[A_ss, A_sb], [A_bs, A_bb]] leaves -A_ss^-1, A_bs A_ss^-1 and the Schur complement
+// A_bb - A_bs A_ss^-1 A_sb.
+#pragma once
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace pyto {
+
+constexpr int kSweepB = 64;
+
+// Element k of a 4-vector held in registers, by selects (a dynamic index would put
+// the array in local memory).
+__device__ __forceinline__ double pick4(double v0, double v1, double v2, double v3, int k) {
+  double r = v0;
+  r = (k == 1) ? v1 : r;
+  r = (k == 2) ? v2 : r;
+  r = (k == 3) ? v3 : r;
+  return r;
+}
+
+// In-place sweep of the symmetric 64 x 64 block held by 256 threads (thread (ty, tx)
+// owns rows ty + 16a, columns tx + 16b), pivots 0..63 in order:
+//   M_pp -> -1/M_pp,  M_pj -> M_pj/M_pp,  M_ip -> M_ip/M_pp,  M_ij -= M_ip M_pj / M_pp,
+// leaving -M^-1.  Padding pivots (identity rows/columns beyond bk) are decoupled, so they
+// are swept with the rest.  The owners of row p publish it (raw and divided by the
+// pivot) in a double-buffered shared row, so each pivot costs one barrier, and the
+// pivot loop stays rolled: the code is executed 64 times from the instruction cache
+// instead of once per pivot from L2.  The block stays bitwise symmetric (M_ip is read
+// as M_pi).  sm: >= 2 * 130 doubles.
+__device__ __forceinline__ void sweep_pivot_rolled(double (&R)[4][4], double* sm) {
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+#pragma unroll 1
+  for (int p = 0; p < 64; ++p) {
+    double* row = sm + (p & 1) * 130;  // [0, 64): M_p:, [64, 128): M_p: / M_pp, 128: 1 / M_pp
+    const int pr = p & 15, pa = p >> 4;
+    if (ty == pr) {  // half a warp: the owners of row p
+      double v[4];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) v[b] = pick4(R[0][b], R[1][b], R[2][b], R[3][b], pa);
+      const unsigned half = 0xFFFFu << (16 * (ty & 1));
+      const double mpp = __shfl_sync(half, pick4(v[0], v[1], v[2], v[3], pa), pr, 16);
+      const double ip = 1.0 / mpp;
+#pragma unroll
+      for (int b = 0; b < 4; ++b) {
+        row[tx + 16 * b] = v[b];
+        row[64 + tx + 16 * b] = v[b] * ip;
+      }
+      if (tx == 0) row[128] = ip;
+    }
+    __syncthreads();
+    double mip[4], rcj[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) mip[a] = row[ty + 16 * a];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) rcj[b] = row[64 + tx + 16 * b];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) R[a][b] = fma(-mip[a], rcj[b], R[a][b]);
+    if (ty == pr) {  // row p: M_pj / M_pp
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+          if (a == pa) R[a][b] = rcj[b];
+    }
+    if (tx == pr) {  // column p: M_ip / M_pp (= M_pi / M_pp), and the pivot itself
+      const double ip = row[128];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+          if (b == pa) R[a][b] = (ty + 16 * a == p) ? -ip : mip[a] * ip;
+    }
+  }
+  __syncthreads();  // the caller may reuse sm
+}
+
+// P = A_KK^-1 of the pivot block at k0 (bk <= 64 pivots; identity padding), by 256 threads
+__device__ __forceinline__ void sweep_pivot_block(long long n, int k0, int bk, const double* __restrict__ A,
+                                                  double* __restrict__ P) {
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double R[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int i = ty + 16 * a, j = tx + 16 * b;
+      R[a][b] = (i < bk && j < bk) ? A[(k0 + i) * n + (k0 + j)] : (i == j ? 1.0 : 0.0);
+    }
+  __shared__ double sm[2 * 130];
+  sweep_pivot_rolled(R, sm);
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) P[(ty + 16 * a) * kSweepB + tx + 16 * b] = -R[a][b];  // P = A_KK^-1
+}
+
+// Rp = A_K: (copy), U = P Rp for the 16 columns from j0.  Only the lower tiles (and the
+// full diagonal tiles) of A are current, so row K right of the pivot block is read from
+// column K below it.
+__device__ __forceinline__ void sweep_panel_cols(long long n, int k0, int bk, const double* __restrict__ A,
+                                                 const double* __restrict__ P, double* __restrict__ Rp,
+                                                 double* __restrict__ U, long long j0) {
+  __shared__ double sP[kSweepB][kSweepB];
+  __shared__ double sR[kSweepB][17];
+  for (int t = threadIdx.x; t < kSweepB * kSweepB; t += blockDim.x) sP[t / kSweepB][t % kSweepB] = P[t];
+  for (int t = threadIdx.x; t < kSweepB * 16; t += blockDim.x) {
+    const int i = t / 16, jj = t % 16;
+    const long long j = j0 + jj;
+    double v = 0.0;
+    if (i < bk && j < n) v = (j < k0 + kSweepB) ? A[(k0 + i) * n + j] : A[j * n + (k0 + i)];
+    sR[i][jj] = v;
+    if (i < bk && j < n) Rp[i * n + j] = v;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < kSweepB * 16; t += blockDim.x) {
+    const int i = t / 16, jj = t % 16;
+    const long long j = j0 + jj;
+    if (i >= bk || j >= n) continue;
+    double acc = 0.0;
+    for (int k = 0; k < bk; ++k) acc = fma(sP[i][k], sR[k][jj], acc);
+    U[i * n + j] = acc;
+  }
+}
+
+// Update of the lower 64 x 64 tile (ti, tj) by 256 threads x (4 x 4) outputs, k in
+// chunks of 32 for the pivot block at k0 (tiles in row or
+// column K take U / -P); k1 >= 0 and (ti, tj) = (k1, k1) / 64: then sweep that tile as
+// the next pivot block into Pn.
+__device__ __forceinline__ void sweep_update_tile(long long n, int k0, int bk, double* __restrict__ A,
+                                                  const double* __restrict__ P, const double* __restrict__ Rp,
+                                                  const double* __restrict__ U, long long ti, long long tj, int k1,
+                                                  double* __restrict__ Pn) {
+  __shared__ double sLU[2][32][65];  // [0]: A_iK for the tile rows (Rp[k][i]); [1]: U_Kj for the tile cols
+  double(&sL)[32][65] = sLU[0];
+  double(&sU)[32][65] = sLU[1];
+  const long long i0 = ti * 64, j0 = tj * 64;
+  const bool rowK = (i0 == k0), colK = (j0 == k0);
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  // a full pivot block: row / column K tiles are U / -P throughout.  A partial one (bk <
+  // 64: the last pivots of a partial sweep) leaves non-pivot rows and columns in those
+  // tiles, which take the rank-bk update below like any other tile.
+  if ((rowK || colK) && bk == kSweepB) {
+    for (int t = threadIdx.x; t < 64 * 64; t += blockDim.x) {
+      const int ii = t / 64, jj = t % 64;
+      const long long i = i0 + ii, j = j0 + jj;
+      if (i >= n || j >= n) continue;
+      double v;
+      if (rowK && colK) v = (ii < bk && jj < bk) ? -P[ii * kSweepB + jj] : A[i * n + j];
+      else if (rowK) v = (ii < bk) ? U[ii * n + j] : A[i * n + j];
+      else v = (jj < bk) ? U[jj * n + i] : A[i * n + j];
+      A[i * n + j] = v;
+    }
+    return;
+  }
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  for (int kc = 0; kc < bk; kc += 32) {
+    __syncthreads();
+    for (int t = threadIdx.x; t < 32 * 64; t += blockDim.x) {
+      const int k = t / 64, c = t % 64;
+      const bool kin = kc + k < bk;
+      sL[k][c] = (kin && i0 + c < n) ? Rp[(kc + k) * n + i0 + c] : 0.0;
+      sU[k][c] = (kin && j0 + c < n) ? U[(kc + k) * n + j0 + c] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int k = 0; k < 32; ++k) {
+      double l[4], u[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) l[a] = sL[k][ty + 16 * a];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) u[b] = sU[k][tx + 16 * b];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = fma(l[a], u[b], acc[a][b]);
+    }
+  }
+  const bool pivot_next = k1 >= 0 && i0 == k1 && j0 == k1;
+  const int bk1 = (int)std::min<long long>(kSweepB, n - k1);
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int ii = ty + 16 * a, jj = tx + 16 * b;
+      const long long i = i0 + ii, j = j0 + jj;
+      if (i < n && j < n) {
+        const bool pi = rowK && ii < bk, pj = colK && jj < bk;  // pivot row / column
+        double v;
+        if (pi && pj) v = -P[ii * kSweepB + jj];
+        else if (pi) v = U[ii * n + j];
+        else if (pj) v = U[jj * n + i];
+        else v = A[i * n + j] - acc[a][b];
+        A[i * n + j] = v;
+        acc[a][b] = v;
+      }
+    }
+  if (!pivot_next) return;
+  // the next pivot block, as k_sweep_pivot would load it (identity padding)
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int i = ty + 16 * a, j = tx + 16 * b;
+      if (!(i < bk1 && j < bk1)) acc[a][b] = (i == j) ? 1.0 : 0.0;
+    }
+  __syncthreads();
+  sweep_pivot_rolled(acc, &sLU[0][0][0]);  // sL, sU are free now
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) Pn[(ty + 16 * a) * kSweepB + tx + 16 * b] = -acc[a][b];
+}
+
+
+}  // namespace pyto

@@ -18,12 +18,20 @@ import scipy.sparse as sp
 
 from .engine import DeviceDeflation
 
+DENSE_COARSE_MAX = 24576  # largest coarse space of the dense coarse inverse
+
 
 class DeflationSolver:
-    """Deflation space + deflated PCG (src/deflation.py:36-584)."""
+    """Deflation space + deflated PCG (src/deflation.py:36-584).
+
+    ``coarse``: how the coarse system W^T K W is solved on the device -- "dense" (explicit
+    FP64 inverse, one GEMV per correction; up to 24,576 unknowns), "nd" (nested
+    dissection on the box grid of groups, for the element-box aggregates of
+    ``create_deflation_groups_box``) or "auto" (nested dissection when the dense inverse
+    would not fit).  ``nd_leaf``: largest box of groups kept as one tree leaf."""
 
     def __init__(self, minNodesPerGroup: int = 15, use_gpu: bool = True, modes: int = 6, shift: float = 1e-10,
-                 shift_relative: bool = False):
+                 shift_relative: bool = False, coarse: str = "auto", nd_leaf: int = 8):
         self.minNodesPerGroup = minNodesPerGroup
         self.maxGroups = 2000
         self.minGroups = 10
@@ -32,6 +40,10 @@ class DeflationSolver:
         self.modes = int(modes)
         self.shift = float(shift)
         self.shift_relative = bool(shift_relative)
+        if coarse not in ("auto", "dense", "nd"):
+            raise ValueError(f"unknown coarse solver {coarse!r} (auto, dense, nd)")
+        self.coarse = coarse
+        self.nd_leaf = int(nd_leaf)
         self._dev = {}
         self.last_info = None
 
@@ -104,6 +116,7 @@ class DeflationSolver:
         self.ws_nGroups, self.ws_nodeGroupNumber = ng, grp
         self.ws_groupCount, self.ws_groupCenter = count, centre / count[:, None]
         self.modes = int(modes)
+        self.box = tuple(int(v) for v in nb)
         self._dev = {}
         return True
 
@@ -140,8 +153,12 @@ class DeflationSolver:
         key = id(grid)
         d = self._dev.get(key)
         if d is None:
+            box = getattr(self, "box", None)
+            coarse = self.coarse
+            if coarse == "auto":  # nested dissection where a dense coarse matrix would not fit
+                coarse = "nd" if box is not None and self.ws_nGroups * self.modes > DENSE_COARSE_MAX else "dense"
             d = DeviceDeflation(grid, self.ws_nodeGroupNumber, self.ws_groupCenter, self.modes, self.shift,
-                                self.shift_relative)
+                                self.shift_relative, coarse=coarse, group_grid=box, leaf=self.nd_leaf)
             self._dev = {key: d}
         return d
 

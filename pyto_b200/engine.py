@@ -336,7 +336,8 @@ class DeviceDeflation:
     (the non-zero block pattern of W^T K W).
     """
 
-    def __init__(self, grid: HexGrid, node_group, centers, modes=6, shift=1e-10, shift_relative=False):
+    def __init__(self, grid: HexGrid, node_group, centers, modes=6, shift=1e-10, shift_relative=False,
+                 coarse="dense", group_grid=None, leaf=8):
         node_group = np.asarray(node_group, dtype=np.int32).ravel()
         centers = np.asarray(centers, dtype=np.float64).reshape(-1, 3)
         ng = centers.shape[0]
@@ -382,21 +383,68 @@ class DeviceDeflation:
         self.nbr_list = torch.as_tensor(gb, device=dev)
         self.ngroups, self.modes = ng, int(modes)
         self.nc = ng * self.modes
-        self.coarse_inv = torch.empty(self.nc * self.nc, dtype=F64, device=dev)
+        if coarse not in ("dense", "nd"):
+            raise ValueError(f"unknown coarse solver {coarse!r} (dense, nd)")
+        self.coarse = coarse
+        self.nd_plan = None
+        if coarse == "nd":
+            # nested dissection on the box grid of groups: no dense coarse matrix
+            if group_grid is None or int(np.prod(group_grid)) != ng:
+                raise ValueError("coarse='nd' needs the box grid (gx, gy, gz) of the groups")
+            self.box = tuple(int(v) for v in group_grid)
+            self._nptr_h, self._nlist_h = np.ascontiguousarray(nptr), np.ascontiguousarray(gb)
+            plan = A.lib().pyto_coarse_nd_plan(*self.box, self.modes, int(leaf), self._nptr_h.ctypes.data,
+                                               self._nlist_h.ctypes.data)
+            if not plan:
+                raise ValueError("pyto_coarse_nd_plan: " + A.last_error())
+            self.nd_plan = plan
+            info = (C.c_double * 5)()
+            nbytes = A.lib().pyto_coarse_nd_bytes(plan, info)
+            self.nd_info = dict(nodes=int(info[0]), depth=int(info[1]), max_front=int(info[2]),
+                                factor_flops=float(info[3]), solve_bytes=float(info[4]), device_bytes=int(nbytes))
+            self.nd_buf = torch.empty(int(nbytes), dtype=torch.uint8, device=dev)
+            A.call("pyto_coarse_nd_bind", plan, A.ptr(self.nd_buf), int(nbytes), A.stream_ptr(dev))
+            self.coarse_inv = None
+        else:
+            self.coarse_inv = torch.empty(self.nc * self.nc, dtype=F64, device=dev)
         self.struct = A.Deflation(ng, self.modes, A.ptr(self.node_group), A.ptr(self.group_ptr),
-                                  A.ptr(self.group_nodes), A.ptr(self.group_center), A.ptr(self.coarse_inv),
+                                  A.ptr(self.group_nodes), A.ptr(self.group_center),
+                                  A.ptr(self.coarse_inv) if self.coarse_inv is not None else None,
                                   float(shift), 1 if shift_relative else 0, int(counts.max()), A.ptr(self.group_box),
                                   A.ptr(self.nbr_ptr), A.ptr(self.nbr_list), self.max_nbr, 0, None, None)
+        if self.nd_plan is not None:
+            self.struct.coarse_nd = self.nd_plan
         self._node_group_np = node_group
         self.use_boundary_lists = True
         self.mask_version = None
         self.sync(grid)
+
+    def nd_solve(self, v, out=None):
+        """mu = (W_f^T K_ff W_f + shift I)^-1 v with the nested-dissection factors of the
+        last set-up (coarse='nd')."""
+        if self.nd_plan is None:
+            raise ValueError("this deflation space uses the dense coarse inverse")
+        mu = out if out is not None else torch.empty_like(v)
+        A.call("pyto_coarse_nd_solve", self.nd_plan, A.ptr(v), A.ptr(mu), A.stream_ptr(v.device))
+        return mu
+
+    def __del__(self):
+        plan = getattr(self, "nd_plan", None)
+        if plan:
+            try:
+                torch.cuda.synchronize(self.node_group.device)
+            except Exception:  # pragma: no cover - interpreter shutdown
+                pass
+            A.lib().pyto_coarse_nd_free(plan)
+            self.nd_plan = None
 
     def sync(self, grid: HexGrid):
         """(Re)build the per-group boundary element lists for the grid's current fixed
         DOFs: elements with a corner in the group and a corner in another group or on a
         fixed DOF (W_f^T K z is formed from these elements only)."""
         if not self.use_boundary_lists:
+            if self.nd_plan is not None:
+                raise ValueError("the nested-dissection coarse solver needs the boundary element lists")
             self.struct.bel_ptr = self.struct.bel_list = self.struct.bel_meta = None
             self.struct.bel_count = 0
             return self

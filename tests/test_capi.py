@@ -13,7 +13,7 @@ from pyto_b200 import _capi as A
 
 def header_symbols():
     txt = open(os.path.join(ROOT, "include", "pyto_b200.h")).read()
-    return sorted(set(re.findall(r"^(?:int|size_t|long long|const char\*)\s*(pyto_\w+)\s*\(", txt, flags=re.M)))
+    return sorted(set(re.findall(r"^(?:int|size_t|long long|const char\*|void|pyto_\w+_t\*)\s*(pyto_\w+)\s*\(", txt, flags=re.M)))
 
 
 def test_library_exports_every_declared_symbol():
