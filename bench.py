@@ -113,7 +113,7 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def build(device, nel, groups, modes, agg=0, leaf=8):
+def build(device, nel, groups, modes, agg=0, leaf=8, coarse="auto"):
     import torch
     from pyto_b200 import _capi as A
     from pyto_b200.deflation import DeflationSolver
@@ -126,7 +126,7 @@ def build(device, nel, groups, modes, agg=0, leaf=8):
     grid = HexGrid(nel, (1.0, 1.0, 1.0), 1.0, 0.3, device=device).set_fixed_dofs(fixed)
     x = grid.tensor(uniform_density(nel, 0.01, 1.0, seed=0))
     rho = grid.filter(2.0, A.FILTER_DENSITY, x)
-    ds = DeflationSolver(modes=modes, shift=1e-14, shift_relative=True, nd_leaf=leaf)
+    ds = DeflationSolver(modes=modes, shift=1e-14, shift_relative=True, coarse=coarse, nd_leaf=leaf)
     if agg > 0:  # element-box aggregates (nested-dissection coarse solver where the dense one cannot hold them)
         ds.create_deflation_groups_box(mesh, (agg, agg, agg), modes=modes)
     else:
@@ -307,6 +307,8 @@ def main():
                     help="deflation by agg^3-element box aggregates instead of the reference partition "
                          "(4 with --modes 3: the 4x4x4-aggregate, 3-translation coarse space)")
     ap.add_argument("--leaf", type=int, default=8, help="nested-dissection leaf size (groups)")
+    ap.add_argument("--coarse", default="auto", choices=["auto", "dense", "nd"],
+                    help="coarse solver of box aggregates: dense inverse, nested dissection, or auto")
     ap.add_argument("--nel", default=None, help="override grid, e.g. 96,48,48 (not a bench line)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--form", default="mixed", choices=["mixed", "fp64"],
@@ -337,7 +339,7 @@ def main():
     from pyto_b200 import _capi as A
 
     nel = tuple(int(v) for v in args.nel.split(",")) if args.nel else NEL
-    P = build(device, nel, args.groups, args.modes, args.agg, args.leaf)
+    P = build(device, nel, args.groups, args.modes, args.agg, args.leaf, args.coarse)
     P["delta"] = args.delta
     g = P["grid"]
     other = "fp64" if args.form == "mixed" else "mixed"

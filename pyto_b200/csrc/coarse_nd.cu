@@ -48,6 +48,7 @@ struct NdNode {
 
 constexpr int kNdRows = 16;      // front rows per CTA of the solve kernels (one warp per row, 4 warps)
 constexpr int kNdMaxFront = 8192;  // largest front (unknowns) staged in shared memory by the solves
+constexpr int kNdDiagBlocks = 256;  // blocks of the diagonal pass (partial sums of |diag|)
 
 }  // namespace pyto
 
@@ -63,7 +64,7 @@ struct pyto_coarse_nd {
   // per node (host): front size, own unknowns, offsets
   std::vector<long long> front_off, fv_off, scr_off;
   std::vector<int> F, own, fg_off, nfg, emap_off, pull_off0, pull_off1, child0, child1, parent;
-  std::vector<int> fgroups, emap, pull;
+  std::vector<int> fgroups, emap, pull, diag_slot;
   // coarse block pushes (sorted by level)
   std::vector<long long> push_dst1, push_dst2;
   std::vector<int> push_slot, push_ld, push_lo;  // push_lo[level .. level+1]
@@ -84,7 +85,8 @@ struct pyto_coarse_nd {
   // offsets of each table inside i64 / i32
   size_t t_front_off, t_fv_off, t_scr_off, t_push_dst1, t_push_dst2;
   size_t t_F, t_own, t_fg_off, t_nfg, t_emap_off, t_pull0, t_pull1, t_child0, t_child1, t_parent, t_fgroups, t_emap,
-      t_pull, t_push_slot, t_push_ld, t_ext_child, t_piv_node, t_pan_item, t_tile_item, t_fwd_item, t_bwd_item;
+      t_pull, t_push_slot, t_push_ld, t_ext_child, t_piv_node, t_pan_item, t_tile_item, t_fwd_item, t_bwd_item,
+      t_diag_slot;
   char* dev = nullptr;
 };
 
@@ -246,8 +248,12 @@ const char* nd_build(pyto_coarse_nd* P, const int32_t* nptr, const int32_t* nlis
   std::vector<std::vector<int>> lvl_items(P->depth + 1);
   std::vector<long long> d1(P->nslots, -1), d2(P->nslots, -1);
   std::vector<int> ld(P->nslots, 0);
+  P->diag_slot.assign(P->ng, -1);
   for (int G = 0; G < P->ng; ++G) {
     const int gi = G % P->gx, gj = (G / P->gx) % P->gy, gk = G / (P->gx * P->gy);
+    for (int sl = nptr[G]; sl < nptr[G + 1]; ++sl)
+      if (nlist[sl] == G) P->diag_slot[G] = sl;
+    if (P->diag_slot[G] < 0) return "a group is missing from its own neighbour list";
     for (int sl = nptr[G]; sl < nptr[G + 1]; ++sl) {
       const int H = nlist[sl];
       if (H < 0 || H >= P->ng) return "neighbour list entry out of range";
@@ -377,6 +383,7 @@ void nd_items(pyto_coarse_nd* P) {
   P->t_tile_item = put32(P->tile_item);
   P->t_fwd_item = put32(P->fwd_item);
   P->t_bwd_item = put32(P->bwd_item);
+  P->t_diag_slot = put32(P->diag_slot);
   size_t o = 0;
   P->o_E = o;
   o = align256(o + (size_t)P->nslots * P->M * P->M * sizeof(double));
@@ -385,7 +392,7 @@ void nd_items(pyto_coarse_nd* P) {
   P->o_fv = o;
   o = align256(o + (size_t)P->fv_doubles * sizeof(double));
   P->o_scr = o;
-  o = align256(o + (size_t)P->scr_doubles * sizeof(double) + 64 * sizeof(double));  // + the diagonal mean
+  o = align256(o + (size_t)(P->scr_doubles + kNdDiagBlocks) * sizeof(double));  // + the diagonal partials
   P->o_i64 = o;
   o = align256(o + P->i64.size() * sizeof(long long));
   P->o_i32 = o;
@@ -402,7 +409,7 @@ struct NdDev {
   double *E, *fronts, *fv, *scr, *mean;
   const long long *front_off, *fv_off, *scr_off, *push_dst1, *push_dst2;
   const int *F, *own, *fg_off, *emap_off, *pull0, *pull1, *child0, *child1, *parent, *fgroups, *emap, *pull,
-      *push_slot, *push_ld, *ext_child, *piv_node, *pan_item, *tile_item, *fwd_item, *bwd_item;
+      *push_slot, *push_ld, *ext_child, *piv_node, *pan_item, *tile_item, *fwd_item, *bwd_item, *diag_slot;
   int M, ng;
 };
 
@@ -441,6 +448,7 @@ static NdDev nd_dev(const pyto_coarse_nd* P) {
   d.tile_item = i32 + P->t_tile_item;
   d.fwd_item = i32 + P->t_fwd_item;
   d.bwd_item = i32 + P->t_bwd_item;
+  d.diag_slot = i32 + P->t_diag_slot;
   d.M = P->M;
   d.ng = P->ng;
   return d;
@@ -476,28 +484,36 @@ __global__ void __launch_bounds__(128) k_nd_from_fixed(NdDev d, const int32_t* _
 }
 
 // diagonal: zero -> 1 (a mode that vanishes on the free DOFs), + shift (relative: times
-// the mean |diagonal|, summed in a fixed order); one CTA
-__global__ void __launch_bounds__(256) k_nd_diag(NdDev d, const int32_t* __restrict__ nptr,
-                                                 const int32_t* __restrict__ nlist, double shift, int relative) {
+// the mean |diagonal|).  Pass 1: partial sums of |diag| over fixed chunks of the
+// unknowns; pass 2: every block sums the partials in order (the same mean in all
+// blocks) and updates its chunk.
+__global__ void __launch_bounds__(256) k_nd_diag_sum(NdDev d) {
   __shared__ double sred[8];
-  const int M = d.M;
-  const long long nc = (long long)d.ng * M;
-  auto diag = [&](long long i) {
-    const int G = (int)(i / M), a = (int)(i - (long long)G * M);
-    int s = nptr[G];
-    while (nlist[s] != G) ++s;
-    return d.E + (long long)s * M * M + a * M + a;
-  };
+  const long long nc = (long long)d.ng * d.M, per = (nc + gridDim.x - 1) / gridDim.x;
+  const long long i0 = blockIdx.x * per, i1 = min(nc, i0 + per);
   double acc = 0.0;
-  if (relative)
-    for (long long i = threadIdx.x; i < nc; i += blockDim.x) acc += fabs(*diag(i));
-  const double tot = block_sum<256>(acc, sred);
+  for (long long i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+    const int G = (int)(i / d.M), a = (int)(i - (long long)G * d.M);
+    acc += fabs(d.E[((long long)d.diag_slot[G] * d.M + a) * d.M + a]);
+  }
+  const double t = block_sum<256>(acc, sred);
+  if (threadIdx.x == 0) d.mean[blockIdx.x] = t;
+}
+
+__global__ void __launch_bounds__(256) k_nd_diag_apply(NdDev d, double shift, int relative) {
   __shared__ double s_sh;
-  if (threadIdx.x == 0) s_sh = relative ? shift * (tot / (double)nc) : shift;
+  const long long nc = (long long)d.ng * d.M, per = (nc + gridDim.x - 1) / gridDim.x;
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int b = 0; b < (int)gridDim.x; ++b) t += d.mean[b];
+    s_sh = relative ? shift * (t / (double)nc) : shift;
+  }
   __syncthreads();
   const double sh = s_sh;
-  for (long long i = threadIdx.x; i < nc; i += blockDim.x) {
-    double* p = diag(i);
+  const long long i0 = blockIdx.x * per, i1 = min(nc, i0 + per);
+  for (long long i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+    const int G = (int)(i / d.M), a = (int)(i - (long long)G * d.M);
+    double* p = d.E + ((long long)d.diag_slot[G] * d.M + a) * d.M + a;
     double v = *p;
     if (v == 0.0) v = 1.0;
     *p = v + sh;
@@ -679,8 +695,9 @@ int nd_factor(const pyto_coarse_nd* P, const int32_t* nptr, const int32_t* nlist
     attr.done();
   }
   k_nd_from_fixed<<<P->ng, 128, 0, st>>>(d, nptr, nlist, gexp);
-  k_nd_diag<<<1, 256, 0, st>>>(d, nptr, nlist, shift, relative);
-  PYTO_COUNT(2);
+  k_nd_diag_sum<<<kNdDiagBlocks, 256, 0, st>>>(d);
+  k_nd_diag_apply<<<kNdDiagBlocks, 256, 0, st>>>(d, shift, relative);
+  PYTO_COUNT(3);
   for (int l = P->depth; l >= 0; --l) {
     const long long f0 = P->lvl_front_lo[l], f1 = P->lvl_front_hi[l];
     PYTO_CUDA(cudaMemsetAsync(d.fronts + f0, 0, (size_t)(f1 - f0) * sizeof(double), st));
