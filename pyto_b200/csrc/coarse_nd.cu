@@ -25,11 +25,13 @@
 // L = A_bs A_ss^-1 (boundary x own), its transpose (own x boundary) and the Schur
 // complement (boundary x boundary).
 //
-// Solve (per coarse correction): up the tree, each node's frontal vector is its own part
-// of v plus its children's boundary parts (gathered through the children's maps into the
-// parent's front), then its boundary part -= L (own part); down the tree, the own
-// unknowns are -[rows of own] . [own part ; solution at the boundary groups], one GEMV
-// over full front rows.  One kernel per level and direction.
+// Solve (per coarse correction): up the tree, a node's own part is its entries of v plus
+// what its children left in its two incoming slots (one per child: no two writes meet,
+// and the sum runs in a fixed order); each boundary row, incoming slots - L . own part,
+// goes straight into the parent's slot of this child through the child's map.  Down the
+// tree, the own unknowns are -[rows of own] . [own part ; solution at the boundary
+// groups], one GEMV over full front rows.  One kernel per level and direction, a warp per
+// front row.
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -46,7 +48,8 @@ struct NdNode {
   std::vector<int> own, bnd;  // group ids: own (box / separator order), boundary (elimination order)
 };
 
-constexpr int kNdRows = 16;      // front rows per CTA of the solve kernels (one warp per row, 4 warps)
+constexpr int kNdRows = 32;       // front rows per CTA of the solve kernels (8 warps, 4 rows each)
+constexpr int kNdThreads = 256;
 constexpr int kNdMaxFront = 8192;  // largest front (unknowns) staged in shared memory by the solves
 constexpr int kNdDiagBlocks = 256;  // blocks of the diagonal pass (partial sums of |diag|)
 
@@ -63,8 +66,8 @@ struct pyto_coarse_nd {
   double flops = 0.0, solve_bytes = 0.0;
   // per node (host): front size, own unknowns, offsets
   std::vector<long long> front_off, fv_off, scr_off;
-  std::vector<int> F, own, fg_off, nfg, emap_off, pull_off0, pull_off1, child0, child1, parent;
-  std::vector<int> fgroups, emap, pull, diag_slot;
+  std::vector<int> F, own, fg_off, nfg, emap_off, cslot, child0, child1, parent;
+  std::vector<int> fgroups, emap, diag_slot;
   // coarse block pushes (sorted by level)
   std::vector<long long> push_dst1, push_dst2;
   std::vector<int> push_slot, push_ld, push_lo;  // push_lo[level .. level+1]
@@ -79,13 +82,13 @@ struct pyto_coarse_nd {
   std::vector<long long> lvl_front_lo, lvl_front_hi;
   long long fronts_doubles = 0, fv_doubles = 0, scr_doubles = 0;
   // device layout: byte offsets in the bound buffer
-  size_t o_E = 0, o_fronts = 0, o_fv = 0, o_scr = 0, o_i64 = 0, o_i32 = 0, bytes = 0;
+  size_t o_E = 0, o_fronts = 0, o_fv = 0, o_in = 0, o_scr = 0, o_i64 = 0, o_i32 = 0, bytes = 0;
   std::vector<long long> i64;  // packed 64-bit tables
   std::vector<int> i32;        // packed 32-bit tables
   // offsets of each table inside i64 / i32
   size_t t_front_off, t_fv_off, t_scr_off, t_push_dst1, t_push_dst2;
-  size_t t_F, t_own, t_fg_off, t_nfg, t_emap_off, t_pull0, t_pull1, t_child0, t_child1, t_parent, t_fgroups, t_emap,
-      t_pull, t_push_slot, t_push_ld, t_ext_child, t_piv_node, t_pan_item, t_tile_item, t_fwd_item, t_bwd_item,
+  size_t t_F, t_own, t_fg_off, t_nfg, t_emap_off, t_cslot, t_child0, t_child1, t_parent, t_fgroups, t_emap,
+      t_push_slot, t_push_ld, t_ext_child, t_piv_node, t_pan_item, t_tile_item, t_fwd_item, t_bwd_item,
       t_diag_slot;
   char* dev = nullptr;
 };
@@ -218,10 +221,9 @@ const char* nd_build(pyto_coarse_nd* P, const int32_t* nptr, const int32_t* nlis
   }
   P->fronts_doubles = fo;
   P->fv_doubles = vo;
-  // children's boundary groups in the parent's front, and the parent's pull maps
+  // children's boundary groups in the parent's front, and which child each node is
   P->emap_off.assign(nn, -1);
-  P->pull_off0.assign(nn, -1);
-  P->pull_off1.assign(nn, -1);
+  P->cslot.assign(nn, -1);
   std::vector<int> loc(P->ng, -1);
   for (int n = 0; n < nn; ++n) {
     const NdNode& d = P->node[n];
@@ -230,15 +232,11 @@ const char* nd_build(pyto_coarse_nd* P, const int32_t* nptr, const int32_t* nlis
     for (int c = 0; c < d.nchild; ++c) {
       const int ch = d.child[c];
       P->emap_off[ch] = (int)P->emap.size();
-      const int po = (int)P->pull.size();
-      (c == 0 ? P->pull_off0 : P->pull_off1)[n] = po;
-      P->pull.insert(P->pull.end(), P->nfg[n], -1);
-      const std::vector<int>& cb = P->node[ch].bnd;
-      for (int k = 0; k < (int)cb.size(); ++k) {
-        const int r = loc[cb[k]];
+      P->cslot[ch] = c;
+      for (int g : P->node[ch].bnd) {
+        const int r = loc[g];
         if (r < 0) return "a child's boundary group is outside its parent's front";
         P->emap.push_back(r);
-        P->pull[po + r] = k;
       }
     }
     for (int r = 0; r < P->nfg[n]; ++r) loc[P->fgroups[P->fg_off[n] + r]] = -1;
@@ -367,14 +365,12 @@ void nd_items(pyto_coarse_nd* P) {
   P->t_fg_off = put32(P->fg_off);
   P->t_nfg = put32(P->nfg);
   P->t_emap_off = put32(P->emap_off);
-  P->t_pull0 = put32(P->pull_off0);
-  P->t_pull1 = put32(P->pull_off1);
+  P->t_cslot = put32(P->cslot);
   P->t_child0 = put32(P->child0);
   P->t_child1 = put32(P->child1);
   P->t_parent = put32(P->parent);
   P->t_fgroups = put32(P->fgroups);
   P->t_emap = put32(P->emap);
-  P->t_pull = put32(P->pull);
   P->t_push_slot = put32(P->push_slot);
   P->t_push_ld = put32(P->push_ld);
   P->t_ext_child = put32(P->ext_child);
@@ -391,6 +387,8 @@ void nd_items(pyto_coarse_nd* P) {
   o = align256(o + (size_t)P->fronts_doubles * sizeof(double));
   P->o_fv = o;
   o = align256(o + (size_t)P->fv_doubles * sizeof(double));
+  P->o_in = o;  // the children's contributions to each front (two slots)
+  o = align256(o + 2 * (size_t)P->fv_doubles * sizeof(double));
   P->o_scr = o;
   o = align256(o + (size_t)(P->scr_doubles + kNdDiagBlocks) * sizeof(double));  // + the diagonal partials
   P->o_i64 = o;
@@ -406,10 +404,9 @@ namespace pyto {
 
 // Device view of a bound plan.
 struct NdDev {
-  double *E, *fronts, *fv, *scr, *mean;
+  double *E, *fronts, *fv, *in0, *in1, *scr, *mean;
   const long long *front_off, *fv_off, *scr_off, *push_dst1, *push_dst2;
-  const int *F, *own, *fg_off, *emap_off, *pull0, *pull1, *child0, *child1, *parent, *fgroups, *emap, *pull,
-      *push_slot, *push_ld, *ext_child, *piv_node, *pan_item, *tile_item, *fwd_item, *bwd_item, *diag_slot;
+  const int *F, *own, *fg_off, *emap_off, *cslot, *child0, *child1, *parent, *fgroups, *emap, *push_slot, *push_ld, *ext_child, *piv_node, *pan_item, *tile_item, *fwd_item, *bwd_item, *diag_slot;
   int M, ng;
 };
 
@@ -419,6 +416,8 @@ static NdDev nd_dev(const pyto_coarse_nd* P) {
   d.E = (double*)(b + P->o_E);
   d.fronts = (double*)(b + P->o_fronts);
   d.fv = (double*)(b + P->o_fv);
+  d.in0 = (double*)(b + P->o_in);
+  d.in1 = d.in0 + P->fv_doubles;
   d.scr = (double*)(b + P->o_scr);
   d.mean = d.scr + P->scr_doubles;
   const long long* i64 = (const long long*)(b + P->o_i64);
@@ -432,14 +431,12 @@ static NdDev nd_dev(const pyto_coarse_nd* P) {
   d.own = i32 + P->t_own;
   d.fg_off = i32 + P->t_fg_off;
   d.emap_off = i32 + P->t_emap_off;
-  d.pull0 = i32 + P->t_pull0;
-  d.pull1 = i32 + P->t_pull1;
+  d.cslot = i32 + P->t_cslot;
   d.child0 = i32 + P->t_child0;
   d.child1 = i32 + P->t_child1;
   d.parent = i32 + P->t_parent;
   d.fgroups = i32 + P->t_fgroups;
   d.emap = i32 + P->t_emap;
-  d.pull = i32 + P->t_pull;
   d.push_slot = i32 + P->t_push_slot;
   d.push_ld = i32 + P->t_push_ld;
   d.ext_child = i32 + P->t_ext_child;
@@ -595,53 +592,62 @@ __global__ void __launch_bounds__(256) k_nd_mirror(NdDev d, int lo) {
   }
 }
 
-// frontal value at front index r of node n (r < own: v's entry; plus the children's
-// boundary parts that map to r)
-__device__ __forceinline__ double nd_gather(const NdDev& d, int n, int r, const double* __restrict__ v, int own) {
-  const int M = d.M, gr = r / M, m = r - gr * M;
-  double x = (r < own) ? v[(long long)d.fgroups[d.fg_off[n] + gr] * M + m] : 0.0;
-  const int c0 = d.child0[n], c1 = d.child1[n];
-  if (c0 >= 0) {
-    const int k = d.pull[d.pull0[n] + gr];
-    if (k >= 0) x += d.fv[d.fv_off[c0] + d.own[c0] + (long long)k * M + m];
+// dot of a front row with the staged vector w (one warp; four independent partial sums,
+// fixed order: every lane, then a xor butterfly)
+__device__ __forceinline__ double nd_row_dot(const double* __restrict__ a, const double* w, int len, int lane) {
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  int i = lane;
+  for (; i + 96 < len; i += 128) {
+    s0 = fma(a[i], w[i], s0);
+    s1 = fma(a[i + 32], w[i + 32], s1);
+    s2 = fma(a[i + 64], w[i + 64], s2);
+    s3 = fma(a[i + 96], w[i + 96], s3);
   }
-  if (c1 >= 0) {
-    const int k = d.pull[d.pull1[n] + gr];
-    if (k >= 0) x += d.fv[d.fv_off[c1] + d.own[c1] + (long long)k * M + m];
-  }
-  return x;
+  for (; i < len; i += 32) s0 = fma(a[i], w[i], s0);
+  double acc = (s0 + s1) + (s2 + s3);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  return acc;
 }
 
-// up the tree, one level: frontal vectors (own part staged in shared memory), boundary
-// part -= L own part; blockIdx.x: (node, first boundary row), one warp per row
-__global__ void __launch_bounds__(128) k_nd_fwd(NdDev d, const double* __restrict__ v, int lo,
-                                                const KrylovState* S) {
+// up the tree, one level; blockIdx.x: (node, first boundary row).  The node's own part is
+// its entries of v plus what its children left in its two incoming slots; each boundary
+// row (incoming slots - L . own part) goes to the parent's incoming slot of this child.
+__global__ void __launch_bounds__(kNdThreads) k_nd_fwd(NdDev d, const double* __restrict__ v, int lo,
+                                                       const KrylovState* S) {
   if (S && S->done) return;
   extern __shared__ double nd_w[];
   const int* it = d.fwd_item + 2LL * (lo + blockIdx.x);
   const int n = it[0], r0 = it[1];
-  const int F = d.F[n], own = d.own[n];
-  for (int i = threadIdx.x; i < own; i += blockDim.x) nd_w[i] = nd_gather(d, n, i, v, own);
+  const int F = d.F[n], own = d.own[n], M = d.M;
+  const long long off = d.fv_off[n];
+  const int* fg = d.fgroups + d.fg_off[n];
+  for (int i = threadIdx.x; i < own; i += blockDim.x) {
+    const int g = i / M;
+    nd_w[i] = (v[(long long)fg[g] * M + (i - g * M)] + d.in0[off + i]) + d.in1[off + i];
+  }
   __syncthreads();
-  double* fvn = d.fv + d.fv_off[n];
   if (r0 == 0)
-    for (int i = threadIdx.x; i < own; i += blockDim.x) fvn[i] = nd_w[i];
+    for (int i = threadIdx.x; i < own; i += blockDim.x) d.fv[off + i] = nd_w[i];
+  const int P = d.parent[n];
+  if (P < 0) return;
+  double* dst = (d.cslot[n] == 0 ? d.in0 : d.in1) + d.fv_off[P];
+  const int* em = d.emap + d.emap_off[n];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const double* A = d.fronts + d.front_off[n];
-  for (int k = r0 + wid; k < min(r0 + kNdRows, F - own); k += 4) {
-    const int row = own + k;
-    const double* a = A + (long long)row * F;
-    double acc = 0.0;
-    for (int i = lane; i < own; i += 32) acc = fma(a[i], nd_w[i], acc);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (lane == 0) fvn[row] = nd_gather(d, n, row, v, own) - acc;
+  for (int k = r0 + wid; k < min(r0 + kNdRows, F - own); k += kNdThreads / 32) {
+    const double acc = nd_row_dot(A + (long long)(own + k) * F, nd_w, own, lane);
+    if (lane == 0) {
+      const int gk = k / M;
+      dst[(long long)em[gk] * M + (k - gk * M)] = (d.in0[off + own + k] + d.in1[off + own + k]) - acc;
+    }
   }
 }
 
 // down the tree, one level: own unknowns = -(front rows of own) . [own part; solution at
-// the boundary groups]; blockIdx.x: (node, first own row), one warp per row
-__global__ void __launch_bounds__(128) k_nd_bwd(NdDev d, double* __restrict__ mu, int lo, const KrylovState* S) {
+// the boundary groups]; blockIdx.x: (node, first own row)
+__global__ void __launch_bounds__(kNdThreads) k_nd_bwd(NdDev d, double* __restrict__ mu, int lo,
+                                                       const KrylovState* S) {
   if (S && S->done) return;
   extern __shared__ double nd_w[];
   const int* it = d.bwd_item + 2LL * (lo + blockIdx.x);
@@ -660,12 +666,8 @@ __global__ void __launch_bounds__(128) k_nd_bwd(NdDev d, double* __restrict__ mu
   __syncthreads();
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const double* A = d.fronts + d.front_off[n];
-  for (int r = r0 + wid; r < min(r0 + kNdRows, own); r += 4) {
-    const double* a = A + (long long)r * F;
-    double acc = 0.0;
-    for (int i = lane; i < F; i += 32) acc = fma(a[i], nd_w[i], acc);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  for (int r = r0 + wid; r < min(r0 + kNdRows, own); r += kNdThreads / 32) {
+    const double acc = nd_row_dot(A + (long long)r * F, nd_w, F, lane);
     if (lane == 0) {
       const int g = r / M;
       mu[(long long)fg[g] * M + (r - g * M)] = -acc;
@@ -741,17 +743,18 @@ int nd_solve(const pyto_coarse_nd* P, const double* v, double* mu, const KrylovS
   if (!P->dev) return PYTO_ERR_ARG;
   const NdDev d = nd_dev(P);
   const size_t shm = (size_t)P->maxF * sizeof(double);
+  PYTO_CUDA(cudaMemsetAsync(d.in0, 0, 2 * (size_t)P->fv_doubles * sizeof(double), st));
   for (int l = P->depth; l >= 0; --l) {
     const int a = P->fwd_lo[l], b = P->fwd_lo[l + 1];
     if (b > a) {
-      k_nd_fwd<<<b - a, 128, shm, st>>>(d, v, a, S);
+      k_nd_fwd<<<b - a, kNdThreads, shm, st>>>(d, v, a, S);
       PYTO_COUNT(1);
     }
   }
   for (int l = 0; l <= P->depth; ++l) {
     const int a = P->bwd_lo[l], b = P->bwd_lo[l + 1];
     if (b > a) {
-      k_nd_bwd<<<b - a, 128, shm, st>>>(d, mu, a, S);
+      k_nd_bwd<<<b - a, kNdThreads, shm, st>>>(d, mu, a, S);
       PYTO_COUNT(1);
     }
   }

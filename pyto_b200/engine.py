@@ -430,13 +430,14 @@ class DeviceDeflation:
 
     def __del__(self):
         plan = getattr(self, "nd_plan", None)
-        if plan:
-            try:
-                torch.cuda.synchronize(self.node_group.device)
-            except Exception:  # pragma: no cover - interpreter shutdown
-                pass
+        if not plan:
+            return
+        self.nd_plan = None
+        try:  # the plan's device buffer is torch's; the host plan must outlive queued work
+            torch.cuda.synchronize(self.node_group.device)
             A.lib().pyto_coarse_nd_free(plan)
-            self.nd_plan = None
+        except Exception:  # pragma: no cover - interpreter shutdown: the process frees it
+            pass
 
     def sync(self, grid: HexGrid):
         """(Re)build the per-group boundary element lists for the grid's current fixed
