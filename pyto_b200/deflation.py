@@ -95,6 +95,9 @@ class DeflationSolver:
         self.ws_nodeGroupNumber = grp
         self.ws_groupCount = count
         self.ws_groupCenter = centre
+        # without merges the partition is a regular nX x nY x nZ box grid (group id
+        # ix + nX iy + nX nY iz): the nested-dissection coarse solver applies to it
+        self.box = (int(nX), int(nY), int(nZ)) if ngroups == ntent else None
         self._dev = {}
         if np.any(self.ws_groupCount < self.minNodesPerGroup):
             warnings.warn(f"deflation groups with very few nodes (smallest {int(np.min(self.ws_groupCount))})")
