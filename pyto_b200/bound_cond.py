@@ -32,10 +32,34 @@ class BC:
 
 
 def impose_dirichlet_bc(A, b, bc: BC):
-    """The reference's row/column elimination has no matrix to act on here: the
-    GPU operator is matrix-free and masks fixed DOFs (src/bound_cond.py:40-70)."""
+    """Dirichlet elimination (src/bound_cond.py:40-70): b - A[:, fixed] g, then the
+    free rows (and, for an assembled matrix, the free columns).
+
+    ``A`` may be PyTO's assembled scipy matrix -- the reference's elimination, returning
+    (A[free][:, free], b[free]) -- or this library's matrix-free operator
+    (``linear_solvers.StiffnessOperator``): the lift A[:, fixed] g is one masked operator
+    application on the GPU, and the operator is returned unchanged (the GPU solvers
+    eliminate the fixed DOFs by masking full-length vectors), with b[free] as a device
+    tensor.  Constraint-matrix BCs raise NotImplementedError, as in the reference."""
     if bc.constraint_matrix is not None:
         raise NotImplementedError("impose_dirichlet_bc not implemented for constraint_matrix BCs; "
                                   "see linear_solvers.solve")
-    raise NotImplementedError("pyto_b200 eliminates Dirichlet DOFs by masking inside the GPU solvers; "
-                              "use linear_solvers.solve with fe_solver.stiff_mtrx")
+    fixed = np.asarray(bc.fixed_dofs, dtype=np.int64)
+    free = bc.free_dofs
+    g = np.zeros(np.shape(b)[0]) if bc.dirichlet_values is None else np.asarray(bc.dirichlet_values, dtype=float)
+    if getattr(A, "is_pyto_operator", False):
+        import torch
+
+        from . import _capi
+        grid = A.grid
+        bd = grid.tensor(b)
+        if g.size and np.any(g != 0):
+            lift = torch.zeros(grid.ndof, dtype=torch.float64, device=grid.device)
+            lift[grid.tensor(fixed, torch.int64)] = grid.tensor(np.broadcast_to(g, fixed.shape).astype(np.float64))
+            bd = bd - grid.matvec(A.s, lift, mode=_capi.MASK_OUT)
+        return A, bd[grid.tensor(free, torch.int64)]
+    b_mod = np.array(b, dtype=float, copy=True)
+    if g.size and np.any(g != 0):
+        b_mod -= A[:, fixed] @ np.broadcast_to(g, fixed.shape)
+    A_mod = A.tocsr()[free, :][:, free]
+    return A_mod, b_mod[free]
