@@ -568,7 +568,7 @@ __global__ void __launch_bounds__(256) k_nd_panel(NdDev d, int lo, int k0) {
   sweep_panel_cols(F, k0, bk, d.fronts + d.front_off[n], P, Rp, Rp + kSweepB * F, it[1]);
 }
 
-__global__ void __launch_bounds__(256, 3) k_nd_update(NdDev d, int lo, int k0) {
+__global__ void __launch_bounds__(256, 2) k_nd_update(NdDev d, int lo, int k0) {
   const int* it = d.tile_item + 3LL * (lo + blockIdx.x);
   const int n = it[0];
   const int bk = min(kSweepB, d.own[n] - k0);
@@ -576,7 +576,7 @@ __global__ void __launch_bounds__(256, 3) k_nd_update(NdDev d, int lo, int k0) {
   const long long F = d.F[n];
   double* P = d.scr + d.scr_off[n];
   double* Rp = P + kSweepB * kSweepB;
-  sweep_update_tile(F, k0, bk, d.fronts + d.front_off[n], P, Rp, Rp + kSweepB * F, it[1], it[2], -1, nullptr);
+  sweep_update_tile(F, k0, bk, d.fronts + d.front_off[n], P, Rp, Rp + kSweepB * F, it[1], it[2], -1, nullptr, 0);
 }
 
 // lower tiles -> upper tiles (the fronts are stored in full after their sweep)
@@ -696,6 +696,11 @@ int nd_factor(const pyto_coarse_nd* P, const int32_t* nptr, const int32_t* nlist
                                    (int)(kNdMaxFront * sizeof(double))));
     attr.done();
   }
+  static PerDevice attr_u;
+  if (attr_u.needed()) {
+    PYTO_CUDA(cudaFuncSetAttribute(k_nd_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSweepTileSmem));
+    attr_u.done();
+  }
   k_nd_from_fixed<<<P->ng, 128, 0, st>>>(d, nptr, nlist, gexp);
   k_nd_diag_sum<<<kNdDiagBlocks, 256, 0, st>>>(d);
   k_nd_diag_apply<<<kNdDiagBlocks, 256, 0, st>>>(d, shift, relative);
@@ -728,7 +733,7 @@ int nd_factor(const pyto_coarse_nd* P, const int32_t* nptr, const int32_t* nlist
     for (int k0 = 0; k0 < P->lvl_maxown[l]; k0 += kSweepB) {
       k_nd_pivot<<<pv1 - pv0, 256, 0, st>>>(d, pv0, k0);
       k_nd_panel<<<pa1 - pa0, 256, 0, st>>>(d, pa0, k0);
-      k_nd_update<<<t1 - t0, 256, 0, st>>>(d, t0, k0);
+      k_nd_update<<<t1 - t0, 256, kSweepTileSmem, st>>>(d, t0, k0);
       PYTO_COUNT(3);
     }
     k_nd_mirror<<<t1 - t0, 256, 0, st>>>(d, t0);

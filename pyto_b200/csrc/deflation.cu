@@ -569,7 +569,7 @@ __global__ void __launch_bounds__(256) k_sweep_panel(long long n, int k0, int bk
 // 256 threads x (4x4) outputs, k in chunks of 32.  k1 >= 0: the CTA of the next
 // pivot tile (k1, k1) -- block 0, so it starts first -- goes on to sweep it in
 // registers and writes Pn = A_k1k1^-1 for the next step, behind the other tiles.
-__global__ void __launch_bounds__(256, 3) k_sweep_update(long long n, int k0, int bk, double* __restrict__ A,
+__global__ void __launch_bounds__(256, 2) k_sweep_update(long long n, int k0, int bk, double* __restrict__ A,
                                                       const double* __restrict__ P, const double* __restrict__ Rp,
                                                       const double* __restrict__ U, int k1, double* __restrict__ Pn) {
   const long long ntiles = gridDim.x;
@@ -582,7 +582,7 @@ __global__ void __launch_bounds__(256, 3) k_sweep_update(long long n, int k0, in
   while (ti * (ti + 1) / 2 > b) --ti;
   while ((ti + 1) * (ti + 2) / 2 <= b) ++ti;
   const long long tj = b - ti * (ti + 1) / 2;
-  sweep_update_tile(n, k0, bk, A, P, Rp, U, ti, tj, k1, Pn);
+  sweep_update_tile(n, k0, bk, A, P, Rp, U, ti, tj, k1, Pn, k1 >= 0 ? (int)std::min<long long>(kSweepB, n - k1) : 0);
 }
 
 // E^-1 = -A: negate the lower tiles (diagonal tiles in full) and mirror them
@@ -1582,6 +1582,11 @@ static int coarse_invert_launch(const pyto_deflation_t* defl, const DpcgWs& W, c
   PYTO_COUNT(1);
   PYTO_LAUNCH_CHECK();
   const int tiles = (int)((n + 63) / 64);
+  static PerDevice attr;
+  if (attr.needed()) {
+    PYTO_CUDA(cudaFuncSetAttribute(k_sweep_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSweepTileSmem));
+    attr.done();
+  }
   // pivot block inverses alternate between two buffers: the update of step K sweeps
   // the pivot block of step K+1 into the other one
   k_sweep_pivot<<<1, 256, 0, st>>>(n, 0, (int)std::min<long long>(kSweepB, n), E, W.P);
@@ -1594,7 +1599,8 @@ static int coarse_invert_launch(const pyto_deflation_t* defl, const DpcgWs& W, c
     const long long k1 = k0 + kSweepB < n ? k0 + kSweepB : -1;
     k_sweep_panel<<<(int)((n + 15) / 16), 256, 0, st>>>(n, (int)k0, bk, E, Pc, W.Rp, W.U);
     PYTO_COUNT(1);
-    k_sweep_update<<<(int)((long long)tiles * (tiles + 1) / 2), 256, 0, st>>>(n, (int)k0, bk, E, Pc, W.Rp, W.U,
+    k_sweep_update<<<(int)((long long)tiles * (tiles + 1) / 2), 256, kSweepTileSmem, st>>>(n, (int)k0, bk, E, Pc,
+                                                                                          W.Rp, W.U,
                                                                              (int)k1, Pn);
     PYTO_COUNT(1);
   }

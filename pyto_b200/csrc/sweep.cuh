@@ -111,14 +111,27 @@ __device__ __forceinline__ void sweep_panel_cols(long long n, int k0, int bk, co
                                                  double* __restrict__ U, long long j0) {
   __shared__ double sP[kSweepB][kSweepB];
   __shared__ double sR[kSweepB][17];
-  for (int t = threadIdx.x; t < kSweepB * kSweepB; t += blockDim.x) sP[t / kSweepB][t % kSweepB] = P[t];
-  for (int t = threadIdx.x; t < kSweepB * 16; t += blockDim.x) {
-    const int i = t / 16, jj = t % 16;
+  // 256 threads: every load of P and of the 16 columns issued before the first store
+  double vp[kSweepB * kSweepB / 256], vr[kSweepB * 16 / 256];
+#pragma unroll
+  for (int r = 0; r < kSweepB * kSweepB / 256; ++r) vp[r] = P[threadIdx.x + 256 * r];
+#pragma unroll
+  for (int r = 0; r < kSweepB * 16 / 256; ++r) {
+    const int t = threadIdx.x + 256 * r, i = t / 16, jj = t % 16;
     const long long j = j0 + jj;
-    double v = 0.0;
-    if (i < bk && j < n) v = (j < k0 + kSweepB) ? A[(k0 + i) * n + j] : A[j * n + (k0 + i)];
-    sR[i][jj] = v;
-    if (i < bk && j < n) Rp[i * n + j] = v;
+    vr[r] = (i < bk && j < n) ? ((j < k0 + kSweepB) ? A[(k0 + i) * n + j] : A[j * n + (k0 + i)]) : 0.0;
+  }
+#pragma unroll
+  for (int r = 0; r < kSweepB * kSweepB / 256; ++r) {
+    const int t = threadIdx.x + 256 * r;
+    sP[t / kSweepB][t % kSweepB] = vp[r];
+  }
+#pragma unroll
+  for (int r = 0; r < kSweepB * 16 / 256; ++r) {
+    const int t = threadIdx.x + 256 * r, i = t / 16, jj = t % 16;
+    const long long j = j0 + jj;
+    sR[i][jj] = vr[r];
+    if (i < bk && j < n) Rp[i * n + j] = vr[r];
   }
   __syncthreads();
   for (int t = threadIdx.x; t < kSweepB * 16; t += blockDim.x) {
@@ -131,17 +144,22 @@ __device__ __forceinline__ void sweep_panel_cols(long long n, int k0, int bk, co
   }
 }
 
-// Update of the lower 64 x 64 tile (ti, tj) by 256 threads x (4 x 4) outputs, k in
-// chunks of 32 for the pivot block at k0 (tiles in row or
-// column K take U / -P); k1 >= 0 and (ti, tj) = (k1, k1) / 64: then sweep that tile as
-// the next pivot block into Pn.
+// Dynamic shared memory of sweep_update_tile: the tile rows' A_iK and the tile columns'
+// U_Kj for all bk <= 64 pivots (2 x 64 x 64 doubles).
+constexpr size_t kSweepTileSmem = 2 * 64 * 64 * sizeof(double);
+
+// Update of the lower 64 x 64 tile (ti, tj) by 256 threads x (4 x 4) outputs for the
+// pivot block at k0 (tiles in row or column K take U / -P); k1 >= 0 and (ti, tj) =
+// (k1, k1) / 64: then sweep that tile as the next pivot block into Pn (bk1 pivots).
+// Every global load of the tile (its A entries, the bk rows of A_iK and U_Kj) is issued
+// before the first is used, then staged in shared memory (kSweepTileSmem, dynamic).
 __device__ __forceinline__ void sweep_update_tile(long long n, int k0, int bk, double* __restrict__ A,
                                                   const double* __restrict__ P, const double* __restrict__ Rp,
                                                   const double* __restrict__ U, long long ti, long long tj, int k1,
-                                                  double* __restrict__ Pn) {
-  __shared__ double sLU[2][32][65];  // [0]: A_iK for the tile rows (Rp[k][i]); [1]: U_Kj for the tile cols
-  double(&sL)[32][65] = sLU[0];
-  double(&sU)[32][65] = sLU[1];
+                                                  double* __restrict__ Pn, int bk1) {
+  extern __shared__ double sw_dyn[];
+  double* sL = sw_dyn;            // [64][64]: A_iK for the tile rows (Rp[k][i0 + c])
+  double* sU = sw_dyn + 64 * 64;  // [64][64]: U_Kj for the tile columns
   const long long i0 = ti * 64, j0 = tj * 64;
   const bool rowK = (i0 == k0), colK = (j0 == k0);
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
@@ -161,35 +179,47 @@ __device__ __forceinline__ void sweep_update_tile(long long n, int k0, int bk, d
     }
     return;
   }
+  // the tile's own entries and the operand rows, all loads in flight together
+  double a_in[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const long long i = i0 + ty + 16 * a, j = j0 + tx + 16 * b;
+      a_in[a][b] = (i < n && j < n) ? A[i * n + j] : 0.0;
+    }
+  constexpr int PER = 64 * 64 / 256;  // operand entries per thread and operand
+#pragma unroll
+  for (int r = 0; r < PER; ++r) {  // 8-byte asynchronous copies (zero-filled outside)
+    const int t = threadIdx.x + 256 * r, k = t / 64, c = t % 64;
+    const bool okl = k < bk && i0 + c < n, oku = k < bk && j0 + c < n;
+    const unsigned dl = (unsigned)__cvta_generic_to_shared(sL + t), du = (unsigned)__cvta_generic_to_shared(sU + t);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dl),
+                 "l"(okl ? Rp + k * n + i0 + c : Rp), "r"(okl ? 8 : 0) : "memory");
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(du),
+                 "l"(oku ? U + k * n + j0 + c : U), "r"(oku ? 8 : 0) : "memory");
+  }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+  __syncthreads();
   double acc[4][4];
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-  for (int kc = 0; kc < bk; kc += 32) {
-    __syncthreads();
-    for (int t = threadIdx.x; t < 32 * 64; t += blockDim.x) {
-      const int k = t / 64, c = t % 64;
-      const bool kin = kc + k < bk;
-      sL[k][c] = (kin && i0 + c < n) ? Rp[(kc + k) * n + i0 + c] : 0.0;
-      sU[k][c] = (kin && j0 + c < n) ? U[(kc + k) * n + j0 + c] : 0.0;
-    }
-    __syncthreads();
 #pragma unroll 4
-    for (int k = 0; k < 32; ++k) {
-      double l[4], u[4];
+  for (int k = 0; k < bk; ++k) {
+    double l[4], u[4];
 #pragma unroll
-      for (int a = 0; a < 4; ++a) l[a] = sL[k][ty + 16 * a];
+    for (int a = 0; a < 4; ++a) l[a] = sL[k * 64 + ty + 16 * a];
 #pragma unroll
-      for (int b = 0; b < 4; ++b) u[b] = sU[k][tx + 16 * b];
+    for (int b = 0; b < 4; ++b) u[b] = sU[k * 64 + tx + 16 * b];
 #pragma unroll
-      for (int a = 0; a < 4; ++a)
+    for (int a = 0; a < 4; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = fma(l[a], u[b], acc[a][b]);
-    }
+      for (int b = 0; b < 4; ++b) acc[a][b] = fma(l[a], u[b], acc[a][b]);
   }
   const bool pivot_next = k1 >= 0 && i0 == k1 && j0 == k1;
-  const int bk1 = (int)std::min<long long>(kSweepB, n - k1);
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
@@ -202,7 +232,7 @@ __device__ __forceinline__ void sweep_update_tile(long long n, int k0, int bk, d
         if (pi && pj) v = -P[ii * kSweepB + jj];
         else if (pi) v = U[ii * n + j];
         else if (pj) v = U[jj * n + i];
-        else v = A[i * n + j] - acc[a][b];
+        else v = a_in[a][b] - acc[a][b];
         A[i * n + j] = v;
         acc[a][b] = v;
       }
@@ -217,7 +247,7 @@ __device__ __forceinline__ void sweep_update_tile(long long n, int k0, int bk, d
       if (!(i < bk1 && j < bk1)) acc[a][b] = (i == j) ? 1.0 : 0.0;
     }
   __syncthreads();
-  sweep_pivot_rolled(acc, &sLU[0][0][0]);  // sL, sU are free now
+  sweep_pivot_rolled(acc, sw_dyn);  // the operand rows are consumed
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
