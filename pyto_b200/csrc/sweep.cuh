@@ -26,61 +26,81 @@ __device__ __forceinline__ double pick4(double v0, double v1, double v2, double 
 }
 
 // In-place sweep of the symmetric 64 x 64 block held by 256 threads (thread (ty, tx)
-// owns rows ty + 16a, columns tx + 16b), pivots 0..63 in order:
-//   M_pp -> -1/M_pp,  M_pj -> M_pj/M_pp,  M_ip -> M_ip/M_pp,  M_ij -= M_ip M_pj / M_pp,
-// leaving -M^-1.  Padding pivots (identity rows/columns beyond bk) are decoupled, so they
-// are swept with the rest.  The owners of row p publish it (raw and divided by the
-// pivot) in a double-buffered shared row, so each pivot costs one barrier, and the
-// pivot loop stays rolled: the code is executed 64 times from the instruction cache
-// instead of once per pivot from L2.  The block stays bitwise symmetric (M_ip is read
-// as M_pi).  sm: >= 2 * 130 doubles.
-__device__ __forceinline__ void sweep_pivot_rolled(double (&R)[4][4], double* sm) {
+// owns rows ty + 16a, columns tx + 16b), leaving -M^-1 (pivot by pivot:
+//   M_pp -> -1/M_pp,  M_pj -> M_pj/M_pp,  M_ip -> M_ip/M_pp,  M_ij -= M_ip M_pj / M_pp).
+// Padding pivots (identity rows/columns beyond bk) are decoupled, so they are swept with
+// the rest.  Blocked by 16: for each 16-pivot block K, one warp sweeps the 16 x 16
+// diagonal block in registers (lane 2r + h holds row r, columns 8h..8h+7; the pivot row
+// and column arrive by shuffles, so the 16 pivots cost no CTA barrier), then all threads
+// apply the block step (U = P M_K: with P = M_KK^-1; M_ij -= M_iK U_Kj; M_Kj = U_Kj,
+// M_iK = U_Ki, M_KK = -P), four barriers per block.  M stays symmetric throughout, so
+// the column panel M_:K is read as the row panel M_K:.  sm: >= kSweepPivotSmem doubles.
+constexpr int kSweepPivotSmem = 2 * 16 * 64 + 16 * 16;
+__device__ __forceinline__ void sweep_pivot_blocked(double (&R)[4][4], double* sm) {
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double* sRow = sm;            // [16][64]: M_K: before the block step
+  double* sU = sm + 16 * 64;    // [16][64]: U = P M_K:
+  double* sP = sm + 2 * 16 * 64;  // [16][16]: P = M_KK^-1
 #pragma unroll 1
-  for (int p = 0; p < 64; ++p) {
-    double* row = sm + (p & 1) * 130;  // [0, 64): M_p:, [64, 128): M_p: / M_pp, 128: 1 / M_pp
-    const int pr = p & 15, pa = p >> 4;
-    if (ty == pr) {  // half a warp: the owners of row p
-      double v[4];
+  for (int K = 0; K < 4; ++K) {
 #pragma unroll
-      for (int b = 0; b < 4; ++b) v[b] = pick4(R[0][b], R[1][b], R[2][b], R[3][b], pa);
-      const unsigned half = 0xFFFFu << (16 * (ty & 1));
-      const double mpp = __shfl_sync(half, pick4(v[0], v[1], v[2], v[3], pa), pr, 16);
-      const double ip = 1.0 / mpp;
+    for (int b = 0; b < 4; ++b) sRow[ty * 64 + tx + 16 * b] = pick4(R[0][b], R[1][b], R[2][b], R[3][b], K);
+    __syncthreads();
+    if (threadIdx.x < 32) {  // warp 0: Gauss-Jordan sweep of M_KK in registers
+      const int l = threadIdx.x, r = l >> 1, h = l & 1;
+      double X[8];
 #pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        row[tx + 16 * b] = v[b];
-        row[64 + tx + 16 * b] = v[b] * ip;
+      for (int k = 0; k < 8; ++k) X[k] = sRow[r * 64 + 16 * K + 8 * h + k];
+#pragma unroll
+      for (int p = 0; p < 16; ++p) {
+        const double mpp = __shfl_sync(0xffffffffu, X[p & 7], 2 * p + (p >> 3));
+        const double ip = 1.0 / mpp;
+        double rowv[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) rowv[k] = __shfl_sync(0xffffffffu, X[k], 2 * p + h);
+        const double colv = __shfl_sync(0xffffffffu, X[p & 7], 2 * r + (p >> 3));
+        const double f = -colv * ip;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) X[k] = fma(f, rowv[k], X[k]);
+        if (r == p) {
+#pragma unroll
+          for (int k = 0; k < 8; ++k) X[k] = rowv[k] * ip;
+        }
+        if ((p >> 3) == h) X[p & 7] = (r == p) ? -ip : colv * ip;
       }
-      if (tx == 0) row[128] = ip;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) sP[r * 16 + 8 * h + k] = -X[k];
     }
     __syncthreads();
-    double mip[4], rcj[4];
+    // U_Kj = sum_k P[ty][k] M_K:[k][j] for the thread's columns j = tx + 16b
 #pragma unroll
-    for (int a = 0; a < 4; ++a) mip[a] = row[ty + 16 * a];
+    for (int b = 0; b < 4; ++b) {
+      double u = 0.0;
 #pragma unroll
-    for (int b = 0; b < 4; ++b) rcj[b] = row[64 + tx + 16 * b];
+      for (int k = 0; k < 16; ++k) u = fma(sP[ty * 16 + k], sRow[k * 64 + tx + 16 * b], u);
+      sU[ty * 64 + tx + 16 * b] = u;
+    }
+    __syncthreads();
 #pragma unroll
     for (int a = 0; a < 4; ++a)
 #pragma unroll
-      for (int b = 0; b < 4; ++b) R[a][b] = fma(-mip[a], rcj[b], R[a][b]);
-    if (ty == pr) {  // row p: M_pj / M_pp
+      for (int b = 0; b < 4; ++b) {
+        const int i = ty + 16 * a, j = tx + 16 * b;
+        if (a == K && b == K) {
+          R[a][b] = -sP[ty * 16 + tx];
+        } else if (a == K) {
+          R[a][b] = sU[ty * 64 + j];
+        } else if (b == K) {
+          R[a][b] = sU[tx * 64 + i];
+        } else {
+          double t = R[a][b];
 #pragma unroll
-      for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b)
-          if (a == pa) R[a][b] = rcj[b];
-    }
-    if (tx == pr) {  // column p: M_ip / M_pp (= M_pi / M_pp), and the pivot itself
-      const double ip = row[128];
-#pragma unroll
-      for (int a = 0; a < 4; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b)
-          if (b == pa) R[a][b] = (ty + 16 * a == p) ? -ip : mip[a] * ip;
-    }
+          for (int k = 0; k < 16; ++k) t = fma(-sRow[k * 64 + i], sU[k * 64 + j], t);
+          R[a][b] = t;
+        }
+      }
+    __syncthreads();
   }
-  __syncthreads();  // the caller may reuse sm
 }
 
 // P = A_KK^-1 of the pivot block at k0 (bk <= 64 pivots; identity padding), by 256 threads
@@ -95,8 +115,8 @@ __device__ __forceinline__ void sweep_pivot_block(long long n, int k0, int bk, c
       const int i = ty + 16 * a, j = tx + 16 * b;
       R[a][b] = (i < bk && j < bk) ? A[(k0 + i) * n + (k0 + j)] : (i == j ? 1.0 : 0.0);
     }
-  __shared__ double sm[2 * 130];
-  sweep_pivot_rolled(R, sm);
+  __shared__ double sm[kSweepPivotSmem];
+  sweep_pivot_blocked(R, sm);
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
@@ -247,7 +267,7 @@ __device__ __forceinline__ void sweep_update_tile(long long n, int k0, int bk, d
       if (!(i < bk1 && j < bk1)) acc[a][b] = (i == j) ? 1.0 : 0.0;
     }
   __syncthreads();
-  sweep_pivot_rolled(acc, sw_dyn);  // the operand rows are consumed
+  sweep_pivot_blocked(acc, sw_dyn);  // the operand rows are consumed
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
