@@ -75,10 +75,13 @@ __device__ __forceinline__ void sweep_pivot_blocked(double (&R)[4][4], double* s
     // U_Kj = sum_k P[ty][k] M_K:[k][j] for the thread's columns j = tx + 16b
 #pragma unroll
     for (int b = 0; b < 4; ++b) {
-      double u = 0.0;
+      double u0 = 0.0, u1 = 0.0;  // two chains of 8
 #pragma unroll
-      for (int k = 0; k < 16; ++k) u = fma(sP[ty * 16 + k], sRow[k * 64 + tx + 16 * b], u);
-      sU[ty * 64 + tx + 16 * b] = u;
+      for (int k = 0; k < 16; k += 2) {
+        u0 = fma(sP[ty * 16 + k], sRow[k * 64 + tx + 16 * b], u0);
+        u1 = fma(sP[ty * 16 + k + 1], sRow[(k + 1) * 64 + tx + 16 * b], u1);
+      }
+      sU[ty * 64 + tx + 16 * b] = u0 + u1;
     }
     __syncthreads();
 #pragma unroll
@@ -93,10 +96,13 @@ __device__ __forceinline__ void sweep_pivot_blocked(double (&R)[4][4], double* s
         } else if (b == K) {
           R[a][b] = sU[tx * 64 + i];
         } else {
-          double t = R[a][b];
+          double t0 = 0.0, t1 = 0.0;  // two chains of 8
 #pragma unroll
-          for (int k = 0; k < 16; ++k) t = fma(-sRow[k * 64 + i], sU[k * 64 + j], t);
-          R[a][b] = t;
+          for (int k = 0; k < 16; k += 2) {
+            t0 = fma(sRow[k * 64 + i], sU[k * 64 + j], t0);
+            t1 = fma(sRow[(k + 1) * 64 + i], sU[(k + 1) * 64 + j], t1);
+          }
+          R[a][b] -= t0 + t1;
         }
       }
     __syncthreads();
