@@ -282,7 +282,7 @@ constexpr int kCrThreads = 128;
 // BSR: E is block-sparse in the neighbour-slot order (block (G, nbr_list[nbr_ptr[G] + j])
 // at slot nbr_ptr[G] + j, M x M row-major): the nested-dissection coarse solver.
 template <int M, bool BSR = false>
-__global__ void __launch_bounds__(kCrThreads) k_coarse_rows2(GridDims g, KHat kh, DeflP dp,
+__global__ void __launch_bounds__(kCrThreads, 3) k_coarse_rows2(GridDims g, KHat kh, DeflP dp,
                                                              const double* __restrict__ s,
                                                              const uint8_t* __restrict__ mask,
                                                              const int32_t* __restrict__ ngrp,
@@ -1519,6 +1519,11 @@ static int coarse_assemble_launch(const pyto_operator_t* op, const double* s, co
       PYTO_CUDA(cudaFuncSetAttribute(k_coarse_rows2<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, need));
       PYTO_CUDA(cudaFuncSetAttribute(k_coarse_rows2<6, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, need));
       PYTO_CUDA(cudaFuncSetAttribute(k_coarse_rows2<3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, need));
+      // three CTAs of ~74 KB per SM (the register bound allows three)
+      PYTO_CUDA(cudaFuncSetAttribute(k_coarse_rows2<6>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+      PYTO_CUDA(cudaFuncSetAttribute(k_coarse_rows2<3>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+      PYTO_CUDA(cudaFuncSetAttribute(k_coarse_rows2<6, true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+      PYTO_CUDA(cudaFuncSetAttribute(k_coarse_rows2<3, true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
       attr.done();
     }
     double ke_rows = 0.0;  // max absolute row sum of Ke (>= its spectral norm)
