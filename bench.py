@@ -453,7 +453,7 @@ def main():
 
     # the other solver form on the same input, for the mixed / FP64 comparison
     u_main = u.clone()
-    for _ in range(2):
+    for _ in range(max(3, args.warmup)):
         solve_step(P, form=other)
     with ClockSampler(local) as clk_other:
         t_other, u_other, info_other = time_solves(P, other, args.steps, device)
