@@ -177,6 +177,39 @@ __device__ __forceinline__ void grid_reduce(const double (&v)[K], double* part /
   }
 }
 
+// Cross-block step of a fused dot product whose block sum bsum is valid in thread 0.
+// With a counter: grid_reduce, the last block writes the total to *dot_out.  Without
+// one (deferred): every block leaves its sum for the kernel that consumes the dot
+// product (deferred_sum), part[1 + b] for block b and part[0] = the number of blocks:
+// no fence, atomic or last-block pass at the end of the producing kernel.
+__device__ __forceinline__ void dot_finish(double bsum, double* part, unsigned* counter, double* dot_out) {
+  const int nb = (int)(gridDim.x * gridDim.y * gridDim.z);
+  if (counter) {
+    const double v[1] = {bsum};
+    grid_reduce<1>(v, part, counter, nb, [&](const double* t) { *dot_out = t[0]; });
+  } else if (threadIdx.x == 0) {
+    const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    part[1 + bid] = bsum;
+    if (bid == 0) part[0] = (double)nb;
+  }
+}
+
+// Total of the block sums left by dot_finish without a counter, in block order (thread
+// t adds blocks t, t + NT, ...; then block_sum): the same bits in every thread of every
+// CTA that calls it.  sred: >= NT/32 + 1 doubles.
+template <int NT>
+__device__ __forceinline__ double deferred_sum(const double* part, double* sred) {
+  const int n = (int)part[0];
+  double a = 0.0;
+  for (int i = threadIdx.x; i < n; i += NT) a += part[1 + i];
+  const double t = block_sum<NT>(a, sred);
+  if (threadIdx.x == 0) sred[NT / 32] = t;
+  __syncthreads();
+  const double r = sred[NT / 32];
+  __syncthreads();
+  return r;
+}
+
 // Workspace carving helper (256-byte aligned sub-buffers).
 struct Carver {
   char* base;

@@ -1120,10 +1120,13 @@ __global__ void __launch_bounds__(kNodeThreads, 4) k_dpcg_update1(GridDims g, Pr
                                                                const uint8_t* __restrict__ fl, T* __restrict__ x,
                                                                T* __restrict__ r, T* __restrict__ z,
                                                                const T* __restrict__ p, const T* __restrict__ q,
-                                                               KrylovState* S, double* part, unsigned* counter) {
-  __shared__ double sred[kNodeThreads / 32];
+                                                               KrylovState* S, double* part, unsigned* counter,
+                                                               const double* qpart) {
+  __shared__ double sred[kNodeThreads / 32 + 1];
   if (S->done) return;
-  const double pq = S->pq, rz = S->rz;
+  // p.Kp: from the operator's block sums (qpart, deferred) or its finished total
+  const double pq = qpart ? deferred_sum<kNodeThreads>(qpart, sred) : S->pq, rz = S->rz;
+  if (qpart && blockIdx.x == 0 && threadIdx.x == 0) S->pq = pq;
   const double alpha = rz / pq;
   if (!(pq > 0.0) || !isfinite(alpha)) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -1291,6 +1294,7 @@ struct DpcgWs {
   uint8_t* fl;
   double *cv, *mu;     // coarse vectors
   double* rpart;       // restriction partials
+  double* qpart;       // the operator's p.Kp block sums, summed by update1
   int32_t* cptr;       // boundary-list chunk table [ngroups+1]
   int32_t* cgrp;       // group of each chunk [kRkMaxChunks]
   unsigned* gcount;    // per-group chunk counters [ngroups]
@@ -1316,6 +1320,7 @@ static DpcgWs carve_dpcg(const pyto_operator_t* op, long long nc, void* ws, size
   W.S = cv.take<KrylovState>(1);
   W.counter = cv.take<unsigned>(64);
   W.part = cv.take<double>(4 * reduce_slots(op));
+  W.qpart = cv.take<double>(reduce_slots(op) + 1);
   W.r = cv.take<double>(3 * g.nnodes);
   W.p = cv.take<double>(3 * g.nnodes);
   W.q = cv.take<double>(3 * g.nnodes);
@@ -1763,9 +1768,9 @@ static int dpcg_run(const pyto_operator_t* op, const T* s, const uint8_t* mask, 
   auto chunk = [&](cudaStream_t cs) -> int {
     int e;
     for (int k = 0; k < every; ++k) {
-      if ((e = matvec_t(op, s, mask, V.p, V.q, W.part, W.counter, &W.S->pq, cs, &W.S->done))) return e;
+      if ((e = matvec_t(op, s, mask, V.p, V.q, W.qpart, nullptr, &W.S->pq, cs, &W.S->done))) return e;
       k_dpcg_update1<T><<<kUpdate1Blocks, kNodeThreads, 0, cs>>>(g, pc, W.w, W.fl, u, V.r, V.z, V.p, V.q, W.S, W.part,
-                                                              W.counter);
+                                                              W.counter, W.qpart);
       PYTO_COUNT(1);
       // mu = Einv W^T K z (from the boundary lists, or K z -> q then W^T q), p = z + beta p - W mu
       if (lists) {
@@ -2023,9 +2028,9 @@ static int dpcg_reliable(const pyto_operator_t* op, const double* s, const uint8
   auto chunk = [&](cudaStream_t cs) -> int {
     int e;
     for (int k = 0; k < every; ++k) {
-      if ((e = matvec_t(op, sT, mask, p, q, W.part, W.counter, &W.S->pq, cs, &W.S->done))) return e;
+      if ((e = matvec_t(op, sT, mask, p, q, W.qpart, nullptr, &W.S->pq, cs, &W.S->done))) return e;
       k_dpcg_update1<T><<<kUpdate1Blocks, kNodeThreads, 0, cs>>>(g, pc, W.w, W.fl, x, r, z, p, q, W.S, W.part,
-                                                              W.counter);
+                                                              W.counter, W.qpart);
       PYTO_COUNT(1);
       if (lists) {
         if ((e = coarse_update_K(op, g, dp, defl, sT, (const T*)z, p, W, nchunks, W.S, 0, cs))) return e;
@@ -2228,7 +2233,7 @@ static int batch_branch(const pyto_batch_item_t& it, const pyto_solve_cfg_t* cfg
                             sb);
   if (!brc) {
     k_dpcg_update1<double><<<kUpdate1Blocks, kNodeThreads, 0, sb>>>(g, pc, W.w, W.fl, it.u, W.r, W.z, W.p, W.q, W.S,
-                                                                W.part, W.counter);
+                                                                W.part, W.counter, nullptr);
     PYTO_COUNT(1);
     brc = coarse_update_K(op, g, dp, defl, it.s, (const double*)W.z, W.p, W, nchunks, W.S, 0, sb);
   }

@@ -369,10 +369,7 @@ __global__ void __launch_bounds__(32 * TY, MINB)
   __syncthreads();
   if (Z1 - 1 >= Z0) output(Z1 - 1);
   if (DOT) {
-    const double bsum = block_sum<NT>(dot, sred);
-    double v[1] = {bsum};
-    grid_reduce<1>(v, part, counter, (int)(gridDim.x * gridDim.y * gridDim.z),
-                   [&](const double* t) { *dot_out = t[0]; });
+    dot_finish(block_sum<NT>(dot, sred), part, counter, dot_out);
   }
 }
 
