@@ -276,7 +276,7 @@ __device__ __forceinline__ double mode_hat_from_base(const double* B, int stride
 // the coarse operator, its inverse and the solve are bitwise reproducible.  Each
 // contribution is rounded once, to 2^-gexp[G], at most 2^-61 of that magnitude
 // bound.  E is accumulated as int64 bits in place; k_coarse_from_fixed converts it.
-// Only the blocks E[G, H] with H <= G are formed (E is symmetric; k_mirror_upper
+// Only the blocks E[G, H] with H <= G are formed (E is symmetric; k_sym_pass
 // copies them into E[H, G]), and the mode loops are unrolled (M = dp.modes).
 constexpr int kCrThreads = 128;
 // BSR: E is block-sparse in the neighbour-slot order (block (G, nbr_list[nbr_ptr[G] + j])
@@ -511,15 +511,6 @@ __global__ void k_coarse_from_fixed(long long n, int modes, const int* __restric
   }
 }
 
-// E[i, j] = E[j, i] for the entries whose row group is below their column group
-// (the blocks k_coarse_rows2 leaves out)
-__global__ void k_mirror_upper(long long n, int modes, double* E) {
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n * n;
-       t += (long long)gridDim.x * blockDim.x) {
-    const long long i = t / n, j = t - i * n;
-    if (i / modes < j / modes) E[t] = E[j * n + i];
-  }
-}
 
 // mean |diag(E)| (one block) -> *out
 __global__ void k_diag_mean(long long nc, const double* __restrict__ E, double* out) {
@@ -530,21 +521,76 @@ __global__ void k_diag_mean(long long nc, const double* __restrict__ E, double* 
   if (threadIdx.x == 0) *out = t / (double)nc;
 }
 
-// (E + E^T)/2, zero rows -> identity, diagonal shift (relative: times mean |diag|)
-__global__ void k_coarse_finish(long long nc, double* E, double shift, const double* mean_diag) {
-  const double sh = mean_diag ? shift * (*mean_diag) : shift;
-  for (long long i = blockIdx.x; i < nc; i += gridDim.x) {
-    for (long long j = threadIdx.x; j < i; j += blockDim.x) {
-      const double a = 0.5 * (E[i * nc + j] + E[j * nc + i]);
-      E[i * nc + j] = a;
-      E[j * nc + i] = a;
+
+// The symmetric passes over the dense coarse matrix, by 32 x 32 tile pairs (I >= J; one
+// CTA of 32 x 8 threads stages tile (I, J) and tile (J, I) with loads along rows and
+// writes both back the same way), entry (i, j) with a = E[i][j], b = E[j][i]:
+//   kSymMirror: the row-group-lower blocks into the upper ones (E is assembled for
+//               group(row) >= group(col) only): both = the value of the lower group side;
+//               entries of one group block are left as they are;
+//   kSymFinish: (E + E^T) / 2, a zero diagonal entry -> 1, plus the diagonal shift;
+//   kSymNegate: -A from the lower 64 x 64 tiles (the sweep's result) into both halves.
+constexpr int kSymMirror = 0, kSymFinish = 1, kSymNegate = 2;
+__global__ void __launch_bounds__(256) k_sym_pass(long long n, int modes, double* E, int op, double shift,
+                                                  const double* mean_diag) {
+  __shared__ double ta[32][33], tb[32][33];
+  const long long t = blockIdx.x;
+  long long I = (long long)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+  while (I * (I + 1) / 2 > t) --I;
+  while ((I + 1) * (I + 2) / 2 <= t) ++I;
+  const long long J = t - I * (I + 1) / 2;
+  const long long i0 = 32 * I, j0 = 32 * J;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+#pragma unroll
+  for (int r = ty; r < 32; r += 8) {
+    const long long ia = i0 + r, ja = j0 + tx, ib = j0 + r, jb = i0 + tx;
+    ta[r][tx] = (ia < n && ja < n) ? E[ia * n + ja] : 0.0;  // rows of tile (I, J)
+    tb[r][tx] = (ib < n && jb < n) ? E[ib * n + jb] : 0.0;  // rows of tile (J, I)
+  }
+  __syncthreads();
+  const double sh = (op == kSymFinish) ? (mean_diag ? shift * (*mean_diag) : shift) : 0.0;
+  // thread (ty, tx) writes row r of tile (I, J): entry (i0 + r, j0 + tx), and row r of
+  // tile (J, I): entry (j0 + r, i0 + tx)
+#pragma unroll
+  for (int r = ty; r < 32; r += 8) {
+    const long long i = i0 + r, j = j0 + tx;
+    if (i < n && j < n) {
+      const double a = ta[r][tx], b = tb[tx][r];  // E[i][j], E[j][i]
+      double v;
+      if (op == kSymMirror) {
+        const long long gi = i / modes, gj = j / modes;
+        v = gi > gj ? a : gi < gj ? b : a;
+      } else if (op == kSymFinish) {
+        v = (i == j) ? ((a == 0.0 ? 1.0 : a) + sh) : 0.5 * (a + b);
+      } else {
+        v = ((i >> 6) >= (j >> 6)) ? -a : -b;
+      }
+      E[i * n + j] = v;
     }
-    if (threadIdx.x == 0) {
-      double d = E[i * nc + i];
-      if (d == 0.0) d = 1.0;  // column of W that vanishes on the free DOFs
-      E[i * nc + i] = d + sh;
+    const long long i2 = j0 + r, j2 = i0 + tx;  // the transposed entry (i2, j2)
+    if (I != J && i2 < n && j2 < n) {
+      const double a = tb[r][tx], b = ta[tx][r];  // E[i2][j2], E[j2][i2]
+      double v;
+      if (op == kSymMirror) {
+        const long long gi = i2 / modes, gj = j2 / modes;
+        v = gi > gj ? a : gi < gj ? b : a;
+      } else if (op == kSymFinish) {
+        v = 0.5 * (b + a);
+      } else {
+        v = ((i2 >> 6) >= (j2 >> 6)) ? -a : -b;
+      }
+      E[i2 * n + j2] = v;
     }
   }
+}
+
+static int sym_pass(long long n, int modes, double* E, int op, double shift, const double* mean_diag,
+                    cudaStream_t st) {
+  const long long nt = (n + 31) / 32;
+  k_sym_pass<<<(int)(nt * (nt + 1) / 2), 256, 0, st>>>(n, modes, E, op, shift, mean_diag);
+  PYTO_COUNT(1);
+  PYTO_LAUNCH_CHECK();
+  return PYTO_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -585,18 +631,6 @@ __global__ void __launch_bounds__(256, 2) k_sweep_update(long long n, int k0, in
   sweep_update_tile(n, k0, bk, A, P, Rp, U, ti, tj, k1, Pn, k1 >= 0 ? (int)std::min<long long>(kSweepB, n - k1) : 0);
 }
 
-// E^-1 = -A: negate the lower tiles (diagonal tiles in full) and mirror them
-// into the upper tiles; each entry pair is handled by one thread
-__global__ void k_negate_sym(long long n, double* A) {
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n * n;
-       t += (long long)gridDim.x * blockDim.x) {
-    const long long i = t / n, j = t - i * n;
-    if ((i >> 6) < (j >> 6)) continue;  // upper tile: written from its mirror
-    const double v = -A[t];
-    A[t] = v;
-    if ((i >> 6) > (j >> 6)) A[j * n + i] = v;
-  }
-}
 
 // ---------------------------------------------------------------------------
 // DPCG pieces
@@ -1566,8 +1600,8 @@ static int coarse_assemble_launch(const pyto_operator_t* op, const double* s, co
     k_coarse_from_fixed<<<(int)std::min<long long>((n * n + 255) / 256, 8 * kNumSMs), 256, 0, st>>>(n, dp.modes,
                                                                                                    W.gexp, E);
     PYTO_COUNT(1);
-    k_mirror_upper<<<(int)std::min<long long>((n * n + 255) / 256, 8 * kNumSMs), 256, 0, st>>>(n, dp.modes, E);
-    PYTO_COUNT(1);
+    const int rc = sym_pass(n, dp.modes, E, kSymMirror, 0.0, nullptr, st);
+    if (rc) return rc;
   } else {
     k_coarse_rows<<<dp.ngroups, kAsmThreads, shm, st>>>(g, make_khat(op), dp, s, mask, defl->node_group,
                                                          defl->group_center, defl->group_box, defl->nbr_ptr,
@@ -1587,9 +1621,10 @@ static int coarse_invert_launch(const pyto_deflation_t* defl, const DpcgWs& W, c
     k_diag_mean<<<1, 256, 0, st>>>(n, E, W.part);
     PYTO_COUNT(1);
   }
-  k_coarse_finish<<<(int)std::min<long long>(n, 4 * kNumSMs), 256, 0, st>>>(
-      n, E, defl->shift, defl->shift_relative ? W.part : nullptr);
-  PYTO_COUNT(1);
+  {
+    const int rc = sym_pass(n, defl->modes, E, kSymFinish, defl->shift, defl->shift_relative ? W.part : nullptr, st);
+    if (rc) return rc;
+  }
   PYTO_LAUNCH_CHECK();
   const int tiles = (int)((n + 63) / 64);
   static PerDevice attr;
@@ -1614,8 +1649,10 @@ static int coarse_invert_launch(const pyto_deflation_t* defl, const DpcgWs& W, c
                                                                              (int)k1, Pn);
     PYTO_COUNT(1);
   }
-  k_negate_sym<<<(int)std::min<long long>((n * n + 255) / 256, 8 * kNumSMs), 256, 0, st>>>(n, E);
-  PYTO_COUNT(1);
+  {
+    const int rc = sym_pass(n, defl->modes, E, kSymNegate, 0.0, nullptr, st);
+    if (rc) return rc;
+  }
   PYTO_LAUNCH_CHECK();
   return PYTO_OK;
 }
