@@ -172,7 +172,38 @@ __device__ __forceinline__ void sweep_panel_cols(long long n, int k0, int bk, co
 
 // Dynamic shared memory of sweep_update_tile: the tile rows' A_iK and the tile columns'
 // U_Kj for all bk <= 64 pivots (2 x 64 x 64 doubles).
-constexpr size_t kSweepTileSmem = 2 * 64 * 64 * sizeof(double);
+constexpr int kSweepP = 68;  // operand row pitch: the tensor-core fragment loads are free of bank conflicts
+constexpr size_t kSweepTileSmem = 2 * 64 * kSweepP * sizeof(double);
+
+// acc[i][j] = sum_k L[k][i] U[k][j] over the 64 x 64 tile (k < kmax, a multiple of 4;
+// L, U: k-major in shared memory, pitch kSweepP) on the FP64 tensor cores: warp w owns
+// rows 8w..8w+7, eight m8n8k4 products per 4 k; lane (g = lane / 4, t = lane % 4) holds
+// A[g][t] = L[k + t][8w + g], B[t][g] = U[k + t][8c + g] and C[g][2t], C[g][2t + 1].
+// The 8 x 64 result rows are written to S (pitch 65) for the caller's own layout.
+__device__ __forceinline__ void sweep_tile_mma(const double* L, const double* U, int kmax, double* S) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+  double c[8][2];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) c[q][0] = c[q][1] = 0.0;
+#pragma unroll 2
+  for (int k = 0; k < kmax; k += 4) {
+    const double a = L[(k + t) * kSweepP + 8 * w + g];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const double b = U[(k + t) * kSweepP + 8 * q + g];
+      asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                   : "+d"(c[q][0]), "+d"(c[q][1])
+                   : "d"(a), "d"(b));
+    }
+  }
+  __syncthreads();  // L and U consumed: S may overlay them
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    S[(8 * w + g) * 65 + 8 * q + 2 * t] = c[q][0];
+    S[(8 * w + g) * 65 + 8 * q + 2 * t + 1] = c[q][1];
+  }
+  __syncthreads();
+}
 
 // Update of the lower 64 x 64 tile (ti, tj) by 256 threads x (4 x 4) outputs for the
 // pivot block at k0 (tiles in row or column K take U / -P); k1 >= 0 and (ti, tj) =
@@ -184,8 +215,8 @@ __device__ __forceinline__ void sweep_update_tile(long long n, int k0, int bk, d
                                                   const double* __restrict__ U, long long ti, long long tj, int k1,
                                                   double* __restrict__ Pn, int bk1) {
   extern __shared__ double sw_dyn[];
-  double* sL = sw_dyn;            // [64][64]: A_iK for the tile rows (Rp[k][i0 + c])
-  double* sU = sw_dyn + 64 * 64;  // [64][64]: U_Kj for the tile columns
+  double* sL = sw_dyn;                 // [64][kSweepP]: A_iK for the tile rows (Rp[k][i0 + c])
+  double* sU = sw_dyn + 64 * kSweepP;  // [64][kSweepP]: U_Kj for the tile columns
   const long long i0 = ti * 64, j0 = tj * 64;
   const bool rowK = (i0 == k0), colK = (j0 == k0);
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
@@ -219,7 +250,8 @@ __device__ __forceinline__ void sweep_update_tile(long long n, int k0, int bk, d
   for (int r = 0; r < PER; ++r) {  // 8-byte asynchronous copies (zero-filled outside)
     const int t = threadIdx.x + 256 * r, k = t / 64, c = t % 64;
     const bool okl = k < bk && i0 + c < n, oku = k < bk && j0 + c < n;
-    const unsigned dl = (unsigned)__cvta_generic_to_shared(sL + t), du = (unsigned)__cvta_generic_to_shared(sU + t);
+    const unsigned dl = (unsigned)__cvta_generic_to_shared(sL + k * kSweepP + c),
+                   du = (unsigned)__cvta_generic_to_shared(sU + k * kSweepP + c);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dl),
                  "l"(okl ? Rp + k * n + i0 + c : Rp), "r"(okl ? 8 : 0) : "memory");
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(du),
@@ -228,23 +260,14 @@ __device__ __forceinline__ void sweep_update_tile(long long n, int k0, int bk, d
   asm volatile("cp.async.commit_group;\n" ::: "memory");
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   __syncthreads();
+  // the rank-bk product on the tensor cores (operand rows >= bk are zero), then each
+  // thread takes its 4 x 4 outputs (rows ty + 16a, columns tx + 16b)
+  sweep_tile_mma(sL, sU, (bk + 3) & ~3, sw_dyn);
   double acc[4][4];
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-#pragma unroll 4
-  for (int k = 0; k < bk; ++k) {
-    double l[4], u[4];
-#pragma unroll
-    for (int a = 0; a < 4; ++a) l[a] = sL[k * 64 + ty + 16 * a];
-#pragma unroll
-    for (int b = 0; b < 4; ++b) u[b] = sU[k * 64 + tx + 16 * b];
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int b = 0; b < 4; ++b) acc[a][b] = fma(l[a], u[b], acc[a][b]);
-  }
+    for (int b = 0; b < 4; ++b) acc[a][b] = sw_dyn[(ty + 16 * a) * 65 + tx + 16 * b];
   const bool pivot_next = k1 >= 0 && i0 == k1 && j0 == k1;
 #pragma unroll
   for (int a = 0; a < 4; ++a)
