@@ -1800,8 +1800,6 @@ static int dpcg_run(const pyto_operator_t* op, const T* s, const uint8_t* mask, 
     PYTO_COUNT(1);
   }
   PYTO_LAUNCH_CHECK();
-  PYTO_CUDA(cudaMemcpyAsync(hs, W.S, sizeof(*hs), cudaMemcpyDeviceToHost, st));
-  PYTO_CUDA(cudaStreamSynchronize(st));
   auto chunk = [&](cudaStream_t cs) -> int {
     int e;
     for (int k = 0; k < every; ++k) {
@@ -1823,8 +1821,11 @@ static int dpcg_run(const pyto_operator_t* op, const T* s, const uint8_t* mask, 
     PYTO_LAUNCH_CHECK();
     return PYTO_OK;
   };
+  // the chunk graph is captured while the set-up queued before it still runs on the GPU
   ChunkGraph cg;
-  if (g_use_graphs && !hs->done && (rc = cg.build(chunk))) return rc;
+  if (g_use_graphs && (rc = cg.build(chunk))) return rc;
+  PYTO_CUDA(cudaMemcpyAsync(hs, W.S, sizeof(*hs), cudaMemcpyDeviceToHost, st));
+  PYTO_CUDA(cudaStreamSynchronize(st));
   while (!hs->done && hs->iters < max_iters) {
     if ((rc = g_use_graphs ? cg.launch(st) : chunk(st))) return rc;
     PYTO_LAUNCH_CHECK();
@@ -2051,17 +2052,10 @@ static int dpcg_reliable(const pyto_operator_t* op, const double* s, const uint8
   if ((rc = reliable(warm))) return rc;
   if ((rc = restart_p())) return rc;
   PYTO_LAUNCH_CHECK();
-  KrylovState hs{};
-  PYTO_CUDA(cudaMemcpyAsync(&hs, W.S, sizeof(hs), cudaMemcpyDeviceToHost, st));
-  PYTO_CUDA(cudaStreamSynchronize(st));
   // the replacement triggers are tested between chunks: at most kReliablePoll
   // iterations apart whatever the caller's polling interval (a longer unreplaced
   // run of the low-precision recurrence loses the accuracy the replacement restores)
   every = std::min(every, kReliablePoll);
-  double rr_ref = hs.rr;
-  double true_prev = hs.true_rr;  // true ||r||^2 at the previous update
-  int updates = 1, restarts = 0, seg0 = 0;
-  const double d2 = delta * delta;
   auto chunk = [&](cudaStream_t cs) -> int {
     int e;
     for (int k = 0; k < every; ++k) {
@@ -2082,8 +2076,16 @@ static int dpcg_reliable(const pyto_operator_t* op, const double* s, const uint8
     PYTO_LAUNCH_CHECK();
     return PYTO_OK;
   };
+  // the chunk graph is captured while the set-up queued before it still runs on the GPU
   ChunkGraph cg;
-  if (g_use_graphs && !hs.converged && (rc = cg.build(chunk))) return rc;
+  if (g_use_graphs && (rc = cg.build(chunk))) return rc;
+  KrylovState hs{};
+  PYTO_CUDA(cudaMemcpyAsync(&hs, W.S, sizeof(hs), cudaMemcpyDeviceToHost, st));
+  PYTO_CUDA(cudaStreamSynchronize(st));
+  double rr_ref = hs.rr;
+  double true_prev = hs.true_rr;  // true ||r||^2 at the previous update
+  int updates = 1, restarts = 0, seg0 = 0;
+  const double d2 = delta * delta;
   while (!hs.converged && hs.iters < cfg->max_iters) {
     if ((rc = g_use_graphs ? cg.launch(st) : chunk(st))) return rc;
     PYTO_LAUNCH_CHECK();
